@@ -1,0 +1,81 @@
+/*
+ * N-step driver for the reference solver built against the single-rank shims
+ * (oracle build only: it links the reference's own .c files under src/).
+ *
+ * The reference main loop (src/main.c:87-118) has no step-count limit and
+ * interleaves logging/saving, so this driver restates only its start-up
+ * (src/main.c:46-85: step/time NPYs, domain_init, fluid_init) and then calls
+ * integrate() (src/integrate.c:9-35) a fixed number of times.
+ *
+ *   tcref_<cfg> <ic_dir> <warmup_steps> <timed_steps> [<out_dir>]
+ *
+ * Environment (as the reference reads it): Re, Pr, coef_dt_adv, coef_dt_dif.
+ * The warm-up steps absorb the reference's first-call lazy initialisation
+ * (FFT plans, linear-system buffers, Laplacian tables); only the timed steps
+ * are clocked. With <out_dir>, the final state is written in the reference's
+ * save layout (src/save.c:74-110) so it can be compared or restarted from.
+ * Prints one JSON line on stdout.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <stdio.h>
+#include <stdlib.h>
+#include <time.h>
+#include <sys/stat.h>
+#include <mpi.h>
+#include "domain.h"
+#include "fluid.h"
+#include "fluid_solver.h"
+#include "integrate.h"
+#include "fileio.h"
+
+static double now(void){
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1.e-9 * (double)ts.tv_nsec;
+}
+
+int main(int argc, char * argv[]){
+  if(argc < 4){
+    fprintf(stderr, "usage: %s <ic_dir> <warmup_steps> <timed_steps> [<out_dir>]\n", argv[0]);
+    return 2;
+  }
+  const char * dirname_ic = argv[1];
+  const long warmup = atol(argv[2]);
+  const long nsteps = atol(argv[3]);
+  const char * outdir = argc > 4 ? argv[4] : NULL;
+  MPI_Init(NULL, NULL);
+  if(0 != fileio.init()) return 1;
+  size_t step = 0;
+  if(0 != fileio.r_serial(dirname_ic, "step", 0, NULL, fileio.npy_size_t, sizeof(size_t), &step)) return 1;
+  double time = 0.;
+  if(0 != fileio.r_serial(dirname_ic, "time", 0, NULL, fileio.npy_double, sizeof(double), &time)) return 1;
+  domain_t domain = {0};
+  if(0 != domain_init(dirname_ic, &domain)) return 1;
+  fluid_t fluid = {0};
+  if(0 != fluid_init(dirname_ic, &domain, &fluid)) return 1;
+  double dt = 0.;
+  for(long n = 0; n < warmup; n++){
+    if(0 != integrate(&domain, &fluid, &dt)) return 1;
+    step += 1;
+    time += dt;
+  }
+  const double tic = now();
+  for(long n = 0; n < nsteps; n++){
+    if(0 != integrate(&domain, &fluid, &dt)) return 1;
+    step += 1;
+    time += dt;
+  }
+  const double toc = now();
+  if(NULL != outdir){
+    mkdir(outdir, 0755);
+    fileio.w_serial(outdir, "step", 0, NULL, fileio.npy_size_t, sizeof(size_t), &step);
+    fileio.w_serial(outdir, "time", 0, NULL, fileio.npy_double, sizeof(double), &time);
+    if(0 != domain_save(outdir, &domain)) return 1;
+    if(0 != fluid_save(outdir, &domain, &fluid)) return 1;
+  }
+  const size_t ncells = domain.glsizes[0] * domain.glsizes[1] * domain.glsizes[2];
+  printf("{\"cells\": %zu, \"warmup\": %ld, \"steps\": %ld, \"seconds\": %.9e, \"dt_last\": %.17e, \"time\": %.17e}\n",
+      ncells, warmup, nsteps, toc - tic, dt, time);
+  MPI_Finalize();
+  return 0;
+}
