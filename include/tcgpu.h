@@ -1,0 +1,224 @@
+/*
+ * tcgpu — B200 (sm_100a) implementation of SimpleTCSolver's RK3 time step
+ * behind the reference's own C entry points.
+ *
+ * Drop-in boundary: the structs below are layout-compatible with the
+ * reference's domain_t / array_t / fluid_t / tdm_t, and every function in the
+ * "reference entry points" section keeps the reference's name, signature,
+ * argument meaning and 0 / non-zero return convention (errors are also printed
+ * to stderr). A C host that links libtcgpu.so instead of the reference's
+ * src/integrate.c, src/decide_dt.c, src/fluid/{predict,correct,boundary}/,
+ * src/fluid/compute_potential.c, src/fluid/update_pressure.c, src/tdm.c,
+ * src/linear_system.c and src/halo.c runs its time step on the GPU.
+ *
+ * One GPU owns the whole domain: mysizes must equal glsizes and offsets be 0
+ * (a single rank). The solver state (device copies of the fields, RK source
+ * terms, spectral buffers) lives in a context created on the first call for a
+ * given fluid_t and released by tcgpu_release().
+ *
+ * Coherence: by default each reference entry point reads the fields it needs
+ * from the caller's host arrays and writes back the fields it changes, so the
+ * caller sees exactly the reference's side effects ("coherent" mode). The
+ * tcgpu_* extensions at the end let a caller keep the state on the GPU across
+ * many steps and copy only when it wants to.
+ */
+#if !defined(TCGPU_H)
+#define TCGPU_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+#if !defined(NDIMS)
+#define NDIMS 3
+#endif
+
+/* ---------------------------------------------------------------- types */
+
+/* opaque: the reference's SimpleDecomp handle; this library never reads it */
+typedef struct sdecomp_info_t_ sdecomp_info_t;
+
+/* include/array.h:9-23 */
+typedef struct {
+  size_t size;
+  int (* nadds)[2];
+  size_t datasize;
+  void * data;
+} array_t;
+
+/* include/domain.h:23-37 */
+typedef struct {
+  sdecomp_info_t * info;
+  bool is_curved;
+  size_t glsizes[NDIMS];
+  size_t mysizes[NDIMS];
+  size_t offsets[NDIMS];
+  double lengths[NDIMS];
+  double * xf, * xc;
+  double * jdxf, * jdxc;
+  double * hxxf, * hxxc;
+  double * hyxf, * hyxc;
+  double hz;
+} domain_t;
+
+/* include/fluid.h:18-36 */
+typedef struct {
+  array_t ux;
+  array_t uy;
+  array_t uz;
+  array_t p;
+  array_t psi;
+  array_t t;
+  array_t srcux[3];
+  array_t srcuy[3];
+  array_t srcuz[3];
+  array_t srct[3];
+  array_t lxx;
+  array_t lyx0, lyx1, lxy;
+  array_t lzx, lxz;
+  array_t lyy0, lyy1;
+  array_t lzy, lyz;
+  array_t lzz;
+  double Re, Pr;
+} fluid_t;
+
+typedef struct tdm_info_t_ tdm_info_t;
+
+/* include/tdm.h:8-42 */
+typedef struct {
+  int (* const construct)(const int size, const int nrhs, const bool is_periodic, const bool is_complex, tdm_info_t ** info);
+  int (* const get_l)(const tdm_info_t * info, double ** l);
+  int (* const get_c)(const tdm_info_t * info, double ** c);
+  int (* const get_u)(const tdm_info_t * info, double ** u);
+  int (* const get_size)(const tdm_info_t * info, int * size);
+  int (* const get_nrhs)(const tdm_info_t * info, int * nrhs);
+  int (* const solve)(const tdm_info_t * info, void * data);
+  int (* const destruct)(tdm_info_t * info);
+} tdm_t;
+
+/* include/runge_kutta.h:8-15 */
+typedef double rkcoef_t[3];
+
+/* ---------------------------------------------------- reference entry points */
+
+/* include/integrate.h:5-9, src/integrate.c:9-35: decide_dt, then three RK
+ * substeps of predict / compute_potential / correct / update_pressure */
+int integrate(const domain_t * domain, fluid_t * fluid, double * dt);
+
+/* include/decide_dt.h:5-9, src/decide_dt.c:125-160; reads coef_dt_adv and
+ * coef_dt_dif from the environment on first use, as the reference does */
+int decide_dt(const domain_t * domain, const fluid_t * fluid, double * dt);
+
+/* include/fluid_solver.h:31-36, src/fluid/predict/main.c:35-110 */
+int fluid_predict_field(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid);
+
+/* include/fluid_solver.h:39-44, src/fluid/compute_potential.c:499-583.
+ * The singular zero-wavenumber mode is pinned by setting its last radial
+ * unknown to zero, so psi (and p) can differ from the reference's by an
+ * additive constant; the reference leaves that constant to round-off. */
+int fluid_compute_potential(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid);
+
+/* include/fluid_solver.h:47-52, src/fluid/correct/main.c:15-28 */
+int fluid_correct_velocity(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid);
+
+/* include/fluid_solver.h:55-60, src/fluid/update_pressure.c:146-173 */
+int fluid_update_pressure(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid);
+
+/* include/fluid_solver.h:64-92, src/fluid/boundary/*.c + src/halo.c:
+ * wall values / Neumann copies, then periodic y and z images */
+int fluid_update_boundaries_ux(const domain_t * domain, array_t * array);
+int fluid_update_boundaries_uy(const domain_t * domain, array_t * array);
+int fluid_update_boundaries_uz(const domain_t * domain, array_t * array);
+int fluid_update_boundaries_p(const domain_t * domain, array_t * array);
+int fluid_update_boundaries_psi(const domain_t * domain, array_t * array);
+int fluid_update_boundaries_t(const domain_t * domain, array_t * array);
+
+/* include/fluid_solver.h:22-28, src/fluid/compute_diffusivity.c */
+double fluid_compute_momentum_diffusivity(const fluid_t * fluid);
+double fluid_compute_scalar_diffusivity(const fluid_t * fluid);
+
+/* include/fluid_solver.h:9-19, src/fluid/init.c:98-122, src/fluid/save.c:8-28:
+ * NPY load/save in the reference layout; Re and Pr come from the environment */
+int fluid_init(const char dirname_ic[], const domain_t * domain, fluid_t * fluid);
+int fluid_save(const char dirname[], const domain_t * domain, const fluid_t * fluid);
+
+/* include/domain.h:40-47, src/domain.c:63-86, 389-432 (single rank) */
+int domain_init(const char dirname_ic[], domain_t * domain);
+int domain_save(const char dirname[], const domain_t * domain);
+
+/* include/tdm.h:44 + src/tdm.c:255-325: batched tri-diagonal solver; solve()
+ * accepts host or device memory and runs on the GPU */
+extern const tdm_t tdm;
+
+/* include/runge_kutta.h:8-15, src/runge_kutta.c:3-15 */
+extern const uint_fast8_t rk_a;
+extern const uint_fast8_t rk_b;
+extern const uint_fast8_t rk_g;
+extern const rkcoef_t rkcoefs[3];
+
+/* ------------------------------------------------------------- extensions */
+/* No counterparts in the reference: run-time replacements for its
+ * compile-time constants, explicit residency control and diagnostics. */
+
+/* replaces src/param/boundary-condition.c and src/param/implicit.c; the
+ * defaults are the reference's shipped values (uy walls 1 / 0, scalar walls
+ * +0.5 / -0.5, implicit diffusion in x only). coef_dt_* < 0 keeps the value
+ * taken from the environment. Applies to contexts created afterwards. */
+typedef struct {
+  double uy_xm, uy_xp;
+  double t_xm, t_xp;
+  int implicit_x, implicit_y, implicit_z;
+  double coef_dt_adv, coef_dt_dif;
+} tcgpu_params_t;
+
+int tcgpu_set_params(const tcgpu_params_t * params);
+int tcgpu_get_params(tcgpu_params_t * params);
+
+/* what the reference entry points copy back to the host besides the fields
+ * they change (bit mask, per context) */
+#define TCGPU_SYNC_SRCS    1u  /* RK source terms after fluid_predict_field */
+#define TCGPU_SYNC_TENSORS 2u  /* velocity-gradient tensors after fluid_predict_field */
+#define TCGPU_NO_COHERENCE 4u  /* copy nothing: the caller uses tcgpu_push/pull */
+#define TCGPU_PIN_HOST     8u  /* page-lock the caller's six field arrays until
+                                  tcgpu_release (faster host<->device copies) */
+int tcgpu_set_coherence(const domain_t * domain, fluid_t * fluid, unsigned flags);
+
+/* field masks for tcgpu_push / tcgpu_pull */
+#define TCGPU_UX  1u
+#define TCGPU_UY  2u
+#define TCGPU_UZ  4u
+#define TCGPU_P   8u
+#define TCGPU_PSI 16u
+#define TCGPU_T   32u
+#define TCGPU_FIELDS 63u
+#define TCGPU_SRCS 64u
+#define TCGPU_TENSORS 128u
+int tcgpu_push(const domain_t * domain, fluid_t * fluid, unsigned fields);
+int tcgpu_pull(const domain_t * domain, fluid_t * fluid, unsigned fields);
+
+/* run nsteps full time steps on the device without host copies; dts (may be
+ * NULL) receives each step's dt */
+int tcgpu_run(const domain_t * domain, fluid_t * fluid, int nsteps, double * dts);
+
+/* logging quantities of src/logging/*.c from the device state:
+ * out[0] max |div u|, out[1..2] energy injection (momentum, scalar),
+ * out[3..4] dissipation (momentum, scalar), out[5..8] total energy
+ * (ux, uy, uz, scalar). Injection and dissipation use the velocity-gradient
+ * tensors of the current fields. */
+int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]);
+
+/* free the device state that belongs to this fluid_t */
+int tcgpu_release(fluid_t * fluid);
+
+/* last error message of this thread ("" when none) */
+const char * tcgpu_last_error(void);
+
+#if defined(__cplusplus)
+}
+#endif
+
+#endif // TCGPU_H

@@ -1,0 +1,75 @@
+// Shared definitions of the tcgpu kernels.
+//
+// HBM layout of the fields is the reference's own (array_macros/fluid/*.h):
+// x fastest, one halo layer in y and z, and in x either the two walls/ghosts
+// (uy, uz, p, psi, t: i = 0..nx+1, row length nx+2) or the faces only
+// (ux: i = 1..nx+1, row length nx+1). Keeping the reference layout makes the
+// host<->device copies of the drop-in entry points single memcpys. Every kernel
+// that writes a cell also writes its periodic images in the y/z halo and the
+// wall value of its row, which is what halo.c and boundary/*.c do on the CPU.
+//
+// RK source terms and increments use the reference's packed interior layout
+// (srcux: i = 2..nx, others i = 1..nx; src/fluid/predict/*.c BEGIN loops).
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace tcgpu {
+
+// Wray RK3, src/runge_kutta.c:8-15
+__host__ __device__ constexpr double rk_alpha(int s) { return s == 0 ? 32. / 60. : s == 1 ? 25. / 60. : 45. / 60.; }
+__host__ __device__ constexpr double rk_beta(int s)  { return s == 0 ? 0. / 60. : s == 1 ? -17. / 60. : -25. / 60.; }
+__host__ __device__ constexpr double rk_gamma(int s) { return rk_alpha(s) + rk_beta(s); }
+
+enum Var { VUX = 0, VUY = 1, VUZ = 2, VT = 3 };
+
+// sizes and metric tables, passed to every kernel by value
+struct Geo {
+  int nx, ny, nz;
+  double hz;
+  // length nx+2, indexed by the reference's i (unused entries are zero)
+  const double * hxxf;
+  const double * hxxc;
+  const double * hyxf;
+  const double * hyxc;
+  const double * jdxf;
+  const double * jdxc;
+};
+
+// runtime replacement of src/param/*.c
+struct Bc {
+  double uy_xm, uy_xp, t_xm, t_xp;
+  int implicit[3];
+};
+
+__host__ __device__ inline size_t cidx(const Geo & g, int i, int j, int k) {
+  return (size_t)i + (size_t)(g.nx + 2) * ((size_t)j + (size_t)(g.ny + 2) * (size_t)k);
+}
+__host__ __device__ inline size_t fidx(const Geo & g, int i, int j, int k) {
+  return (size_t)(i - 1) + (size_t)(g.nx + 1) * ((size_t)j + (size_t)(g.ny + 2) * (size_t)k);
+}
+__host__ __device__ inline size_t ncell_c(const Geo & g) { return (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2); }
+__host__ __device__ inline size_t ncell_f(const Geo & g) { return (size_t)(g.nx + 1) * (g.ny + 2) * (g.nz + 2); }
+// packed interior index; i0 = 2 for ux, 1 otherwise
+__host__ __device__ inline size_t pidx(int n_i, int ny, int ii, int j, int k) {
+  return (size_t)ii + (size_t)n_i * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
+}
+
+// periodic images of interior (j, k) in the one-layer halo, including the
+// corner written by the z exchange after the y exchange (src/halo.c:18-142);
+// ny, nz >= 2 (the FFTs require powers of two >= 4)
+template <typename F>
+__device__ inline void for_images(int j, int k, int ny, int nz, F && f) {
+  const int jj = (j == 1) ? ny + 1 : (j == ny) ? 0 : -1;
+  const int kk = (k == 1) ? nz + 1 : (k == nz) ? 0 : -1;
+  if (jj >= 0) f(jj, k);
+  if (kk >= 0) f(j, kk);
+  if (jj >= 0 && kk >= 0) f(jj, kk);
+}
+
+// device-side status word: set by kernels, read by the host after a step
+enum : unsigned { ST_NONFINITE = 1u, ST_BADDT = 2u };
+
+}  // namespace tcgpu

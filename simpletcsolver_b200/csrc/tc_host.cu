@@ -1,0 +1,931 @@
+// Host runtime of tcgpu: per-fluid device contexts, the step schedule (one
+// CUDA stream, the full time step captured once as a CUDA graph), host<->device
+// coherence, and the exported C entry points of include/tcgpu.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "tcgpu.h"
+#include "tc_common.cuh"
+#include "tc_kernels.h"
+
+using namespace tcgpu;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+static int fail(const char * fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  fprintf(stderr, "tcgpu: %s\n", buf);
+  fflush(stderr);
+  return 1;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) return fail("%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ parameters
+// defaults: the reference's shipped src/param/boundary-condition.c and implicit.c
+static tcgpu_params_t g_params = {1.0, 0.0, 0.5, -0.5, 1, 0, 0, -1.0, -1.0};
+static std::mutex g_mutex;
+
+static int env_double(const char * name, double * value) {
+  // src/config.c:14-46
+  const char * s = getenv(name);
+  if (s == nullptr) return fail("%s not found", name);
+  errno = 0;
+  *value = strtod(s, nullptr);
+  if (errno != 0) return fail("%s: invalid value as double", name);
+  return 0;
+}
+
+// ------------------------------------------------------------------ context
+struct Ctx {
+  const fluid_t * key = nullptr;
+  int nx = 0, ny = 0, nz = 0;
+  size_t nc = 0, nf = 0;
+  Geo g{};
+  Bc bc{};
+  Coefs cf{};
+  XFactors xf{};
+  YZFactors yf{};
+  Poisson ps{};
+  Fields f{};
+  double * src[4][2]{};
+  double * delta[4]{};
+  double * tab_y = nullptr;
+  double * tab_z = nullptr;
+  double * base = nullptr;
+  double * dt_caps = nullptr;
+  double * dtp = nullptr;
+  unsigned long long * dtmin = nullptr;
+  unsigned * status = nullptr;
+  double * diag_out = nullptr;
+  double * diag_part = nullptr;
+  Tensors tn{};
+  bool have_tn = false;
+  double coef_adv = 0., coef_dif = 0.;
+  double Re = 0., Pr = 0., nu = 0., kappa = 0.;
+  double caps_h[3] = {0., 0., 0.};
+  unsigned coherence = 0;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t step_graph = nullptr;
+  std::vector<void *> pinned;     // caller arrays registered with cudaHostRegister
+  double * h_scalar = nullptr;    // pinned: dt in / out
+  unsigned * h_status = nullptr;  // pinned
+  std::vector<void *> allocs;
+};
+
+static std::map<const fluid_t *, Ctx *> g_ctx;
+
+static double * dalloc(Ctx & c, size_t n) {
+  void * p = nullptr;
+  if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, n * sizeof(double));
+  c.allocs.push_back(p);
+  return static_cast<double *>(p);
+}
+
+static void destroy_ctx(Ctx * c) {
+  if (c == nullptr) return;
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  for (void * p : c->pinned) cudaHostUnregister(p);
+  for (void * p : c->allocs) cudaFree(p);
+  if (c->h_scalar) cudaFreeHost(c->h_scalar);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+static bool is_pow2(size_t n) { return n >= 4 && (n & (n - 1)) == 0; }
+
+// metric accessors of the reference's domain_t (array_macros/domain/*.h)
+struct Metric {
+  std::vector<double> hxxf, hxxc, hyxf, hyxc, jdxf, jdxc;  // length nx+2, index = i
+};
+
+static void read_metric(const domain_t * d, int nx, Metric & m) {
+  m.hxxf.assign(nx + 3, 0.);
+  m.hxxc.assign(nx + 3, 0.);
+  m.hyxf.assign(nx + 3, 0.);
+  m.hyxc.assign(nx + 3, 0.);
+  m.jdxf.assign(nx + 3, 0.);
+  m.jdxc.assign(nx + 3, 0.);
+  for (int i = 1; i <= nx + 1; i++) {
+    m.hxxf[i] = d->hxxf[i - 1];
+    m.hyxf[i] = d->hyxf[i - 1];
+    m.jdxf[i] = d->jdxf[i - 1];
+  }
+  for (int i = 0; i <= nx + 1; i++) {
+    m.hxxc[i] = d->hxxc[i];
+    m.hyxc[i] = d->hyxc[i];
+    m.jdxc[i] = d->jdxc[i];
+  }
+}
+
+static int resolve_coefs(Ctx & c) {
+  if (g_params.coef_dt_adv >= 0.) c.coef_adv = g_params.coef_dt_adv;
+  else if (env_double("coef_dt_adv", &c.coef_adv)) return 1;
+  if (g_params.coef_dt_dif >= 0.) c.coef_dif = g_params.coef_dt_dif;
+  else if (env_double("coef_dt_dif", &c.coef_dif)) return 1;
+  return 0;
+}
+
+// diffusivities and the diffusive dt limits (src/decide_dt.c:89-115)
+static int set_physics(Ctx & c, const fluid_t * fl, const domain_t * d) {
+  if (c.Re == fl->Re && c.Pr == fl->Pr && c.nu != 0.) return 0;
+  c.Re = fl->Re;
+  c.Pr = fl->Pr;
+  c.nu = 1. / fl->Re;                      // compute_diffusivity.c
+  c.kappa = 1. / fl->Re / fl->Pr;
+  const double diffusivity = fmax(c.nu, c.kappa);
+  double gs[3];
+  gs[0] = 1.7976931348623157e308;
+  for (int i = 0; i <= c.nx + 1; i++) gs[0] = fmin(gs[0], d->hxxc[i]);
+  gs[1] = d->hyxc[1];
+  gs[2] = d->hz;
+  for (int dim = 0; dim < 3; dim++) {
+    const double v = c.coef_dif / diffusivity * 0.5 / 3 * pow(gs[dim], 2.);
+    c.caps_h[dim] = c.bc.implicit[dim] ? 0. : v;
+  }
+  CK(cudaMemcpy(c.dt_caps, c.caps_h, sizeof(c.caps_h), cudaMemcpyHostToDevice));
+  if (c.step_graph) {
+    cudaGraphExecDestroy(c.step_graph);
+    c.step_graph = nullptr;
+  }
+  return 0;
+}
+
+static int build_tables(Ctx & c, const domain_t * d) {
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  const size_t L = (size_t)nx + 2;
+  Metric m;
+  read_metric(d, nx, m);
+  const double hz = d->hz;
+  auto HXXF = [&](int i) { return m.hxxf[i]; };
+  auto HXXC = [&](int i) { return m.hxxc[i]; };
+  auto HYXF = [&](int i) { return m.hyxf[i]; };
+  auto HYXC = [&](int i) { return m.hyxc[i]; };
+  auto JDXF = [&](int i) { return m.jdxf[i]; };
+  auto JDXC = [&](int i) { return m.jdxc[i]; };
+  std::vector<double> T((size_t)NCOEF_ARRAYS * L, 0.);
+  auto col = [&](int n) { return T.data() + (size_t)n * L; };
+  enum { F_INVJD, F_A1, F_A2, F_A3, F_B1, F_B2, F_C1, F_C2, F_HD1, F_HD2, F_LXL, F_LXC, F_LXU, F_LYL, F_LYC, F_LYU,
+         F_E1, F_E2, C_LYX1F, C_WM, C_WP, C_INVHXXF, C_INVHYXC, C_INVHYXF, C_LYY1, C_INVJDXC, C_A1, C_A2, C_B, C_CZ,
+         C_HD, C_LXL, C_LXC, C_LXU, C_LYL, C_LYC, C_LYU, C_JF, C_E1, C_E2, C_HDA1, C_HDA2, C_PXL, C_PXU, C_PYL, C_PZL,
+         NCOL };
+  static_assert(NCOL == NCOEF_ARRAYS, "coefficient table count");
+  for (int i = 2; i <= nx; i++) {   // ux at face i (ux.c)
+    col(F_INVJD)[i] = 1. / JDXF(i);
+    col(F_A1)[i] = 0.5 * JDXF(i - 1) / HXXF(i - 1);
+    col(F_A2)[i] = 0.5 * JDXF(i) / HXXF(i);
+    col(F_A3)[i] = 0.5 * JDXF(i + 1) / HXXF(i + 1);
+    col(F_B1)[i] = 0.5 * JDXC(i - 1) / HYXC(i - 1);
+    col(F_B2)[i] = 0.5 * JDXC(i) / HYXC(i);
+    col(F_C1)[i] = 0.5 * JDXC(i - 1) / hz;
+    col(F_C2)[i] = 0.5 * JDXC(i) / hz;
+    const double djdhx_xm = -JDXF(i - 1) / HXXF(i - 1) + JDXF(i) / HXXF(i);
+    const double djdhx_xp = -JDXF(i) / HXXF(i) + JDXF(i + 1) / HXXF(i + 1);
+    col(F_HD1)[i] = 0.5 * djdhx_xm;
+    col(F_HD2)[i] = 0.5 * djdhx_xp;
+    const double l = 1. / JDXF(i) * JDXC(i - 1) / HXXC(i - 1) / HXXC(i - 1);   // ux.c:38-43
+    const double u = 1. / JDXF(i) * JDXC(i) / HXXC(i) / HXXC(i);
+    col(F_LXL)[i] = l;
+    col(F_LXC)[i] = -l - u;
+    col(F_LXU)[i] = u;
+    const double ly = 1. / HYXF(i) / HYXF(i);                                 // ux.c:52-54
+    col(F_LYL)[i] = ly;
+    col(F_LYC)[i] = -ly - ly;
+    col(F_LYU)[i] = ly;
+    col(F_E1)[i] = JDXF(i) / HYXF(i);
+    col(F_E2)[i] = JDXF(i) / hz;
+  }
+  for (int i = 1; i <= nx + 1; i++) {  // face quantities
+    const double djdhx = -JDXC(i - 1) / HXXC(i - 1) + JDXC(i) / HXXC(i);
+    col(C_LYX1F)[i] = -1. / JDXF(i) * djdhx;                                  // lyx.c:79-82
+    col(C_WM)[i] = (i == 1) ? 0. : 0.5;
+    col(C_WP)[i] = (i == nx + 1) ? 0. : 0.5;
+    col(C_INVHXXF)[i] = 1. / HXXF(i);
+    col(C_INVHYXF)[i] = 1. / HYXF(i);
+    col(C_JF)[i] = JDXF(i) / HXXF(i);
+  }
+  for (int i = 1; i <= nx; i++) {      // cell-centred variables at i
+    col(C_INVHYXC)[i] = 1. / HYXC(i);
+    const double djdhx = -JDXF(i) / HXXF(i) + JDXF(i + 1) / HXXF(i + 1);
+    col(C_LYY1)[i] = 1. / JDXC(i) * djdhx;                                    // lyy.c:79-82
+    col(C_INVJDXC)[i] = 1. / JDXC(i);
+    col(C_A1)[i] = 0.5 * JDXF(i) / HXXF(i);
+    col(C_A2)[i] = 0.5 * JDXF(i + 1) / HXXF(i + 1);
+    col(C_B)[i] = 0.5 * JDXC(i) / HYXC(i);
+    col(C_CZ)[i] = 0.5 * JDXC(i) / hz;
+    col(C_HD)[i] = 0.5 * djdhx;
+    const double l = 1. / JDXC(i) * JDXF(i) / HXXF(i) / HXXF(i);              // uy.c:38-43
+    const double u = 1. / JDXC(i) * JDXF(i + 1) / HXXF(i + 1) / HXXF(i + 1);
+    col(C_LXL)[i] = l;
+    col(C_LXC)[i] = -l - u;
+    col(C_LXU)[i] = u;
+    const double ly = 1. / HYXC(i) / HYXC(i);
+    col(C_LYL)[i] = ly;
+    col(C_LYC)[i] = -ly - ly;
+    col(C_LYU)[i] = ly;
+    col(C_E1)[i] = JDXC(i) / HYXC(i);
+    col(C_E2)[i] = JDXC(i) / hz;
+    const double dm = -JDXC(i - 1) / HXXC(i - 1) + JDXC(i) / HXXC(i);
+    const double dp = -JDXC(i) / HXXC(i) + JDXC(i + 1) / HXXC(i + 1);
+    col(C_HDA1)[i] = 0.5 * dm;
+    col(C_HDA2)[i] = 0.5 * dp;
+    col(C_PXL)[i] = JDXF(i) / HXXF(i) / HXXF(i);
+    col(C_PXU)[i] = JDXF(i + 1) / HXXF(i + 1) / HXXF(i + 1);
+    col(C_PYL)[i] = JDXC(i) / HYXC(i) / HYXC(i);
+    col(C_PZL)[i] = JDXC(i) / hz / hz;
+  }
+  double * dT = dalloc(c, T.size());
+  if (!dT) return fail("cudaMalloc of coefficient tables failed");
+  CK(cudaMemcpy(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const double * cols[NCOL];
+  for (int n = 0; n < NCOL; n++) cols[n] = dT + (size_t)n * L;
+  Coefs & cf = c.cf;
+  const double ** dst[NCOL] = {&cf.f_invjd, &cf.f_a1, &cf.f_a2, &cf.f_a3, &cf.f_b1, &cf.f_b2, &cf.f_c1, &cf.f_c2,
+      &cf.f_hd1, &cf.f_hd2, &cf.f_lxl, &cf.f_lxc, &cf.f_lxu, &cf.f_lyl, &cf.f_lyc, &cf.f_lyu, &cf.f_e1, &cf.f_e2,
+      &cf.c_lyx1f, &cf.c_wm, &cf.c_wp, &cf.c_invhxxf, &cf.c_invhyxc, &cf.c_invhyxf, &cf.c_lyy1, &cf.c_invjdxc,
+      &cf.c_a1, &cf.c_a2, &cf.c_b, &cf.c_cz, &cf.c_hd, &cf.c_lxl, &cf.c_lxc, &cf.c_lxu, &cf.c_lyl, &cf.c_lyc,
+      &cf.c_lyu, &cf.c_jf, &cf.c_e1, &cf.c_e2, &cf.c_hda1, &cf.c_hda2, &cf.c_pxl, &cf.c_pxu, &cf.c_pyl, &cf.c_pzl};
+  for (int n = 0; n < NCOL; n++) *dst[n] = cols[n];
+  const double lz = 1. / hz / hz;
+  cf.lz_l = lz;
+  cf.lz_c = -lz - lz;
+  cf.lz_u = lz;
+  cf.inv_hz = 1. / hz;
+
+  // geometry tables
+  std::vector<double> G(6 * L, 0.);
+  for (int i = 0; i <= nx + 1; i++) {
+    G[0 * L + i] = m.hxxf[i];
+    G[1 * L + i] = m.hxxc[i];
+    G[2 * L + i] = m.hyxf[i];
+    G[3 * L + i] = m.hyxc[i];
+    G[4 * L + i] = m.jdxf[i];
+    G[5 * L + i] = m.jdxc[i];
+  }
+  double * dG = dalloc(c, G.size());
+  if (!dG) return fail("cudaMalloc failed");
+  CK(cudaMemcpy(dG, G.data(), G.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c.g.nx = nx;
+  c.g.ny = ny;
+  c.g.nz = nz;
+  c.g.hz = hz;
+  c.g.hxxf = dG;
+  c.g.hxxc = dG + L;
+  c.g.hyxf = dG + 2 * L;
+  c.g.hyxc = dG + 3 * L;
+  c.g.jdxf = dG + 4 * L;
+  c.g.jdxc = dG + 5 * L;
+
+  // packed per-variable Laplacians for the implicit solves
+  std::vector<double> P((size_t)4 * 6 * L, 0.);  // [var][lx l c u, ly l c u][L]
+  for (int v = 0; v < 4; v++) {
+    const int i0 = (v == VUX) ? 2 : 1;
+    const int n = nx - i0 + 1;
+    for (int e = 0; e < n; e++) {
+      const int i = e + i0;
+      double * b = P.data() + (size_t)v * 6 * L;
+      if (v == VUX) {
+        b[0 * L + e] = col(F_LXL)[i]; b[1 * L + e] = col(F_LXC)[i]; b[2 * L + e] = col(F_LXU)[i];
+        b[3 * L + e] = col(F_LYL)[i]; b[4 * L + e] = col(F_LYC)[i]; b[5 * L + e] = col(F_LYU)[i];
+      } else {
+        b[0 * L + e] = col(C_LXL)[i]; b[1 * L + e] = col(C_LXC)[i]; b[2 * L + e] = col(C_LXU)[i];
+        b[3 * L + e] = col(C_LYL)[i]; b[4 * L + e] = col(C_LYC)[i]; b[5 * L + e] = col(C_LYU)[i];
+      }
+    }
+  }
+  double * dP = dalloc(c, P.size());
+  if (!dP) return fail("cudaMalloc failed");
+  CK(cudaMemcpy(dP, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c.xf.stride = L;
+  for (int v = 0; v < 4; v++) {
+    c.xf.n[v] = (v == VUX) ? nx - 1 : nx;
+    c.xf.lap_l[v] = dP + (size_t)v * 6 * L;
+    c.xf.lap_c[v] = dP + (size_t)v * 6 * L + L;
+    c.xf.lap_u[v] = dP + (size_t)v * 6 * L + 2 * L;
+  }
+  c.xf.lo = dalloc(c, 12 * L);
+  c.xf.w = dalloc(c, 12 * L);
+  c.xf.v = dalloc(c, 12 * L);
+  if (c.bc.implicit[1] || c.bc.implicit[2]) {
+    YZFactors & yf = c.yf;
+    yf.max_i = nx;
+    yf.stride_y = (size_t)nx * ny;
+    yf.stride_z = (size_t)nz;
+    for (int v = 0; v < 4; v++) {
+      yf.n_i[v] = (v == VUX) ? nx - 1 : nx;
+      yf.lapy_l[v] = dP + (size_t)v * 6 * L + 3 * L;
+      yf.lapy_c[v] = dP + (size_t)v * 6 * L + 4 * L;
+      yf.lapy_u[v] = dP + (size_t)v * 6 * L + 5 * L;
+    }
+    yf.lapz_l = cf.lz_l;
+    yf.lapz_c = cf.lz_c;
+    yf.lapz_u = cf.lz_u;
+    yf.l = dalloc(c, 12 * (size_t)nx);
+    yf.c = dalloc(c, 12 * (size_t)nx);
+    yf.u = dalloc(c, 12 * (size_t)nx);
+    yf.v = dalloc(c, 12 * yf.stride_y);
+    yf.w = dalloc(c, 12 * yf.stride_y);
+    yf.q1 = dalloc(c, 12 * yf.stride_y);
+    yf.lz = dalloc(c, 12);
+    yf.cz = dalloc(c, 12);
+    yf.uz = dalloc(c, 12);
+    yf.vz = dalloc(c, 12 * (size_t)nz);
+    yf.wz = dalloc(c, 12 * (size_t)nz);
+    yf.q1z = dalloc(c, 12 * (size_t)nz);
+  }
+
+  // Poisson tables (compute_potential.c:173-211, 311-349)
+  const int nyh = ny / 2 + 1;
+  c.ps.nyh = nyh;
+  std::vector<double> tl(nx), tu(nx), base(nx), tz(nz), ty((size_t)nx * nyh);
+  for (int i = 1; i <= nx; i++) {
+    tl[i - 1] = 1. / JDXC(i) * JDXF(i) / HXXF(i) / HXXF(i);
+    tu[i - 1] = 1. / JDXC(i) * JDXF(i + 1) / HXXF(i + 1) / HXXF(i + 1);
+    base[i - 1] = -tl[i - 1] - tu[i - 1];
+  }
+  const double g_pi = 3.14159265358979324;
+  std::vector<double> ey(nyh), ez(nz);
+  for (int n = 0; n < nyh; n++) {
+    const double s = sin(g_pi * n / ny);
+    ey[n] = -4. * (s * s);
+  }
+  for (int n = 0; n < nz; n++) {
+    const double s = sin(g_pi * n / nz);
+    ez[n] = -4. * (s * s);
+    tz[n] = ez[n] / hz / hz;
+  }
+  for (int i = 1; i <= nx; i++)
+    for (int n = 0; n < nyh; n++) ty[(size_t)(i - 1) * nyh + n] = ey[n] / HYXC(i) / HYXC(i);
+  double * dtl = dalloc(c, nx);
+  double * dtu = dalloc(c, nx);
+  c.base = dalloc(c, nx);
+  c.tab_z = dalloc(c, nz);
+  c.tab_y = dalloc(c, (size_t)nx * nyh);
+  if (!dtl || !dtu || !c.base || !c.tab_z || !c.tab_y) return fail("cudaMalloc failed");
+  CK(cudaMemcpy(dtl, tl.data(), nx * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dtu, tu.data(), nx * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c.base, base.data(), nx * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c.tab_z, tz.data(), nz * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c.tab_y, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice));
+  c.ps.tl = dtl;
+  c.ps.tu = dtu;
+  // twiddles exp(-2 pi i m / N), m < N/2, from libm
+  auto twiddles = [&](int N) -> double2 * {
+    std::vector<double> tw(N);  // N/2 complex
+    for (int k = 0; k < N / 2; k++) {
+      const double a = 2. * g_pi * k / N;
+      tw[2 * k] = cos(a);
+      tw[2 * k + 1] = -sin(a);
+    }
+    double * p = dalloc(c, N);
+    if (p) cudaMemcpy(p, tw.data(), N * sizeof(double), cudaMemcpyHostToDevice);
+    return reinterpret_cast<double2 *>(p);
+  };
+  c.ps.tw_y = twiddles(ny);
+  c.ps.tw_z = twiddles(nz);
+  const size_t nspec = (size_t)nx * nz * nyh;
+  c.ps.spec = reinterpret_cast<double2 *>(dalloc(c, 2 * nspec));
+  c.ps.vscr = dalloc(c, nspec);
+  if (!c.ps.tw_y || !c.ps.tw_z || !c.ps.spec || !c.ps.vscr) return fail("cudaMalloc of Poisson buffers failed");
+  return 0;
+}
+
+static int check_domain(const domain_t * d) {
+  if (d == nullptr) return fail("domain is NULL");
+  for (int dim = 0; dim < 3; dim++) {
+    if (d->mysizes[dim] != d->glsizes[dim] || d->offsets[dim] != 0)
+      return fail("only a single rank owning the whole domain is supported (dim %d: mysize %zu, glsize %zu, offset %zu)",
+                  dim, d->mysizes[dim], d->glsizes[dim], d->offsets[dim]);
+  }
+  const size_t nx = d->glsizes[0], ny = d->glsizes[1], nz = d->glsizes[2];
+  if (nx < 2 || nx > 512) return fail("nx = %zu outside the supported range [2, 512]", nx);
+  if (!is_pow2(ny) || !is_pow2(nz) || ny > 2048 || nz > 2048)
+    return fail("ny = %zu and nz = %zu must be powers of two in [4, 2048]", ny, nz);
+  if (!d->hxxf || !d->hxxc || !d->hyxf || !d->hyxc || !d->jdxf || !d->jdxc)
+    return fail("domain metric arrays are not initialised");
+  return 0;
+}
+
+static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
+  if (check_domain(d)) return nullptr;
+  Ctx * c = new Ctx();
+  c->key = fl;
+  c->nx = (int)d->glsizes[0];
+  c->ny = (int)d->glsizes[1];
+  c->nz = (int)d->glsizes[2];
+  c->nc = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  c->nf = (size_t)(c->nx + 1) * (c->ny + 2) * (c->nz + 2);
+  c->bc.uy_xm = g_params.uy_xm;
+  c->bc.uy_xp = g_params.uy_xp;
+  c->bc.t_xm = g_params.t_xm;
+  c->bc.t_xp = g_params.t_xp;
+  c->bc.implicit[0] = g_params.implicit_x ? 1 : 0;
+  c->bc.implicit[1] = g_params.implicit_y ? 1 : 0;
+  c->bc.implicit[2] = g_params.implicit_z ? 1 : 0;
+  auto bad = [&](const char * what) { fail("%s", what); destroy_ctx(c); return (Ctx *)nullptr; };
+  if (resolve_coefs(*c)) { destroy_ctx(c); return nullptr; }
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return bad("cudaStreamCreate failed");
+  c->f.ux = dalloc(*c, c->nf);
+  c->f.uy = dalloc(*c, c->nc);
+  c->f.uz = dalloc(*c, c->nc);
+  c->f.p = dalloc(*c, c->nc);
+  c->f.psi = dalloc(*c, c->nc);
+  c->f.t = dalloc(*c, c->nc);
+  if (!c->f.ux || !c->f.uy || !c->f.uz || !c->f.p || !c->f.psi || !c->f.t) return bad("cudaMalloc of fields failed");
+  const size_t nin = (size_t)c->nx * c->ny * c->nz;
+  for (int v = 0; v < 4; v++) {
+    const size_t n = (v == VUX) ? (size_t)(c->nx - 1) * c->ny * c->nz : nin;
+    c->src[v][0] = dalloc(*c, n);
+    c->src[v][1] = dalloc(*c, n);
+    c->delta[v] = dalloc(*c, n);
+    if (!c->src[v][0] || !c->src[v][1] || !c->delta[v]) return bad("cudaMalloc of source terms failed");
+  }
+  c->dt_caps = dalloc(*c, 3);
+  c->dtp = dalloc(*c, 1);
+  c->dtmin = reinterpret_cast<unsigned long long *>(dalloc(*c, 1));
+  c->status = reinterpret_cast<unsigned *>(dalloc(*c, 1));
+  c->diag_out = dalloc(*c, 16);
+  c->diag_part = dalloc(*c, (size_t)DIAG_BLOCKS_MAX * 9);
+  if (!c->dt_caps || !c->dtp || !c->dtmin || !c->status || !c->diag_out || !c->diag_part) return bad("cudaMalloc failed");
+  const unsigned long long one = 0x3ff0000000000000ull;
+  if (cudaMemcpy(c->dtmin, &one, sizeof(one), cudaMemcpyHostToDevice) != cudaSuccess) return bad("cudaMemcpy failed");
+  if (cudaMallocHost(&c->h_scalar, 64 * sizeof(double)) != cudaSuccess) return bad("cudaMallocHost failed");
+  if (cudaMallocHost(&c->h_status, sizeof(unsigned) * 4) != cudaSuccess) return bad("cudaMallocHost failed");
+  if (build_tables(*c, d)) { destroy_ctx(c); return nullptr; }
+  poisson_smem_limits();
+  c->nu = 0.;
+  if (set_physics(*c, fl, d)) { destroy_ctx(c); return nullptr; }
+  return c;
+}
+
+static Ctx * get_ctx(const domain_t * d, const fluid_t * fl) {
+  if (fl == nullptr) { fail("fluid is NULL"); return nullptr; }
+  std::lock_guard<std::mutex> lk(g_mutex);
+  auto it = g_ctx.find(fl);
+  if (it != g_ctx.end()) {
+    Ctx * c = it->second;
+    if (d != nullptr && (c->nx != (int)d->glsizes[0] || c->ny != (int)d->glsizes[1] || c->nz != (int)d->glsizes[2])) {
+      destroy_ctx(c);
+      g_ctx.erase(it);
+    } else {
+      if (d != nullptr && set_physics(*c, fl, d)) return nullptr;
+      return c;
+    }
+  }
+  if (d == nullptr) { fail("no device state for this fluid yet"); return nullptr; }
+  Ctx * c = create_ctx(d, fl);
+  if (c) g_ctx[fl] = c;
+  return c;
+}
+
+// ------------------------------------------------------------------ schedule
+static double * s_new(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 1 : 0]; }
+static double * s_old(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 0 : 1]; }
+
+static void enqueue_factors(Ctx & c) {
+  if (c.bc.implicit[0]) launch_xfactors(c.xf, c.dtp, c.nu, c.kappa, c.st);
+  if (c.bc.implicit[1] || c.bc.implicit[2]) launch_yzfactors(c.g, c.yf, c.dtp, c.nu, c.kappa, c.st);
+}
+
+static void enqueue_predict(Ctx & c, int rk) {
+  double * sn[4], * so[4];
+  for (int v = 0; v < 4; v++) {
+    sn[v] = s_new(c, v, rk);
+    so[v] = s_old(c, v, rk);
+  }
+  launch_rhs_delta(c.g, c.bc, c.cf, c.nu, c.kappa, c.f, so, sn, c.delta, c.dtp, rk, c.st);
+  const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
+  if (!iy && !iz) {
+    launch_xsolve(c.g, c.bc, c.xf, rk, c.bc.implicit[0] ? XS_SOLVE_APPLY : XS_APPLY, c.f, c.delta, c.st);
+    return;
+  }
+  if (c.bc.implicit[0]) launch_xsolve(c.g, c.bc, c.xf, rk, XS_SOLVE, c.f, c.delta, c.st);
+  if (iy) launch_ysolve(c.g, c.yf, rk, c.delta, c.st);
+  if (iz) launch_zsolve(c.g, c.yf, rk, c.delta, c.st);
+  launch_xsolve(c.g, c.bc, c.xf, rk, XS_APPLY, c.f, c.delta, c.st);
+}
+
+static void enqueue_potential(Ctx & c, int rk) {
+  launch_poisson(c.g, c.cf, c.ps, c.f, c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st);
+}
+
+static void enqueue_correct(Ctx & c, int rk, int what) {
+  launch_correct(c.g, c.bc, c.cf, c.f, c.dtp, rk, c.nu, what, c.st);
+}
+
+static void enqueue_step(Ctx & c) {
+  launch_decide_dt(c.g, c.f, c.coef_adv, c.dt_caps, c.dtmin, c.dtp, c.status, c.st);
+  enqueue_factors(c);
+  for (int rk = 0; rk < 3; rk++) {
+    enqueue_predict(c, rk);
+    enqueue_potential(c, rk);
+    enqueue_correct(c, rk, CORRECT_VELOCITY | CORRECT_PRESSURE);
+  }
+}
+
+static int launch_step(Ctx & c) {
+  if (c.step_graph == nullptr) {
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(c);
+    CK(cudaStreamEndCapture(c.st, &graph));
+    cudaError_t e = cudaGraphInstantiate(&c.step_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail("cudaGraphInstantiate failed: %s", cudaGetErrorString(e));
+  }
+  CK(cudaGraphLaunch(c.step_graph, c.st));
+  return 0;
+}
+
+// set the device dt from a host value (stage-by-stage entry points)
+static int set_dt(Ctx & c, double dt) {
+  *c.h_scalar = dt;
+  CK(cudaMemcpyAsync(c.dtp, c.h_scalar, sizeof(double), cudaMemcpyHostToDevice, c.st));
+  return 0;
+}
+
+static int finish(Ctx & c, const char * what) {
+  CK(cudaMemcpyAsync(c.h_status, c.status, sizeof(unsigned), cudaMemcpyDeviceToHost, c.st));
+  cudaError_t e = cudaStreamSynchronize(c.st);
+  if (e != cudaSuccess) return fail("%s: %s", what, cudaGetErrorString(e));
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail("%s: %s", what, cudaGetErrorString(e));
+  if (*c.h_status) {
+    const unsigned s = *c.h_status;
+    cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.st);
+    cudaStreamSynchronize(c.st);
+    if (s & ST_NONFINITE) return fail("%s: non-finite velocity in the field", what);
+    if (s & ST_BADDT) return fail("%s: invalid time step size", what);
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------ coherence
+static size_t field_count(const Ctx & c, unsigned bit) { return bit == TCGPU_UX ? c.nf : c.nc; }
+
+static double * dev_field(Ctx & c, unsigned bit) {
+  switch (bit) {
+    case TCGPU_UX: return c.f.ux;
+    case TCGPU_UY: return c.f.uy;
+    case TCGPU_UZ: return c.f.uz;
+    case TCGPU_P: return c.f.p;
+    case TCGPU_PSI: return c.f.psi;
+    default: return c.f.t;
+  }
+}
+
+static const array_t * host_field(const fluid_t * fl, unsigned bit) {
+  switch (bit) {
+    case TCGPU_UX: return &fl->ux;
+    case TCGPU_UY: return &fl->uy;
+    case TCGPU_UZ: return &fl->uz;
+    case TCGPU_P: return &fl->p;
+    case TCGPU_PSI: return &fl->psi;
+    default: return &fl->t;
+  }
+}
+
+static int check_host_array(const Ctx & c, const array_t * a, size_t n, const char * name) {
+  if (a->data == nullptr) return fail("%s: host array is NULL", name);
+  if (a->datasize != 0 && a->datasize != n * sizeof(double))
+    return fail("%s: host array holds %zu bytes, %zu expected", name, a->datasize, n * sizeof(double));
+  (void)c;
+  return 0;
+}
+
+static const char * field_name(unsigned bit) {
+  switch (bit) {
+    case TCGPU_UX: return "ux";
+    case TCGPU_UY: return "uy";
+    case TCGPU_UZ: return "uz";
+    case TCGPU_P: return "p";
+    case TCGPU_PSI: return "psi";
+    default: return "t";
+  }
+}
+
+static int push_fields(Ctx & c, const fluid_t * fl, unsigned mask) {
+  for (unsigned bit = 1; bit <= TCGPU_T; bit <<= 1) {
+    if (!(mask & bit)) continue;
+    const array_t * a = host_field(fl, bit);
+    const size_t n = field_count(c, bit);
+    if (check_host_array(c, a, n, field_name(bit))) return 1;
+    CK(cudaMemcpyAsync(dev_field(c, bit), a->data, n * sizeof(double), cudaMemcpyHostToDevice, c.st));
+  }
+  return 0;
+}
+
+static int pull_fields(Ctx & c, fluid_t * fl, unsigned mask) {
+  for (unsigned bit = 1; bit <= TCGPU_T; bit <<= 1) {
+    if (!(mask & bit)) continue;
+    const array_t * a = host_field(fl, bit);
+    const size_t n = field_count(c, bit);
+    if (check_host_array(c, a, n, field_name(bit))) return 1;
+    CK(cudaMemcpyAsync(a->data, dev_field(c, bit), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  }
+  return 0;
+}
+
+static int ensure_tensors(Ctx & c) {
+  if (c.have_tn) return 0;
+  const size_t nface = (size_t)(c.nx + 1) * (c.ny + 2) * (c.nz + 2);
+  const size_t ncent = (size_t)c.nx * (c.ny + 2) * (c.nz + 2);
+  const bool face[11] = {false, true, true, true, true, false, false, false, true, false, false};
+  for (int s = 0; s < 11; s++) {
+    c.tn.a[s] = dalloc(c, face[s] ? nface : ncent);
+    if (!c.tn.a[s]) return fail("cudaMalloc of tensors failed");
+  }
+  c.have_tn = true;
+  return 0;
+}
+
+static int pull_tensors(Ctx & c, fluid_t * fl) {
+  if (ensure_tensors(c)) return 1;
+  launch_tensors(c.g, c.cf, c.f, c.tn, c.st);
+  const size_t nface = (size_t)(c.nx + 1) * (c.ny + 2) * (c.nz + 2);
+  const size_t ncent = (size_t)c.nx * (c.ny + 2) * (c.nz + 2);
+  array_t * dst[11] = {&fl->lxx, &fl->lxy, &fl->lxz, &fl->lyx0, &fl->lyx1, &fl->lyy0, &fl->lyy1, &fl->lyz,
+                       &fl->lzx, &fl->lzy, &fl->lzz};
+  const bool face[11] = {false, true, true, true, true, false, false, false, true, false, false};
+  for (int s = 0; s < 11; s++) {
+    if (dst[s]->data == nullptr) continue;
+    CK(cudaMemcpyAsync(dst[s]->data, c.tn.a[s], (face[s] ? nface : ncent) * sizeof(double),
+                       cudaMemcpyDeviceToHost, c.st));
+  }
+  return 0;
+}
+
+// reset_srcs (predict/main.c:8-25): the reference swaps the alpha and beta
+// buffers of the caller's fluid_t; the same swap is mirrored there, and with
+// TCGPU_SYNC_SRCS the device terms are copied into them.
+static int mirror_srcs(Ctx & c, fluid_t * fl, int rk) {
+  array_t * arrs[4] = {fl->srcux, fl->srcuy, fl->srcuz, fl->srct};
+  for (int v = 0; v < 4; v++) {
+    void * tmp = arrs[v][0].data;
+    arrs[v][0].data = arrs[v][1].data;
+    arrs[v][1].data = tmp;
+  }
+  if (!(c.coherence & TCGPU_SYNC_SRCS)) return 0;
+  for (int v = 0; v < 4; v++) {
+    const size_t n = (v == VUX) ? (size_t)(c.nx - 1) * c.ny * c.nz : (size_t)c.nx * c.ny * c.nz;
+    if (arrs[v][0].data) CK(cudaMemcpyAsync(arrs[v][0].data, s_new(c, v, rk), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    if (arrs[v][1].data && rk != 0)
+      CK(cudaMemcpyAsync(arrs[v][1].data, s_old(c, v, rk), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  }
+  return 0;
+}
+
+static bool coherent(const Ctx & c) { return !(c.coherence & TCGPU_NO_COHERENCE); }
+
+static int apply_bcs(Ctx & c, unsigned mask) {
+  const BcKind kinds[6] = {BC_UX, BC_UY, BC_UZ, BC_P, BC_PSI, BC_T};
+  for (int s = 0; s < 6; s++) {
+    const unsigned bit = 1u << s;
+    if (mask & bit) launch_bc(c.g, c.bc, kinds[s], dev_field(c, bit), c.st);
+  }
+  return 0;
+}
+
+// ------------------------------------------------------------------ exported API
+extern "C" {
+
+const uint_fast8_t rk_a = 0;
+const uint_fast8_t rk_b = 1;
+const uint_fast8_t rk_g = 2;
+const rkcoef_t rkcoefs[3] = {
+    {32. / 60., 0. / 60., 32. / 60. + 0. / 60.},
+    {25. / 60., -17. / 60., 25. / 60. + -17. / 60.},
+    {45. / 60., -25. / 60., 45. / 60. + -25. / 60.},
+};
+
+const char * tcgpu_last_error(void) { return g_last_error.c_str(); }
+
+int tcgpu_set_params(const tcgpu_params_t * params) {
+  if (params == nullptr) return fail("params is NULL");
+  std::lock_guard<std::mutex> lk(g_mutex);
+  g_params = *params;
+  return 0;
+}
+
+int tcgpu_get_params(tcgpu_params_t * params) {
+  if (params == nullptr) return fail("params is NULL");
+  *params = g_params;
+  return 0;
+}
+
+int tcgpu_set_coherence(const domain_t * domain, fluid_t * fluid, unsigned flags) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  c->coherence = flags;
+  if ((flags & TCGPU_PIN_HOST) && c->pinned.empty()) {
+    for (unsigned bit = 1; bit <= TCGPU_T; bit <<= 1) {
+      const array_t * a = host_field(fluid, bit);
+      if (a->data == nullptr) continue;
+      const size_t n = field_count(*c, bit) * sizeof(double);
+      if (cudaHostRegister(a->data, n, cudaHostRegisterDefault) == cudaSuccess) c->pinned.push_back(a->data);
+      else cudaGetLastError();
+    }
+  }
+  return 0;
+}
+
+int tcgpu_push(const domain_t * domain, fluid_t * fluid, unsigned fields) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (push_fields(*c, fluid, fields & TCGPU_FIELDS)) return 1;
+  apply_bcs(*c, fields & TCGPU_FIELDS);
+  return finish(*c, "tcgpu_push");
+}
+
+int tcgpu_pull(const domain_t * domain, fluid_t * fluid, unsigned fields) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (pull_fields(*c, fluid, fields & TCGPU_FIELDS)) return 1;
+  if ((fields & TCGPU_TENSORS) && pull_tensors(*c, fluid)) return 1;
+  return finish(*c, "tcgpu_pull");
+}
+
+int tcgpu_run(const domain_t * domain, fluid_t * fluid, int nsteps, double * dts) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (nsteps > 64 && dts != nullptr) {
+    for (int s0 = 0; s0 < nsteps; s0 += 64) {
+      const int n = nsteps - s0 < 64 ? nsteps - s0 : 64;
+      if (tcgpu_run(domain, fluid, n, dts + s0)) return 1;
+    }
+    return 0;
+  }
+  for (int s = 0; s < nsteps; s++) {
+    if (launch_step(*c)) return 1;
+    if (dts) CK(cudaMemcpyAsync(c->h_scalar + s, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  }
+  if (finish(*c, "tcgpu_run")) return 1;
+  if (dts) memcpy(dts, c->h_scalar, sizeof(double) * nsteps);
+  return 0;
+}
+
+int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  launch_diagnostics(c->g, c->cf, c->bc, c->f, c->nu, c->kappa, c->diag_out, c->diag_part, c->st);
+  CK(cudaMemcpyAsync(c->h_scalar, c->diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (finish(*c, "tcgpu_diagnostics")) return 1;
+  memcpy(out, c->h_scalar, 9 * sizeof(double));
+  return 0;
+}
+
+int tcgpu_release(fluid_t * fluid) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  auto it = g_ctx.find(fluid);
+  if (it == g_ctx.end()) return 0;
+  destroy_ctx(it->second);
+  g_ctx.erase(it);
+  return 0;
+}
+
+double fluid_compute_momentum_diffusivity(const fluid_t * fluid) { return 1. / fluid->Re; }
+double fluid_compute_scalar_diffusivity(const fluid_t * fluid) { return 1. / fluid->Re / fluid->Pr; }
+
+int decide_dt(const domain_t * domain, const fluid_t * fluid, double * dt) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
+  launch_decide_dt(c->g, c->f, c->coef_adv, c->dt_caps, c->dtmin, c->dtp, c->status, c->st);
+  CK(cudaMemcpyAsync(c->h_scalar, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (finish(*c, "decide_dt")) return 1;
+  *dt = *c->h_scalar;
+  return 0;
+}
+
+int fluid_predict_field(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid) {
+  if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  const int rk = (int)rkstep;
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
+  if (set_dt(*c, dt)) return 1;
+  if ((c->coherence & TCGPU_SYNC_TENSORS) && coherent(*c) && pull_tensors(*c, fluid)) return 1;
+  enqueue_factors(*c);
+  enqueue_predict(*c, rk);
+  if (coherent(*c)) {
+    if (pull_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_T)) return 1;
+    if (mirror_srcs(*c, fluid, rk)) return 1;
+  }
+  return finish(*c, "fluid_predict_field");
+}
+
+int fluid_compute_potential(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid) {
+  if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
+  if (set_dt(*c, dt)) return 1;
+  enqueue_potential(*c, (int)rkstep);
+  if (coherent(*c) && pull_fields(*c, fluid, TCGPU_PSI)) return 1;
+  return finish(*c, "fluid_compute_potential");
+}
+
+int fluid_correct_velocity(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid) {
+  if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_PSI)) return 1;
+  if (set_dt(*c, dt)) return 1;
+  enqueue_correct(*c, (int)rkstep, CORRECT_VELOCITY);
+  if (coherent(*c) && pull_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
+  return finish(*c, "fluid_correct_velocity");
+}
+
+int fluid_update_pressure(const domain_t * domain, const size_t rkstep, const double dt, fluid_t * fluid) {
+  if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  // inside integrate() this update runs fused with the velocity correction
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_P | TCGPU_PSI)) return 1;
+  if (set_dt(*c, dt)) return 1;
+  enqueue_correct(*c, (int)rkstep, CORRECT_PRESSURE);
+  if (coherent(*c) && pull_fields(*c, fluid, TCGPU_P)) return 1;
+  return finish(*c, "fluid_update_pressure");
+}
+
+int integrate(const domain_t * domain, fluid_t * fluid, double * dt) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
+  if (launch_step(*c)) return 1;
+  CK(cudaMemcpyAsync(c->h_scalar, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (coherent(*c)) {
+    if (pull_fields(*c, fluid, TCGPU_FIELDS)) return 1;
+    // three predict calls swap the caller's alpha/beta source buffers three times
+    array_t * arrs[4] = {fluid->srcux, fluid->srcuy, fluid->srcuz, fluid->srct};
+    for (int v = 0; v < 4; v++) {
+      void * tmp = arrs[v][0].data;
+      arrs[v][0].data = arrs[v][1].data;
+      arrs[v][1].data = tmp;
+    }
+  }
+  if (finish(*c, "integrate")) return 1;
+  *dt = *c->h_scalar;
+  return 0;
+}
+
+// fluid_update_boundaries_* on a single host array: it travels through a
+// scratch device buffer; no solver context is needed or touched.
+static int bc_entry(const domain_t * domain, array_t * array, BcKind kind, const char * name) {
+  if (check_domain(domain)) return 1;
+  if (array == nullptr || array->data == nullptr) return fail("%s: array is NULL", name);
+  Geo g{};
+  g.nx = (int)domain->glsizes[0];
+  g.ny = (int)domain->glsizes[1];
+  g.nz = (int)domain->glsizes[2];
+  Bc bc{};
+  bc.uy_xm = g_params.uy_xm;
+  bc.uy_xp = g_params.uy_xp;
+  bc.t_xm = g_params.t_xm;
+  bc.t_xp = g_params.t_xp;
+  const size_t n = (kind == BC_UX) ? ncell_f(g) : ncell_c(g);
+  if (array->datasize != 0 && array->datasize != n * sizeof(double))
+    return fail("%s: array holds %zu bytes, %zu expected", name, array->datasize, n * sizeof(double));
+  double * dbuf = nullptr;
+  CK(cudaMalloc(&dbuf, n * sizeof(double)));
+  cudaError_t e = cudaMemcpy(dbuf, array->data, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    launch_bc(g, bc, kind, dbuf, 0);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(array->data, dbuf, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dbuf);
+  if (e != cudaSuccess) return fail("%s: %s", name, cudaGetErrorString(e));
+  return 0;
+}
+
+int fluid_update_boundaries_ux(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_UX, "fluid_update_boundaries_ux"); }
+int fluid_update_boundaries_uy(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_UY, "fluid_update_boundaries_uy"); }
+int fluid_update_boundaries_uz(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_UZ, "fluid_update_boundaries_uz"); }
+int fluid_update_boundaries_p(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_P, "fluid_update_boundaries_p"); }
+int fluid_update_boundaries_psi(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_PSI, "fluid_update_boundaries_psi"); }
+int fluid_update_boundaries_t(const domain_t * d, array_t * a) { return bc_entry(d, a, BC_T, "fluid_update_boundaries_t"); }
+
+}  // extern "C"
+
+extern "C" int tcgpu_report_error(const char * msg) { return fail("%s", msg); }

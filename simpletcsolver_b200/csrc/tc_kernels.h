@@ -1,0 +1,164 @@
+// Kernel-side data structures and launchers of the tcgpu library.
+#pragma once
+
+#include "tc_common.cuh"
+
+namespace tcgpu {
+
+// Device pointers of the state fields (reference layout with halos).
+struct Fields {
+  double * ux;
+  double * uy;
+  double * uz;
+  double * p;
+  double * psi;
+  double * t;
+};
+
+// Per-radial-index coefficient tables (length nx+2, indexed by the reference
+// i), computed on the host once per context with the reference's operand
+// order. f_* belong to ux at face i, c_* to the cell-centred variables at i.
+struct Coefs {
+  const double * f_invjd;  // 1 / JDXF(i)
+  const double * f_a1;     // 0.5 JDXF(i-1) / HXXF(i-1)
+  const double * f_a2;     // 0.5 JDXF(i)   / HXXF(i)
+  const double * f_a3;     // 0.5 JDXF(i+1) / HXXF(i+1)
+  const double * f_b1;     // 0.5 JDXC(i-1) / HYXC(i-1)
+  const double * f_b2;     // 0.5 JDXC(i)   / HYXC(i)
+  const double * f_c1;     // 0.5 JDXC(i-1) / hz
+  const double * f_c2;     // 0.5 JDXC(i)   / hz
+  const double * f_hd1;    // 0.5 (-JDXF(i-1)/HXXF(i-1) + JDXF(i)/HXXF(i))
+  const double * f_hd2;    // 0.5 (-JDXF(i)/HXXF(i) + JDXF(i+1)/HXXF(i+1))
+  const double * f_lxl;    // ux Laplacian in x (ux.c:34-47)
+  const double * f_lxc;
+  const double * f_lxu;
+  const double * f_lyl;    // ux Laplacian in y (ux.c:48-58)
+  const double * f_lyc;
+  const double * f_lyu;
+  const double * f_e1;     // JDXF(i) / HYXF(i)
+  const double * f_e2;     // JDXF(i) / hz
+  const double * c_lyx1f;  // -1/JDXF(i) (-JDXC(i-1)/HXXC(i-1) + JDXC(i)/HXXC(i))   lyx.c:70-83
+  const double * c_wm;     // 0 at i = 1, else 0.5
+  const double * c_wp;     // 0 at i = nx+1, else 0.5
+  const double * c_invhxxf;
+  const double * c_invhyxc;
+  const double * c_invhyxf;
+  const double * c_lyy1;   // 1/JDXC(i) (-JDXF(i)/HXXF(i) + JDXF(i+1)/HXXF(i+1))    lyy.c:70-83
+  const double * c_invjdxc;
+  const double * c_a1;     // 0.5 JDXF(i)   / HXXF(i)
+  const double * c_a2;     // 0.5 JDXF(i+1) / HXXF(i+1)
+  const double * c_b;      // 0.5 JDXC(i) / HYXC(i)
+  const double * c_cz;     // 0.5 JDXC(i) / hz
+  const double * c_hd;     // 0.5 (-JDXF(i)/HXXF(i) + JDXF(i+1)/HXXF(i+1))
+  const double * c_lxl;    // centred Laplacian in x (uy.c:34-47, uz.c, t.c)
+  const double * c_lxc;
+  const double * c_lxu;
+  const double * c_lyl;    // centred Laplacian in y
+  const double * c_lyc;
+  const double * c_lyu;
+  const double * c_jf;     // JDXF(i) / HXXF(i)
+  const double * c_e1;     // JDXC(i) / HYXC(i)
+  const double * c_e2;     // JDXC(i) / hz
+  const double * c_hda1;   // 0.5 (-JDXC(i-1)/HXXC(i-1) + JDXC(i)/HXXC(i))
+  const double * c_hda2;   // 0.5 (-JDXC(i)/HXXC(i) + JDXC(i+1)/HXXC(i+1))
+  const double * c_pxl;    // JDXF(i)/HXXF(i)/HXXF(i)        update_pressure.c:51-56
+  const double * c_pxu;    // JDXF(i+1)/HXXF(i+1)/HXXF(i+1)
+  const double * c_pyl;    // JDXC(i)/HYXC(i)/HYXC(i)        :86-90
+  const double * c_pzl;    // JDXC(i)/hz/hz                  :118-122
+  double lz_l, lz_c, lz_u; // Laplacian in z
+  double inv_hz;
+};
+constexpr int NCOEF_ARRAYS = 46;
+
+// Radial Thomas factors for the three substeps x four variables.
+struct XFactors {
+  int n[4];                 // nx-1 for ux, nx otherwise
+  size_t stride;            // >= nx
+  const double * lap_l[4];  // per-variable Laplacian coefficients, packed e = i - i0
+  const double * lap_c[4];
+  const double * lap_u[4];
+  double * lo;              // [12][stride]
+  double * w;
+  double * v;
+};
+
+// Periodic y / z factors (planar configuration with implicit y and z).
+struct YZFactors {
+  int n_i[4];
+  int max_i;
+  size_t stride_y;          // max_i * ny
+  size_t stride_z;          // nz
+  const double * lapy_l[4];
+  const double * lapy_c[4];
+  const double * lapy_u[4];
+  double lapz_l, lapz_c, lapz_u;
+  double * l;               // [12][max_i]
+  double * c;
+  double * u;
+  double * v;               // [12][max_i][ny]
+  double * w;
+  double * q1;
+  double * lz;              // [12]
+  double * cz;
+  double * uz;
+  double * vz;              // [12][nz]
+  double * wz;
+  double * q1z;
+};
+
+// Poisson solver state.
+struct Poisson {
+  int nyh;                  // ny/2 + 1
+  double2 * spec;           // [nx][nz][nyh] complex spectra
+  double * vscr;            // [nx][nz][nyh] elimination factors
+  const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny/2
+  const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz/2
+  const double * tl;        // radial l_i (compute_potential.c:197-200), length nx
+  const double * tu;        // radial u_i
+  const double * ihy2;      // 1 / HYXC(i)^2 as (1/HYXC)/HYXC, length nx (index i-1)
+  const double * hyxc;      // HYXC(i), length nx (index i-1)
+  const double * eval_y;    // -4 sin^2(pi m / ny), m < nyh
+  const double * eval_z;    // -4 sin^2(pi m / nz), m < nz
+};
+
+void launch_rhs_delta(const Geo & g, const Bc & bc, const Coefs & cf, double nu, double kappa,
+                      const Fields & f, double * const s_old[4], double * const s_new[4],
+                      double * const d[4], const double * dtp, int rkstep, cudaStream_t st);
+void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);
+enum { XS_SOLVE_APPLY = 0, XS_SOLVE = 1, XS_APPLY = 2 };
+void launch_xsolve(const Geo & g, const Bc & bc, const XFactors & xf, int rkstep, int mode,
+                   const Fields & f, double * const d[4], cudaStream_t st);
+void launch_yzfactors(const Geo & g, const YZFactors & yf, const double * dtp, double nu, double kappa, cudaStream_t st);
+void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st);
+void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st);
+int xsolve_elems(int nx);
+
+// tab_y[i][ky] = ey/hyxc/hyxc, tab_z[kz] = ez/hz/hz, base[i] = -l_i - u_i
+void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+                    const double * tab_y, const double * tab_z, const double * base,
+                    const double * dtp, int rkstep, cudaStream_t st);
+void poisson_smem_limits();
+enum { CORRECT_VELOCITY = 1, CORRECT_PRESSURE = 2 };
+void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+                    int rkstep, double nu, int what, cudaStream_t st);
+
+// decide_dt: dt_caps[0..2] are the diffusive limits (0 when that direction is
+// implicit), written to *dtp together with status bits in *status
+void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,
+                      unsigned long long * dtmin, double * dtp, unsigned * status, cudaStream_t st);
+
+// boundary conditions + periodic images of a single field (boundary/*.c)
+enum BcKind { BC_UX = 0, BC_UY, BC_UZ, BC_P, BC_PSI, BC_T };
+void launch_bc(const Geo & g, const Bc & bc, BcKind kind, double * a, cudaStream_t st);
+
+// velocity-gradient tensors with halos (predict/l*.c), for logging/statistics
+struct Tensors { double * a[11]; };  // lxx lxy lxz lyx0 lyx1 lyy0 lyy1 lyz lzx lzy lzz
+void launch_tensors(const Geo & g, const Coefs & cf, const Fields & f, const Tensors & tn, cudaStream_t st);
+
+// logging reductions (src/logging/*.c); out: 9 doubles on the device,
+// partial: DIAG_BLOCKS x 9 doubles of scratch
+constexpr int DIAG_BLOCKS_MAX = 296;
+void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const Fields & f, double nu, double kappa,
+                        double * out, double * partial, cudaStream_t st);
+
+}  // namespace tcgpu
