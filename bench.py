@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Throughput of SimpleTCSolver's RK3 time step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tcgpu|reference]
+
+Workload: the Taylor-Couette case at Re=1e4 on the 256x1024x512 grid (FP64),
+seeded synthetic noisy circular-Couette initial field. One step = decide_dt +
+three RK substeps of predict / Poisson / correct / pressure (src/integrate.c).
+
+Metric: Mcell-steps/s = nx*ny*nz * steps / device seconds, summed over ranks.
+  value     device time of K steps with the state resident in HBM (CUDA events
+            on the library's stream, the step replayed as one CUDA graph)
+  e2e       the same K steps through the reference entry point integrate()
+            with host arrays: every step copies ux, uy, uz, p, t host->device
+            and ux, uy, uz, p, t, psi back (page-locked host memory)
+  roofline  the kernel with the largest share of the step: algorithmic bytes
+            per launch / its mean launch time from events around each launch
+Multi-GPU: the path does not shard (global FFTs, single-rank drop-in), so N GPUs
+run N independent replicas ("scaling": "weak"); time = max over ranks.
+
+--impl reference times the reference's own CPU code (oracle/_ref/tcref_tc,
+built from the reference sources) on this host's cores: P single-rank
+processes, each integrating a 64x128x64 sample of the same case, throughput
+summed; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import datetime
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s on 1 B200 (plain FP64 vs chosen form); torque err vs FP64 fine"
+UNIT = "Mcell-steps/s"
+WORKLOAD = "taylor-couette 256x1024x512 Re=1e4 fp64"
+SAMPLE_GRID = (64, 128, 64)
+
+# algorithmic bytes per cell and launch (8-byte words; the radial implicit solve
+# is counted as its own pass): reads + writes each kernel must do
+KERNELS = ["DTMIN", "DTFINAL", "FACTORS", "RHS", "XSOLVE", "YZSOLVE", "DIV_FFTY", "FFTZ_FWD", "TDM",
+           "FFTZ_INV", "IFFTY", "CORRECT"]
+BYTES_PER_CELL = {
+    "DTMIN": 3 * 8,                            # ux, uy, uz
+    # 5 fields read, srcA_new + delta written (104 B); substeps 2 and 3 also read srcA_old (136 B)
+    "RHS": (104.0 + 136.0 + 136.0) / 3.0,
+    "XSOLVE": 12 * 8,                          # delta, u read; u written (4 variables)
+    "DIV_FFTY": 3 * 8 + 8,                     # ux, uy, uz read; half-spectrum written
+    "FFTZ_FWD": 16, "TDM": 16, "FFTZ_INV": 16,  # spectrum read + written
+    "IFFTY": 8 + 8,                            # spectrum read, psi written
+    "CORRECT": 9 * 8,                          # psi, ux, uy, uz, p read; ux, uy, uz, p written
+}
+MODEL_BYTES_PER_CELL_STEP = 936.0              # minimum-pass model of the whole step (FP64)
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["tcgpu", "reference"], default="tcgpu")
+    ap.add_argument("--grid", type=str, default="256x1024x512")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ------------------------------------------------------------------ ranks
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def aggregate(elapsed_s: float, units: float, world: int):
+    """Max elapsed time and summed units over ranks (all ranks call this)."""
+    if world == 1:
+        return elapsed_s, units
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([elapsed_s], dtype=torch.float64, device=dev)
+    u = torch.tensor([units], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def __enter__(self):
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.tmp.flush()
+        rows = list(csv.reader(io.StringIO(open(self.tmp.name).read())))
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        top = max(sm)
+        load = [v for v in sm if v >= 0.5 * top] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU reference
+def ref_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "tcref_tc")
+    return p if os.path.exists(p) else None
+
+
+def cpu_reference_run(steps: int, warmup: int):
+    """The reference's own integrate() on this host's cores: P concurrent
+    single-rank processes on a 64x128x64 sample of the workload."""
+    from simpletcsolver_b200 import ic
+    nx, ny, nz = SAMPLE_GRID
+    case = ic.taylor_couette(nx, ny, nz, 1.0e4)
+    binary = ref_binary()
+    cores = len(os.sched_getaffinity(0))
+    procs = max(1, min(cores, 64))
+    with tempfile.TemporaryDirectory() as td:
+        d0 = ic.write_ic(case, os.path.join(td, "ic"))
+        env = dict(os.environ, **ic.case_env(case))
+        if binary is not None:
+            kind = "reference"
+            runs = [subprocess.Popen([binary, d0, str(max(1, warmup)), str(steps)], env=env, stdout=subprocess.PIPE,
+                                     stderr=subprocess.DEVNULL, text=True) for _ in range(procs)]
+            rates = []
+            for r in runs:
+                out, _ = r.communicate(timeout=3600)
+                line = [x for x in out.splitlines() if x.startswith("{")][-1]
+                res = json.loads(line)
+                rates.append(res["cells"] * res["steps"] / res["seconds"] / 1e6)
+            value = sum(rates)
+            sample = (f"{procs} concurrent single-rank reference processes (oracle/_ref/tcref_tc, the reference's "
+                      f"own C sources), each {nx}x{ny}x{nz} at Re=1e4, {warmup} warm-up + {steps} timed steps; "
+                      f"rates summed")
+        else:
+            kind = "port"
+            from oracle import tc_numpy as tn
+            prm = tn.Params(coef_dt_adv=case.coef_dt_adv, coef_dt_dif=case.coef_dt_dif)
+            d = tn.load_domain(d0)
+            fl = tn.load_fluid(d, d0, case.Re, case.Pr, prm)
+            tn.integrate(d, fl, prm)
+            t0 = time.perf_counter()
+            n = max(1, min(steps, 3))
+            for _ in range(n):
+                tn.integrate(d, fl, prm)
+            value = case.ncells * n / (time.perf_counter() - t0) / 1e6
+            procs = 1
+            sample = f"numpy restatement, 1 process, {nx}x{ny}x{nz}, {n} steps"
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample}
+
+
+# ------------------------------------------------------------------ GPU arm
+def parse_grid(s):
+    nx, ny, nz = (int(v) for v in s.lower().split("x"))
+    return nx, ny, nz
+
+
+def gpu_arm(args, rank, world, local):
+    import ctypes as C
+    from simpletcsolver_b200 import abi, build, ic
+    from simpletcsolver_b200.solver import Solver
+    build.build()
+    lib = abi.load()
+    if lib.tcgpu_set_device(local) != 0:
+        raise RuntimeError(abi.last_error(lib))
+    nx, ny, nz = parse_grid(args.grid)
+    case = ic.taylor_couette(nx, ny, nz, 1.0e4)
+    td = tempfile.mkdtemp(prefix="tcbench")
+    d0 = ic.write_ic(case, os.path.join(td, "ic"))
+    s = Solver.from_ic(d0, case=case, lib=lib)
+    s.set_coherence(abi.PIN_HOST)
+    s.push()
+    K, W = args.steps, args.warmup
+    s.run(W)                                     # warm-up, graph capture
+    ncell = case.ncells
+
+    def timed(nsteps, instrument):
+        el = C.c_float(0.)
+        kms = (C.c_double * 12)()
+        kl = (C.c_int * 12)()
+        dts = (C.c_double * max(nsteps, 1))()
+        done = 0
+        total_ms = 0.0
+        ktot = [0.0] * 12
+        ltot = [0] * 12
+        while done < nsteps:
+            n = min(64, nsteps - done)
+            rc = lib.tcgpu_run_timed(C.byref(s.domain), C.byref(s.fluid), n, instrument, dts, C.byref(el), kms, kl)
+            if rc != 0:
+                raise RuntimeError(abi.last_error(lib))
+            total_ms += el.value
+            ktot = [a + b for a, b in zip(ktot, kms)]
+            ltot = [a + b for a, b in zip(ltot, kl)]
+            done += n
+        return total_ms, ktot, ltot
+
+    lib.tcgpu_run_timed.argtypes = [C.POINTER(abi.DomainT), C.POINTER(abi.FluidT), C.c_int, C.c_int,
+                                    abi.c_double_p, C.POINTER(C.c_float), C.c_double * 12, C.c_int * 12]
+    import torch
+    barrier(world)
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms, _, launches = timed(K, 0)
+    barrier(world)
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
+    elapsed, units = aggregate(ms / 1e3, ncell * K, world)
+    value = units / elapsed / 1e6
+
+    # per-kernel accounting: events around every launch of K instrumented steps
+    kms_total, kdev, klaunch = timed(K, 1)
+    per_kernel = {}
+    for i, name in enumerate(KERNELS):
+        if klaunch[i] == 0:
+            continue
+        avg = kdev[i] / klaunch[i]
+        entry = {"launches": klaunch[i], "ms_total": kdev[i], "share": kdev[i] / kms_total, "ms_per_launch": avg}
+        if name in BYTES_PER_CELL:
+            gbs = BYTES_PER_CELL[name] * ncell / (avg / 1e3) / 1e9
+            entry["gbs"] = gbs
+        per_kernel[name] = entry
+    dom = max((k for k in per_kernel if k in BYTES_PER_CELL), key=lambda k: per_kernel[k]["ms_total"])
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = per_kernel[dom]["gbs"]
+    traffic = measured_traffic(dom, ncell)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "algorithmic_bytes_per_launch": BYTES_PER_CELL[dom] * ncell,
+                "peak_source": "measured" if "hbm_gbs" in peaks and os.path.exists(
+                    os.path.join(ROOT, "MEASURED_PEAKS.json")) else "fallback"}
+    step_model = MODEL_BYTES_PER_CELL_STEP * ncell / (ms / K / 1e3) / 1e9
+    for k in per_kernel:
+        if "gbs" in per_kernel[k]:
+            per_kernel[k]["frac"] = per_kernel[k]["gbs"] / peak
+
+    e2e = None
+    if not args.no_e2e:
+        t0 = time.perf_counter()
+        for _ in range(K):
+            s.integrate()
+        el = time.perf_counter() - t0
+        e_el, e_units = aggregate(el, ncell * K, world)
+        nf = (nx + 1) * (ny + 2) * (nz + 2)
+        nc = (nx + 2) * (ny + 2) * (nz + 2)
+        e2e = {"value": e_units / e_el / 1e6, "unit": UNIT, "h2d_bytes_per_step": (nf + 4 * nc) * 8,
+               "d2h_bytes_per_step": (nf + 5 * nc) * 8, "timing": "host wall clock around synchronous integrate()"}
+    s.release()
+    gpu_launches = sum(launches)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_run(max(2, min(args.steps, 5)), 1)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": elapsed * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field (no dataset involved)",
+            "config": {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz], "Re": 1.0e4,
+                       "coef_dt_adv": case.coef_dt_adv, "implicit": "x", "parallelism": f"replicas{world}",
+                       "l2": "no flush: every field (1.09 GB at 256x1024x512) exceeds the 126 MB L2"},
+            "roofline": roofline,
+            "step_model": {"bytes_per_cell_step": MODEL_BYTES_PER_CELL_STEP, "achieved_gbs": step_model,
+                           "frac": step_model / peak},
+            "kernels": per_kernel,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clk.summary(),
+            "gpu_launches": gpu_launches,
+        }
+        print(json.dumps(out))
+    return 0
+
+
+def measured_traffic(kernel: str, ncell: int):
+    """DRAM bytes per launch from the committed ncu summary of that kernel
+    (profiles/*.txt lines 'kernel: NAME dram_bytes_per_cell: X')."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith(".txt"):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            parts = line.split()
+            if len(parts) >= 4 and parts[0] == "kernel:" and parts[1] == kernel and parts[2] == "dram_bytes_per_cell:":
+                return float(parts[3]) * ncell
+    return None
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    cpu = cpu_reference_run(args.steps, args.warmup)
+    nx, ny, nz = parse_grid(args.grid)
+    out = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field",
+           "config": {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz],
+                      "sample_grid": list(SAMPLE_GRID)},
+           "cpu_baseline": cpu,
+           "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    rank, world, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return reference_arm(args, rank, world)
+        return gpu_arm(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

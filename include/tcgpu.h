@@ -204,6 +204,35 @@ int tcgpu_pull(const domain_t * domain, fluid_t * fluid, unsigned fields);
  * NULL) receives each step's dt */
 int tcgpu_run(const domain_t * domain, fluid_t * fluid, int nsteps, double * dts);
 
+/* kernels of one time step, for tcgpu_run_timed's per-kernel accounting */
+typedef enum {
+  TCGPU_K_DTMIN = 0,     /* CFL reduction (decide_dt_adv) */
+  TCGPU_K_DTFINAL,       /* dt from the reduction and the diffusive limits */
+  TCGPU_K_FACTORS,       /* implicit-solve elimination factors for the step */
+  TCGPU_K_RHS,           /* fused right-hand sides + RK increment (predict) */
+  TCGPU_K_XSOLVE,        /* radial implicit solve + update + boundaries */
+  TCGPU_K_YZSOLVE,       /* periodic implicit solves in y and z */
+  TCGPU_K_DIV_FFTY,      /* divergence + forward y transform */
+  TCGPU_K_FFTZ_FWD,      /* forward z transform */
+  TCGPU_K_TDM,           /* radial Poisson solve per wavenumber pair */
+  TCGPU_K_FFTZ_INV,      /* backward z transform */
+  TCGPU_K_IFFTY,         /* backward y transform -> psi */
+  TCGPU_K_CORRECT,       /* velocity correction + pressure update */
+  TCGPU_K_COUNT
+} tcgpu_kernel_t;
+
+/* tcgpu_run, timed with CUDA events recorded on the library's own stream.
+ * elapsed_ms: device time of the nsteps steps. With instrument != 0 the steps
+ * run as individual launches with an event after each kernel, and
+ * kernel_ms[TCGPU_K_COUNT] / kernel_launches[TCGPU_K_COUNT] receive the summed
+ * device time and launch count per kernel kind (otherwise the captured CUDA
+ * graph runs and only the launch counts are filled). Any output may be NULL. */
+int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int instrument, double * dts,
+                    float * elapsed_ms, double * kernel_ms, int * kernel_launches);
+
+/* select the CUDA device used by contexts created afterwards in this thread */
+int tcgpu_set_device(int device);
+
 /* logging quantities of src/logging/*.c from the device state:
  * out[0] max |div u|, out[1..2] energy injection (momentum, scalar),
  * out[3..4] dissipation (momentum, scalar), out[5..8] total energy

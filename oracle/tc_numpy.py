@@ -211,13 +211,21 @@ def bc_t(d, t, prm):   # src/fluid/boundary/t.c
     halo_yz(t)
 
 
+def _rdiv(q, c):
+    """q / c for a real divisor, componentwise when q is complex (C99 Annex G
+    semantics of double _Complex / double, as the reference computes it)."""
+    if np.iscomplexobj(q):
+        return (q.real / c) + 1j * (q.imag / c)
+    return q / c
+
+
 def gtsv(l, c, u, q, singular_guard=True):
     """Thomas algorithm along axis 0 of q (src/tdm.c:17-50); l, c, u have
     length n along axis 0 and broadcast against q[i]. q is overwritten."""
     n = q.shape[0]
     v = np.empty((n,) + np.broadcast(c[0], q[0]).shape if np.ndim(c) > 1 else (n,))
     v[0] = u[0] / c[0]
-    q[0] = q[0] / c[0]
+    q[0] = _rdiv(q[0], c[0])
     for i in range(1, n - 1):
         val = 1.0 / (c[i] - l[i] * v[i - 1])
         v[i] = val * (u[i])
@@ -251,7 +259,7 @@ def tdm_periodic(l, c, u, q):
     num = q0[n - 1] - u[n - 1] * q0[0] - l[n - 1] * q0[n - 2]
     den = c[n - 1] + u[n - 1] * q1[0] + l[n - 1] * q1[n - 2]
     with np.errstate(divide="ignore", invalid="ignore"):
-        last = np.where(np.abs(den) < DBL_EPSILON, 0.0, num / den)
+        last = np.where(np.abs(den) < DBL_EPSILON, 0.0, _rdiv(num, den))
     q0[n - 1] = last
     q0[:n - 1] = q0[:n - 1] + q0[n - 1] * q1
     return q0
@@ -786,3 +794,51 @@ def integrate(d: Domain, fl: Fluid, prm: Params, gauge: str = "pin") -> float:
         correct_velocity(d, rk, dt, fl, prm)
         update_pressure(d, rk, dt, fl, prm)
     return dt
+
+
+# ---------------------------------------------------------------- logging
+
+def diagnostics(d: Domain, fl: Fluid) -> dict:
+    """src/logging/divergence.c:32-91, injection.c:31-103,
+    dissipation.c:27-371, total_energy.c:22-93, from the current fields."""
+    nx = d.nx
+    T = compute_tensors(d, fl)
+    out = {}
+    out["divmax"] = float(np.max(np.abs(divergence(d, fl.ux, fl.uy, fl.uz))))
+    nu = 1.0 / fl.Re
+    kappa = 1.0 / fl.Re / fl.Pr
+    j = slice(1, d.ny + 1)
+    k = slice(1, d.nz + 1)
+    tyx_m = T["lyx0"][k, j, 1] + T["lyx1"][k, j, 1] + T["lxy"][k, j, 1]
+    tyx_p = T["lyx0"][k, j, nx + 1] + T["lyx1"][k, j, nx + 1] + T["lxy"][k, j, nx + 1]
+    inj = (-d.jdxf[1] / d.hxxf[1] * fl.uy[k, j, 0] * tyx_m
+           + d.jdxf[nx + 1] / d.hxxf[nx + 1] * fl.uy[k, j, nx + 1] * tyx_p)
+    out["injection_u"] = nu * float(np.sum(inj))
+    t = fl.t
+    inj_t = (-d.jdxf[1] / d.hxxf[1] * t[k, j, 0] / d.hxxf[1] * (-t[k, j, 0] + t[k, j, 1])
+             + d.jdxf[nx + 1] / d.hxxf[nx + 1] * t[k, j, nx + 1] / d.hxxf[nx + 1] * (-t[k, j, nx] + t[k, j, nx + 1]))
+    out["injection_t"] = kappa * float(np.sum(inj_t))
+    F = lambda a: V(d, a, 1, nx + 1)
+    Cc = lambda a: V(d, a, 1, nx)
+    jf = M(d.jdxf, 1, nx + 1)
+    jc = M(d.jdxc, 1, nx)
+    lyx = F(T["lyx0"]) + F(T["lyx1"])
+    lxy = F(T["lxy"])
+    lzx = F(T["lzx"])
+    lxz = F(T["lxz"])
+    lyy = Cc(T["lyy0"]) + Cc(T["lyy1"])
+    dis = (np.sum(jc * Cc(T["lxx"]) * (Cc(T["lxx"]) + Cc(T["lxx"])))
+           + np.sum(jf * lyx * (lyx + lxy)) + np.sum(jf * lzx * (lzx + lxz)) + np.sum(jf * lxy * (lxy + lyx))
+           + np.sum(jc * lyy * (lyy + lyy)) + np.sum(jc * Cc(T["lzy"]) * (Cc(T["lzy"]) + Cc(T["lyz"])))
+           + np.sum(jf * lxz * (lxz + lzx)) + np.sum(jc * Cc(T["lyz"]) * (Cc(T["lyz"]) + Cc(T["lzy"])))
+           + np.sum(jc * Cc(T["lzz"]) * (Cc(T["lzz"]) + Cc(T["lzz"]))))
+    out["dissipation_u"] = nu * float(dis)
+    dtx = (-V(d, t, 1, nx + 1, -1) + V(d, t, 1, nx + 1)) / M(d.hxxf, 1, nx + 1)
+    dty = (-V(d, t, 1, nx, 0, -1) + V(d, t, 1, nx)) / M(d.hyxc, 1, nx)
+    dtz = (-V(d, t, 1, nx, 0, 0, -1) + V(d, t, 1, nx)) / d.hz
+    out["dissipation_t"] = kappa * float(np.sum(jf * dtx ** 2) + np.sum(jc * dty ** 2) + np.sum(jc * dtz ** 2))
+    out["energy_ux"] = float(np.sum(M(d.jdxf, 2, nx) * 0.5 * V(d, fl.ux, 2, nx) ** 2))
+    out["energy_uy"] = float(np.sum(jc * 0.5 * V(d, fl.uy, 1, nx) ** 2))
+    out["energy_uz"] = float(np.sum(jc * 0.5 * V(d, fl.uz, 1, nx) ** 2))
+    out["energy_t"] = float(np.sum(jc * 0.5 * V(d, fl.t, 1, nx) ** 2))
+    return out

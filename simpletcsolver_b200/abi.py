@@ -102,7 +102,7 @@ def declared_symbols(header: str = HEADER):
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     names = set(re.findall(r"^\s*(?:extern\s+)?(?:const\s+)?[\w\s\*]+?\b(\w+)\s*\(", src, flags=re.M))
     names |= set(re.findall(r"^\s*extern\s+const\s+\w+\s+(\w+)", src, flags=re.M))
-    return sorted(n for n in names if n not in ("if", "defined"))
+    return sorted(n for n in names if n not in ("if", "defined", "int", "double", "void"))
 
 
 def _bind(lib, sigs):

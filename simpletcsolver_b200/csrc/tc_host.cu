@@ -84,6 +84,7 @@ struct Ctx {
   unsigned coherence = 0;
   cudaStream_t st = nullptr;
   cudaGraphExec_t step_graph = nullptr;
+  int graph_launches[TCGPU_K_COUNT] = {0};
   std::vector<void *> pinned;     // caller arrays registered with cudaHostRegister
   double * h_scalar = nullptr;    // pinned: dt in / out
   unsigned * h_status = nullptr;  // pinned
@@ -499,12 +500,38 @@ static Ctx * get_ctx(const domain_t * d, const fluid_t * fl) {
 }
 
 // ------------------------------------------------------------------ schedule
+// Optional per-kernel accounting: an event after each launch (instrumented
+// runs only) and a launch count per kernel kind.
+struct Recorder {
+  bool events = false;
+  cudaStream_t st = nullptr;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  size_t used = 0;
+  int launches[TCGPU_K_COUNT] = {0};
+  void mark(int k, int n = 1) {
+    launches[k] += n;
+    if (!events) return;
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev.push_back(e);
+      kind.push_back(k);
+    }
+    kind[used] = k;
+    cudaEventRecord(ev[used++], st);
+  }
+  ~Recorder() { for (auto e : ev) cudaEventDestroy(e); }
+};
+static thread_local Recorder * g_rec = nullptr;
+static void mark(int k, int n = 1) { if (g_rec) g_rec->mark(k, n); }
+
 static double * s_new(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 1 : 0]; }
 static double * s_old(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 0 : 1]; }
 
 static void enqueue_factors(Ctx & c) {
-  if (c.bc.implicit[0]) launch_xfactors(c.xf, c.dtp, c.nu, c.kappa, c.st);
-  if (c.bc.implicit[1] || c.bc.implicit[2]) launch_yzfactors(c.g, c.yf, c.dtp, c.nu, c.kappa, c.st);
+  if (c.bc.implicit[0]) { launch_xfactors(c.xf, c.dtp, c.nu, c.kappa, c.st); mark(TCGPU_K_FACTORS); }
+  if (c.bc.implicit[1] || c.bc.implicit[2]) { launch_yzfactors(c.g, c.yf, c.dtp, c.nu, c.kappa, c.st); mark(TCGPU_K_FACTORS); }
 }
 
 static void enqueue_predict(Ctx & c, int rk) {
@@ -514,27 +541,41 @@ static void enqueue_predict(Ctx & c, int rk) {
     so[v] = s_old(c, v, rk);
   }
   launch_rhs_delta(c.g, c.bc, c.cf, c.nu, c.kappa, c.f, so, sn, c.delta, c.dtp, rk, c.st);
+  mark(TCGPU_K_RHS);
   const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
   if (!iy && !iz) {
     launch_xsolve(c.g, c.bc, c.xf, rk, c.bc.implicit[0] ? XS_SOLVE_APPLY : XS_APPLY, c.f, c.delta, c.st);
+    mark(TCGPU_K_XSOLVE);
     return;
   }
-  if (c.bc.implicit[0]) launch_xsolve(c.g, c.bc, c.xf, rk, XS_SOLVE, c.f, c.delta, c.st);
-  if (iy) launch_ysolve(c.g, c.yf, rk, c.delta, c.st);
-  if (iz) launch_zsolve(c.g, c.yf, rk, c.delta, c.st);
+  if (c.bc.implicit[0]) { launch_xsolve(c.g, c.bc, c.xf, rk, XS_SOLVE, c.f, c.delta, c.st); mark(TCGPU_K_XSOLVE); }
+  if (iy) { launch_ysolve(c.g, c.yf, rk, c.delta, c.st); mark(TCGPU_K_YZSOLVE, 4); }
+  if (iz) { launch_zsolve(c.g, c.yf, rk, c.delta, c.st); mark(TCGPU_K_YZSOLVE, 4); }
   launch_xsolve(c.g, c.bc, c.xf, rk, XS_APPLY, c.f, c.delta, c.st);
+  mark(TCGPU_K_XSOLVE);
 }
 
 static void enqueue_potential(Ctx & c, int rk) {
-  launch_poisson(c.g, c.cf, c.ps, c.f, c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st);
+  PoissonMarks pm;
+  pm.mark = g_rec ? &mark : nullptr;
+  pm.k_div = TCGPU_K_DIV_FFTY;
+  pm.k_fwd = TCGPU_K_FFTZ_FWD;
+  pm.k_tdm = TCGPU_K_TDM;
+  pm.k_inv = TCGPU_K_FFTZ_INV;
+  pm.k_ify = TCGPU_K_IFFTY;
+  launch_poisson(c.g, c.cf, c.ps, c.f, c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st, pm);
 }
 
 static void enqueue_correct(Ctx & c, int rk, int what) {
   launch_correct(c.g, c.bc, c.cf, c.f, c.dtp, rk, c.nu, what, c.st);
+  mark(TCGPU_K_CORRECT);
 }
 
 static void enqueue_step(Ctx & c) {
-  launch_decide_dt(c.g, c.f, c.coef_adv, c.dt_caps, c.dtmin, c.dtp, c.status, c.st);
+  launch_dtmin(c.g, c.f, c.dtmin, c.status, c.st);
+  mark(TCGPU_K_DTMIN);
+  launch_dtfinal(c.coef_adv, c.dt_caps, c.dtmin, c.dtp, c.status, c.st);
+  mark(TCGPU_K_DTFINAL);
   enqueue_factors(c);
   for (int rk = 0; rk < 3; rk++) {
     enqueue_predict(c, rk);
@@ -546,9 +587,14 @@ static void enqueue_step(Ctx & c) {
 static int launch_step(Ctx & c) {
   if (c.step_graph == nullptr) {
     cudaGraph_t graph;
+    Recorder count;
+    Recorder * prev = g_rec;
+    g_rec = &count;
     CK(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
     enqueue_step(c);
     CK(cudaStreamEndCapture(c.st, &graph));
+    g_rec = prev;
+    for (int k = 0; k < TCGPU_K_COUNT; k++) c.graph_launches[k] = count.launches[k];
     cudaError_t e = cudaGraphInstantiate(&c.step_graph, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail("cudaGraphInstantiate failed: %s", cudaGetErrorString(e));
@@ -784,6 +830,58 @@ int tcgpu_run(const domain_t * domain, fluid_t * fluid, int nsteps, double * dts
   return 0;
 }
 
+int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int instrument, double * dts,
+                    float * elapsed_ms, double * kernel_ms, int * kernel_launches) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (nsteps < 0 || nsteps > 64) return fail("tcgpu_run_timed: nsteps must be in [0, 64]");
+  Recorder rec;
+  rec.events = instrument != 0;
+  rec.st = c->st;
+  if (!instrument && c->step_graph == nullptr && launch_step(*c)) return 1;   // capture outside the timing
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaEventRecord(e0, c->st));
+  if (instrument) rec.mark(TCGPU_K_DTMIN, 0);   // start marker, counts nothing
+  for (int s = 0; s < nsteps; s++) {
+    if (instrument) {
+      g_rec = &rec;
+      enqueue_step(*c);
+      g_rec = nullptr;
+    } else {
+      if (launch_step(*c)) return 1;
+    }
+    if (dts) CK(cudaMemcpyAsync(c->h_scalar + s, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  }
+  CK(cudaEventRecord(e1, c->st));
+  if (finish(*c, "tcgpu_run_timed")) return 1;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (elapsed_ms) *elapsed_ms = ms;
+  if (dts) memcpy(dts, c->h_scalar, sizeof(double) * nsteps);
+  if (kernel_ms) {
+    for (int k = 0; k < TCGPU_K_COUNT; k++) kernel_ms[k] = 0.;
+    for (size_t i = 1; i < rec.used; i++) {
+      float d = 0.f;
+      cudaEventElapsedTime(&d, rec.ev[i - 1], rec.ev[i]);
+      kernel_ms[rec.kind[i]] += d;
+    }
+  }
+  if (kernel_launches) {
+    for (int k = 0; k < TCGPU_K_COUNT; k++) kernel_launches[k] = instrument ? rec.launches[k] : c->graph_launches[k] * nsteps;
+  }
+  return 0;
+}
+
+int tcgpu_set_device(int device) {
+  CK(cudaSetDevice(device));
+  return 0;
+}
+
 int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
@@ -874,6 +972,8 @@ int integrate(const domain_t * domain, fluid_t * fluid, double * dt) {
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
   if (launch_step(*c)) return 1;
   CK(cudaMemcpyAsync(c->h_scalar, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  // a rejected step (non-finite field, invalid dt) leaves the caller's arrays untouched
+  if (finish(*c, "integrate")) return 1;
   if (coherent(*c)) {
     if (pull_fields(*c, fluid, TCGPU_FIELDS)) return 1;
     // three predict calls swap the caller's alpha/beta source buffers three times

@@ -133,10 +133,15 @@ void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, double * con
 void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st);
 int xsolve_elems(int nx);
 
+// optional per-launch callback of the host's kernel accounting
+struct PoissonMarks {
+  void (*mark)(int kind, int n) = nullptr;
+  int k_div = 0, k_fwd = 0, k_tdm = 0, k_inv = 0, k_ify = 0;
+};
 // tab_y[i][ky] = ey/hyxc/hyxc, tab_z[kz] = ez/hz/hz, base[i] = -l_i - u_i
 void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
                     const double * tab_y, const double * tab_z, const double * base,
-                    const double * dtp, int rkstep, cudaStream_t st);
+                    const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm = PoissonMarks());
 void poisson_smem_limits();
 enum { CORRECT_VELOCITY = 1, CORRECT_PRESSURE = 2 };
 void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
@@ -146,6 +151,9 @@ void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields
 // implicit), written to *dtp together with status bits in *status
 void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,
                       unsigned long long * dtmin, double * dtp, unsigned * status, cudaStream_t st);
+void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st);
+void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,
+                    unsigned * status, cudaStream_t st);
 
 // boundary conditions + periodic images of a single field (boundary/*.c)
 enum BcKind { BC_UX = 0, BC_UY, BC_UZ, BC_P, BC_PSI, BC_T };

@@ -171,10 +171,19 @@ __global__ void dtfinal_kernel(double coef_adv, const double * caps, unsigned lo
   *dtmin = 0x3ff0000000000000ull;  // 1.0, the reference's starting value
 }
 
+void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
+  dtmin_kernel<<<148 * 8, 256, 0, st>>>(g, f.ux, f.uy, f.uz, dtmin, status);
+}
+
+void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,
+                    unsigned * status, cudaStream_t st) {
+  dtfinal_kernel<<<1, 1, 0, st>>>(coef_adv, dt_caps, dtmin, dtp, status);
+}
+
 void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,
                       unsigned long long * dtmin, double * dtp, unsigned * status, cudaStream_t st) {
-  dtmin_kernel<<<148 * 8, 256, 0, st>>>(g, f.ux, f.uy, f.uz, dtmin, status);
-  dtfinal_kernel<<<1, 1, 0, st>>>(coef_adv, dt_caps, dtmin, dtp, status);
+  launch_dtmin(g, f, dtmin, status, st);
+  launch_dtfinal(coef_adv, dt_caps, dtmin, dtp, status, st);
 }
 
 // --------------------------------------------------------------- boundary conditions

@@ -259,19 +259,25 @@ static int pick_lines(int n, int maxlines) {
 
 void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
                     const double * tab_y, const double * tab_z, const double * base,
-                    const double * dtp, int rkstep, cudaStream_t st) {
+                    const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
+  auto mark = [&](int k) { if (pm.mark) pm.mark(k, 1); };
   const int P = pick_lines(g.ny, 8);
   const size_t smy = sizeof(double2) * 2 * (size_t)P * g.ny;
   dim3 gy((g.nx + 2 * P - 1) / (2 * P), g.nz);
   div_ffty_kernel<<<gy, 256, smy, st>>>(g, cf, ps, P, f.ux, f.uy, f.uz, dtp, rkstep);
+  mark(pm.k_div);
   const int TM = pick_lines(g.nz, 16);
   const size_t smz = sizeof(double2) * 2 * (size_t)TM * g.nz;
   dim3 gz(g.nx, (ps.nyh + TM - 1) / TM);
   fftz_kernel<-1><<<gz, 256, smz, st>>>(g, ps, TM);
+  mark(pm.k_fwd);
   const long long nl = (long long)ps.nyh * g.nz;
   tdm_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+  mark(pm.k_tdm);
   fftz_kernel<+1><<<gz, 256, smz, st>>>(g, ps, TM);
+  mark(pm.k_inv);
   iffty_kernel<<<gy, 256, smy, st>>>(g, ps, P, f.psi);
+  mark(pm.k_ify);
 }
 
 void poisson_smem_limits() {
