@@ -45,15 +45,14 @@ UNIT = "Mcell-steps/s"
 WORKLOAD = "taylor-couette 256x1024x512 Re=1e4 fp64"
 SAMPLE_GRID = (64, 128, 64)
 
-# algorithmic bytes per cell and launch (8-byte words; the radial implicit solve
-# is counted as its own pass): reads + writes each kernel must do
-KERNELS = ["DTMIN", "DTFINAL", "FACTORS", "RHS", "XSOLVE", "YZSOLVE", "DIV_FFTY", "FFTZ_FWD", "TDM",
+# algorithmic bytes per cell and launch (8-byte words): reads + writes each kernel must do
+KERNELS = ["DTMIN", "DTFINAL", "FACTORS", "PREDICT", "APPLY", "YZSOLVE", "DIV_FFTY", "FFTZ_FWD", "TDM",
            "FFTZ_INV", "IFFTY", "CORRECT"]
 BYTES_PER_CELL = {
     "DTMIN": 3 * 8,                            # ux, uy, uz
-    # 5 fields read, srcA_new + delta written (104 B); substeps 2 and 3 also read srcA_old (136 B)
-    "RHS": (104.0 + 136.0 + 136.0) / 3.0,
-    "XSOLVE": 12 * 8,                          # delta, u read; u written (4 variables)
+    # fused predict: 5 fields read, srcA_new + new ux, uy, uz, t written (104 B);
+    # substeps 2 and 3 also read srcA_old (136 B)
+    "PREDICT": (104.0 + 136.0 + 136.0) / 3.0,
     "DIV_FFTY": 3 * 8 + 8,                     # ux, uy, uz read; half-spectrum written
     "FFTZ_FWD": 16, "TDM": 16, "FFTZ_INV": 16,  # spectrum read + written
     "IFFTY": 8 + 8,                            # spectrum read, psi written

@@ -209,8 +209,9 @@ typedef enum {
   TCGPU_K_DTMIN = 0,     /* CFL reduction (decide_dt_adv) */
   TCGPU_K_DTFINAL,       /* dt from the reduction and the diffusive limits */
   TCGPU_K_FACTORS,       /* implicit-solve elimination factors for the step */
-  TCGPU_K_RHS,           /* fused right-hand sides + RK increment (predict) */
-  TCGPU_K_XSOLVE,        /* radial implicit solve + update + boundaries */
+  TCGPU_K_PREDICT,       /* fused predict: right-hand sides, RK increment,
+                            radial implicit solve, update, boundaries */
+  TCGPU_K_APPLY,         /* update after the y / z solves (planar case) */
   TCGPU_K_YZSOLVE,       /* periodic implicit solves in y and z */
   TCGPU_K_DIV_FFTY,      /* divergence + forward y transform */
   TCGPU_K_FFTZ_FWD,      /* forward z transform */

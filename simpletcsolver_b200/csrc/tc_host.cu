@@ -64,9 +64,10 @@ struct Ctx {
   XFactors xf{};
   YZFactors yf{};
   Poisson ps{};
-  Fields f{};
+  Fields fb[2]{};       // ux, uy, uz, t double-buffered; p and psi shared
+  int cur = 0;          // buffer holding the current state
   double * src[4][2]{};
-  double * delta[4]{};
+  DeltaSet ds{};
   double * tab_y = nullptr;
   double * tab_z = nullptr;
   double * base = nullptr;
@@ -83,8 +84,9 @@ struct Ctx {
   double caps_h[3] = {0., 0., 0.};
   unsigned coherence = 0;
   cudaStream_t st = nullptr;
-  cudaGraphExec_t step_graph = nullptr;
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // one per starting buffer
   int graph_launches[TCGPU_K_COUNT] = {0};
+  Fields & f() { return fb[cur]; }
   std::vector<void *> pinned;     // caller arrays registered with cudaHostRegister
   double * h_scalar = nullptr;    // pinned: dt in / out
   unsigned * h_status = nullptr;  // pinned
@@ -104,7 +106,7 @@ static double * dalloc(Ctx & c, size_t n) {
 static void destroy_ctx(Ctx * c) {
   if (c == nullptr) return;
   if (c->st) cudaStreamSynchronize(c->st);
-  if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+  for (int b = 0; b < 2; b++) if (c->step_graph[b]) cudaGraphExecDestroy(c->step_graph[b]);
   for (void * p : c->pinned) cudaHostUnregister(p);
   for (void * p : c->allocs) cudaFree(p);
   if (c->h_scalar) cudaFreeHost(c->h_scalar);
@@ -165,9 +167,11 @@ static int set_physics(Ctx & c, const fluid_t * fl, const domain_t * d) {
     c.caps_h[dim] = c.bc.implicit[dim] ? 0. : v;
   }
   CK(cudaMemcpy(c.dt_caps, c.caps_h, sizeof(c.caps_h), cudaMemcpyHostToDevice));
-  if (c.step_graph) {
-    cudaGraphExecDestroy(c.step_graph);
-    c.step_graph = nullptr;
+  for (int b = 0; b < 2; b++) {
+    if (c.step_graph[b]) {
+      cudaGraphExecDestroy(c.step_graph[b]);
+      c.step_graph[b] = nullptr;
+    }
   }
   return 0;
 }
@@ -184,13 +188,10 @@ static int build_tables(Ctx & c, const domain_t * d) {
   auto HYXC = [&](int i) { return m.hyxc[i]; };
   auto JDXF = [&](int i) { return m.jdxf[i]; };
   auto JDXC = [&](int i) { return m.jdxc[i]; };
-  std::vector<double> T((size_t)NCOEF_ARRAYS * L, 0.);
-  auto col = [&](int n) { return T.data() + (size_t)n * L; };
-  enum { F_INVJD, F_A1, F_A2, F_A3, F_B1, F_B2, F_C1, F_C2, F_HD1, F_HD2, F_LXL, F_LXC, F_LXU, F_LYL, F_LYC, F_LYU,
-         F_E1, F_E2, C_LYX1F, C_WM, C_WP, C_INVHXXF, C_INVHYXC, C_INVHYXF, C_LYY1, C_INVJDXC, C_A1, C_A2, C_B, C_CZ,
-         C_HD, C_LXL, C_LXC, C_LXU, C_LYL, C_LYC, C_LYU, C_JF, C_E1, C_E2, C_HDA1, C_HDA2, C_PXL, C_PXU, C_PYL, C_PZL,
-         NCOL };
-  static_assert(NCOL == NCOEF_ARRAYS, "coefficient table count");
+  if (L > (size_t)CSTRIDE) return fail("nx = %d too large for the coefficient tables", nx);
+  std::vector<double> T((size_t)NCOEF_TABLES * CSTRIDE, 0.);
+  auto col = [&](int n) { return T.data() + (size_t)n * CSTRIDE; };
+  constexpr int NCOL = NCOEF_TABLES;
   for (int i = 2; i <= nx; i++) {   // ux at face i (ux.c)
     col(F_INVJD)[i] = 1. / JDXF(i);
     col(F_A1)[i] = 0.5 * JDXF(i - 1) / HXXF(i - 1);
@@ -259,8 +260,9 @@ static int build_tables(Ctx & c, const domain_t * d) {
   if (!dT) return fail("cudaMalloc of coefficient tables failed");
   CK(cudaMemcpy(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice));
   const double * cols[NCOL];
-  for (int n = 0; n < NCOL; n++) cols[n] = dT + (size_t)n * L;
+  for (int n = 0; n < NCOL; n++) cols[n] = dT + (size_t)n * CSTRIDE;
   Coefs & cf = c.cf;
+  cf.tab = dT;
   const double ** dst[NCOL] = {&cf.f_invjd, &cf.f_a1, &cf.f_a2, &cf.f_a3, &cf.f_b1, &cf.f_b2, &cf.f_c1, &cf.f_c2,
       &cf.f_hd1, &cf.f_hd2, &cf.f_lxl, &cf.f_lxc, &cf.f_lxu, &cf.f_lyl, &cf.f_lyc, &cf.f_lyu, &cf.f_e1, &cf.f_e2,
       &cf.c_lyx1f, &cf.c_wm, &cf.c_wp, &cf.c_invhxxf, &cf.c_invhyxc, &cf.c_invhyxf, &cf.c_lyy1, &cf.c_invjdxc,
@@ -419,7 +421,7 @@ static int check_domain(const domain_t * d) {
                   dim, d->mysizes[dim], d->glsizes[dim], d->offsets[dim]);
   }
   const size_t nx = d->glsizes[0], ny = d->glsizes[1], nz = d->glsizes[2];
-  if (nx < 2 || nx > 512) return fail("nx = %zu outside the supported range [2, 512]", nx);
+  if (nx < 2 || nx > 256) return fail("nx = %zu outside the supported range [2, 256]", nx);
   if (!is_pow2(ny) || !is_pow2(nz) || ny > 2048 || nz > 2048)
     return fail("ny = %zu and nz = %zu must be powers of two in [4, 2048]", ny, nz);
   if (!d->hxxf || !d->hxxc || !d->hyxf || !d->hyxc || !d->jdxf || !d->jdxc)
@@ -446,20 +448,30 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   auto bad = [&](const char * what) { fail("%s", what); destroy_ctx(c); return (Ctx *)nullptr; };
   if (resolve_coefs(*c)) { destroy_ctx(c); return nullptr; }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return bad("cudaStreamCreate failed");
-  c->f.ux = dalloc(*c, c->nf);
-  c->f.uy = dalloc(*c, c->nc);
-  c->f.uz = dalloc(*c, c->nc);
-  c->f.p = dalloc(*c, c->nc);
-  c->f.psi = dalloc(*c, c->nc);
-  c->f.t = dalloc(*c, c->nc);
-  if (!c->f.ux || !c->f.uy || !c->f.uz || !c->f.p || !c->f.psi || !c->f.t) return bad("cudaMalloc of fields failed");
+  double * p = dalloc(*c, c->nc);
+  double * psi = dalloc(*c, c->nc);
+  if (!p || !psi) return bad("cudaMalloc of fields failed");
+  for (int b = 0; b < 2; b++) {
+    Fields & F = c->fb[b];
+    F.ux = dalloc(*c, c->nf);
+    F.uy = dalloc(*c, c->nc);
+    F.uz = dalloc(*c, c->nc);
+    F.t = dalloc(*c, c->nc);
+    F.p = p;
+    F.psi = psi;
+    if (!F.ux || !F.uy || !F.uz || !F.t) return bad("cudaMalloc of fields failed");
+  }
   const size_t nin = (size_t)c->nx * c->ny * c->nz;
+  const bool need_delta = c->bc.implicit[1] || c->bc.implicit[2];
   for (int v = 0; v < 4; v++) {
     const size_t n = (v == VUX) ? (size_t)(c->nx - 1) * c->ny * c->nz : nin;
     c->src[v][0] = dalloc(*c, n);
     c->src[v][1] = dalloc(*c, n);
-    c->delta[v] = dalloc(*c, n);
-    if (!c->src[v][0] || !c->src[v][1] || !c->delta[v]) return bad("cudaMalloc of source terms failed");
+    if (!c->src[v][0] || !c->src[v][1]) return bad("cudaMalloc of source terms failed");
+    if (need_delta) {
+      c->ds.d[v] = dalloc(*c, n);
+      if (!c->ds.d[v]) return bad("cudaMalloc of increments failed");
+    }
   }
   c->dt_caps = dalloc(*c, 3);
   c->dtp = dalloc(*c, 1);
@@ -535,24 +547,26 @@ static void enqueue_factors(Ctx & c) {
 }
 
 static void enqueue_predict(Ctx & c, int rk) {
-  double * sn[4], * so[4];
+  SrcSet ss;
   for (int v = 0; v < 4; v++) {
-    sn[v] = s_new(c, v, rk);
-    so[v] = s_old(c, v, rk);
+    ss.new_[v] = s_new(c, v, rk);
+    ss.old_[v] = s_old(c, v, rk);
   }
-  launch_rhs_delta(c.g, c.bc, c.cf, c.nu, c.kappa, c.f, so, sn, c.delta, c.dtp, rk, c.st);
-  mark(TCGPU_K_RHS);
+  const Fields in = c.fb[c.cur];
+  const Fields out = c.fb[c.cur ^ 1];
   const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
   if (!iy && !iz) {
-    launch_xsolve(c.g, c.bc, c.xf, rk, c.bc.implicit[0] ? XS_SOLVE_APPLY : XS_APPLY, c.f, c.delta, c.st);
-    mark(TCGPU_K_XSOLVE);
-    return;
+    launch_predict(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, PREDICT_APPLY, c.st);
+    mark(TCGPU_K_PREDICT);
+  } else {
+    launch_predict(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, PREDICT_DELTA, c.st);
+    mark(TCGPU_K_PREDICT);
+    if (iy) { launch_ysolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
+    if (iz) { launch_zsolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
+    launch_apply(c.g, c.bc, in, out, c.ds, c.st);
+    mark(TCGPU_K_APPLY);
   }
-  if (c.bc.implicit[0]) { launch_xsolve(c.g, c.bc, c.xf, rk, XS_SOLVE, c.f, c.delta, c.st); mark(TCGPU_K_XSOLVE); }
-  if (iy) { launch_ysolve(c.g, c.yf, rk, c.delta, c.st); mark(TCGPU_K_YZSOLVE, 4); }
-  if (iz) { launch_zsolve(c.g, c.yf, rk, c.delta, c.st); mark(TCGPU_K_YZSOLVE, 4); }
-  launch_xsolve(c.g, c.bc, c.xf, rk, XS_APPLY, c.f, c.delta, c.st);
-  mark(TCGPU_K_XSOLVE);
+  c.cur ^= 1;
 }
 
 static void enqueue_potential(Ctx & c, int rk) {
@@ -563,16 +577,16 @@ static void enqueue_potential(Ctx & c, int rk) {
   pm.k_tdm = TCGPU_K_TDM;
   pm.k_inv = TCGPU_K_FFTZ_INV;
   pm.k_ify = TCGPU_K_IFFTY;
-  launch_poisson(c.g, c.cf, c.ps, c.f, c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st, pm);
+  launch_poisson(c.g, c.cf, c.ps, c.f(), c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st, pm);
 }
 
 static void enqueue_correct(Ctx & c, int rk, int what) {
-  launch_correct(c.g, c.bc, c.cf, c.f, c.dtp, rk, c.nu, what, c.st);
+  launch_correct(c.g, c.bc, c.cf, c.f(), c.dtp, rk, c.nu, what, c.st);
   mark(TCGPU_K_CORRECT);
 }
 
 static void enqueue_step(Ctx & c) {
-  launch_dtmin(c.g, c.f, c.dtmin, c.status, c.st);
+  launch_dtmin(c.g, c.f(), c.dtmin, c.status, c.st);
   mark(TCGPU_K_DTMIN);
   launch_dtfinal(c.coef_adv, c.dt_caps, c.dtmin, c.dtp, c.status, c.st);
   mark(TCGPU_K_DTFINAL);
@@ -585,7 +599,8 @@ static void enqueue_step(Ctx & c) {
 }
 
 static int launch_step(Ctx & c) {
-  if (c.step_graph == nullptr) {
+  const int p = c.cur;
+  if (c.step_graph[p] == nullptr) {
     cudaGraph_t graph;
     Recorder count;
     Recorder * prev = g_rec;
@@ -594,12 +609,14 @@ static int launch_step(Ctx & c) {
     enqueue_step(c);
     CK(cudaStreamEndCapture(c.st, &graph));
     g_rec = prev;
+    c.cur = p;   // capture only recorded the launches
     for (int k = 0; k < TCGPU_K_COUNT; k++) c.graph_launches[k] = count.launches[k];
-    cudaError_t e = cudaGraphInstantiate(&c.step_graph, graph, 0);
+    cudaError_t e = cudaGraphInstantiate(&c.step_graph[p], graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail("cudaGraphInstantiate failed: %s", cudaGetErrorString(e));
   }
-  CK(cudaGraphLaunch(c.step_graph, c.st));
+  CK(cudaGraphLaunch(c.step_graph[p], c.st));
+  c.cur = p ^ 1;   // three predicts per step: the state ends in the other buffer
   return 0;
 }
 
@@ -630,13 +647,14 @@ static int finish(Ctx & c, const char * what) {
 static size_t field_count(const Ctx & c, unsigned bit) { return bit == TCGPU_UX ? c.nf : c.nc; }
 
 static double * dev_field(Ctx & c, unsigned bit) {
+  const Fields & f = c.f();
   switch (bit) {
-    case TCGPU_UX: return c.f.ux;
-    case TCGPU_UY: return c.f.uy;
-    case TCGPU_UZ: return c.f.uz;
-    case TCGPU_P: return c.f.p;
-    case TCGPU_PSI: return c.f.psi;
-    default: return c.f.t;
+    case TCGPU_UX: return f.ux;
+    case TCGPU_UY: return f.uy;
+    case TCGPU_UZ: return f.uz;
+    case TCGPU_P: return f.p;
+    case TCGPU_PSI: return f.psi;
+    default: return f.t;
   }
 }
 
@@ -707,7 +725,7 @@ static int ensure_tensors(Ctx & c) {
 
 static int pull_tensors(Ctx & c, fluid_t * fl) {
   if (ensure_tensors(c)) return 1;
-  launch_tensors(c.g, c.cf, c.f, c.tn, c.st);
+  launch_tensors(c.g, c.cf, c.f(), c.tn, c.st);
   const size_t nface = (size_t)(c.nx + 1) * (c.ny + 2) * (c.nz + 2);
   const size_t ncent = (size_t)c.nx * (c.ny + 2) * (c.nz + 2);
   array_t * dst[11] = {&fl->lxx, &fl->lxy, &fl->lxz, &fl->lyx0, &fl->lyx1, &fl->lyy0, &fl->lyy1, &fl->lyz,
@@ -838,7 +856,10 @@ int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int in
   Recorder rec;
   rec.events = instrument != 0;
   rec.st = c->st;
-  if (!instrument && c->step_graph == nullptr && launch_step(*c)) return 1;   // capture outside the timing
+  if (!instrument && c->step_graph[c->cur] == nullptr) {
+    // capture both parities outside the timed region
+    if (launch_step(*c) || launch_step(*c) || finish(*c, "tcgpu_run_timed")) return 1;
+  }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -885,7 +906,7 @@ int tcgpu_set_device(int device) {
 int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
-  launch_diagnostics(c->g, c->cf, c->bc, c->f, c->nu, c->kappa, c->diag_out, c->diag_part, c->st);
+  launch_diagnostics(c->g, c->cf, c->bc, c->f(), c->nu, c->kappa, c->diag_out, c->diag_part, c->st);
   CK(cudaMemcpyAsync(c->h_scalar, c->diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   if (finish(*c, "tcgpu_diagnostics")) return 1;
   memcpy(out, c->h_scalar, 9 * sizeof(double));
@@ -908,7 +929,7 @@ int decide_dt(const domain_t * domain, const fluid_t * fluid, double * dt) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
-  launch_decide_dt(c->g, c->f, c->coef_adv, c->dt_caps, c->dtmin, c->dtp, c->status, c->st);
+  launch_decide_dt(c->g, c->f(), c->coef_adv, c->dt_caps, c->dtmin, c->dtp, c->status, c->st);
   CK(cudaMemcpyAsync(c->h_scalar, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   if (finish(*c, "decide_dt")) return 1;
   *dt = *c->h_scalar;

@@ -18,7 +18,18 @@ struct Fields {
 // Per-radial-index coefficient tables (length nx+2, indexed by the reference
 // i), computed on the host once per context with the reference's operand
 // order. f_* belong to ux at face i, c_* to the cell-centred variables at i.
+// All tables live in one allocation laid out [table][CSTRIDE] so that a
+// thread's coefficients are reached from one base pointer with compile-time
+// offsets (tab + table * CSTRIDE + i); nx + 2 <= CSTRIDE.
+constexpr int CSTRIDE = 264;
+enum CoefTable {
+  F_INVJD, F_A1, F_A2, F_A3, F_B1, F_B2, F_C1, F_C2, F_HD1, F_HD2, F_LXL, F_LXC, F_LXU, F_LYL, F_LYC, F_LYU,
+  F_E1, F_E2, C_LYX1F, C_WM, C_WP, C_INVHXXF, C_INVHYXC, C_INVHYXF, C_LYY1, C_INVJDXC, C_A1, C_A2, C_B, C_CZ,
+  C_HD, C_LXL, C_LXC, C_LXU, C_LYL, C_LYC, C_LYU, C_JF, C_E1, C_E2, C_HDA1, C_HDA2, C_PXL, C_PXU, C_PYL, C_PZL,
+  NCOEF_TABLES
+};
 struct Coefs {
+  const double * tab;      // base of the [table][CSTRIDE] block
   const double * f_invjd;  // 1 / JDXF(i)
   const double * f_a1;     // 0.5 JDXF(i-1) / HXXF(i-1)
   const double * f_a2;     // 0.5 JDXF(i)   / HXXF(i)
@@ -68,7 +79,7 @@ struct Coefs {
   double lz_l, lz_c, lz_u; // Laplacian in z
   double inv_hz;
 };
-constexpr int NCOEF_ARRAYS = 46;
+constexpr int NCOEF_ARRAYS = NCOEF_TABLES;
 
 // Radial Thomas factors for the three substeps x four variables.
 struct XFactors {
@@ -121,17 +132,26 @@ struct Poisson {
   const double * eval_z;    // -4 sin^2(pi m / nz), m < nz
 };
 
-void launch_rhs_delta(const Geo & g, const Bc & bc, const Coefs & cf, double nu, double kappa,
-                      const Fields & f, double * const s_old[4], double * const s_new[4],
-                      double * const d[4], const double * dtp, int rkstep, cudaStream_t st);
+// RK source terms of one substep: old_ (srcA of the previous substep) and new_
+struct SrcSet {
+  const double * old_[4];
+  double * new_[4];
+};
+// increments (packed interior layout), used by the planar y / z solves
+struct DeltaSet {
+  double * d[4];
+};
+enum { PREDICT_APPLY = 0, PREDICT_DELTA = 1 };
+void launch_predict(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu, double kappa,
+                    const Fields & in, const Fields & out, const SrcSet & ss, const DeltaSet & ds,
+                    const double * dtp, int rkstep, int mode, cudaStream_t st);
+int predict_warps(int nx);
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);
-enum { XS_SOLVE_APPLY = 0, XS_SOLVE = 1, XS_APPLY = 2 };
-void launch_xsolve(const Geo & g, const Bc & bc, const XFactors & xf, int rkstep, int mode,
-                   const Fields & f, double * const d[4], cudaStream_t st);
+void launch_apply(const Geo & g, const Bc & bc, const Fields & in, const Fields & out, const DeltaSet & ds,
+                  cudaStream_t st);
 void launch_yzfactors(const Geo & g, const YZFactors & yf, const double * dtp, double nu, double kappa, cudaStream_t st);
-void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st);
-void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st);
-int xsolve_elems(int nx);
+void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st);
+void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st);
 
 // optional per-launch callback of the host's kernel accounting
 struct PoissonMarks {

@@ -124,35 +124,34 @@ __global__ void __launch_bounds__(256)
 dtmin_kernel(Geo g, const double * __restrict__ ux, const double * __restrict__ uy,
              const double * __restrict__ uz, unsigned long long * dtmin, unsigned * status) {
   const double small = 1.e-8;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const long long total = (long long)nx * ny * nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   double m = 1.;
   bool bad = false;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-       c += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(c % nx) + 1;
-    const long long r = c / nx;
-    const int j = (int)(r % ny) + 1;
-    const int k = (int)(r / ny) + 1;
-    if (i >= 2) {
-      const double v = __ldg(ux + fidx(g, i, j, k));
-      bad |= !isfinite(v);
-      m = fmin(m, __ldg(g.hxxf + i) / (fabs(v) + small));
+  if (i <= g.nx && j <= g.ny) {
+    const double hx = __ldg(g.hxxf + i), hy = __ldg(g.hyxc + i), hz = g.hz;
+    for (int k = blockIdx.z + 1; k <= g.nz; k += gridDim.z) {
+      if (i >= 2) {
+        const double v = __ldg(ux + fidx(g, i, j, k));
+        bad |= !isfinite(v);
+        m = fmin(m, hx / (fabs(v) + small));
+      }
+      const double vy = __ldg(uy + cidx(g, i, j, k));
+      const double vz = __ldg(uz + cidx(g, i, j, k));
+      bad |= !isfinite(vy) || !isfinite(vz);
+      m = fmin(m, hy / (fabs(vy) + small));
+      m = fmin(m, hz / (fabs(vz) + small));
     }
-    const double vy = __ldg(uy + cidx(g, i, j, k));
-    const double vz = __ldg(uz + cidx(g, i, j, k));
-    bad |= !isfinite(vy) || !isfinite(vz);
-    m = fmin(m, __ldg(g.hyxc + i) / (fabs(vy) + small));
-    m = fmin(m, g.hz / (fabs(vz) + small));
   }
   __shared__ double red[8];
   m = warp_min(m);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = t & 31, wid = t >> 5;
   if (lane == 0) red[wid] = m;
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, (unsigned)ST_NONFINITE);
   __syncthreads();
   if (wid == 0) {
-    double v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 1.;
+    double v = (lane < 8) ? red[lane] : 1.;
     v = warp_min(v);
     if (lane == 0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
   }
@@ -172,7 +171,9 @@ __global__ void dtfinal_kernel(double coef_adv, const double * caps, unsigned lo
 }
 
 void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
-  dtmin_kernel<<<148 * 8, 256, 0, st>>>(g, f.ux, f.uy, f.uz, dtmin, status);
+  dim3 block(32, 8, 1);
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 16 ? g.nz : 16);
+  dtmin_kernel<<<grid, block, 0, st>>>(g, f.ux, f.uy, f.uz, dtmin, status);
 }
 
 void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,

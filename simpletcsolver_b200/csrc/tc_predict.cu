@@ -1,18 +1,18 @@
 // Predict stage: fluid_predict_field (src/fluid/predict/main.c:35-110).
 //
-// rhs_delta_kernel  one thread per cell (i, j, k) computes the right-hand sides
-//                   of ux (face i), uy, uz and t (centre i) in registers, the
-//                   velocity-gradient tensors they need included, and writes the
-//                   new explicit source term and the RK increment
-//                   delta = dt (alpha srcA + beta srcA_prev + gamma srcG).
-//                   srcG (implicit diffusion + pressure gradient) never leaves
-//                   registers.
+// predict_kernel    one CTA row per radial line, one thread per cell: the
+//                   right-hand sides of ux (face i), uy, uz and t (centre i) in
+//                   registers, velocity-gradient tensors included; the new
+//                   explicit source terms; the RK increment
+//                   delta = dt (alpha srcA + beta srcA_prev + gamma srcG), srcG
+//                   (implicit diffusion + pressure gradient) never leaving
+//                   registers; the radial implicit solve (src/tdm.c:17-50) as
+//                   block-wide scans of affine maps; u + delta written to the
+//                   other buffer with walls and periodic images (boundary/*.c,
+//                   halo.c). One pass over the fields per substep.
 // xfactor_kernel    line-independent Thomas factors of the radial implicit
 //                   systems (I - k L_x) for the three substeps, from dt on the device.
-// xsolve_kernel     one warp per radial line: the Thomas recurrences of
-//                   src/tdm.c:17-50 evaluated as warp-wide scans of affine maps,
-//                   then u += delta with the wall values and periodic images
-//                   (boundary/*.c, halo.c) written in the same pass.
+// apply_kernel      u + delta after the y / z solves (planar configuration).
 // ysolve/zsolve     periodic (Sherman-Morrison, src/tdm.c:66-106) solves in y
 //                   and z for the planar configuration, one thread per line.
 #include "tc_common.cuh"
@@ -22,65 +22,69 @@ namespace tcgpu {
 
 #define LD(p) __ldg(p)
 
-// ------------------------------------------------------------ rhs + delta
-__global__ void __launch_bounds__(256)
-rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
-                 const double * __restrict__ ux, const double * __restrict__ uy,
-                 const double * __restrict__ uz, const double * __restrict__ p,
-                 const double * __restrict__ t,
-                 const double * __restrict__ s_old0, const double * __restrict__ s_old1,
-                 const double * __restrict__ s_old2, const double * __restrict__ s_old3,
-                 double * __restrict__ s_new0, double * __restrict__ s_new1,
-                 double * __restrict__ s_new2, double * __restrict__ s_new3,
-                 double * __restrict__ d0, double * __restrict__ d1,
-                 double * __restrict__ d2, double * __restrict__ d3,
-                 const double * __restrict__ dtp, int rkstep) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
-  if (i > g.nx || j > g.ny) return;
+// ------------------------------------------------------------ rhs + delta of one cell
+// Right-hand sides of ux (face i), uy, uz, t (centre i), the new explicit
+// source terms (written to s_new*) and the RK increments dl[0..3]
+// (dl[0] is 0 at i = 1, where ux has no unknown). u0 returns the cell's
+// current values.
+__device__ __forceinline__ void cell_rhs_delta(
+    const Geo & g, const Bc & bc, const Coefs & cf, double nu, double kappa,
+    const double * __restrict__ ux, const double * __restrict__ uy,
+    const double * __restrict__ uz, const double * __restrict__ p,
+    const double * __restrict__ t,
+    const double * __restrict__ s_old0, const double * __restrict__ s_old1,
+    const double * __restrict__ s_old2, const double * __restrict__ s_old3,
+    double * __restrict__ s_new0, double * __restrict__ s_new1,
+    double * __restrict__ s_new2, double * __restrict__ s_new3,
+    int i, int j, int k, double ca, double cb, double cg, bool use_old,
+    double dl[4], double u0[4]) {
   const int nx = g.nx;
-  const double dt = *dtp;
-  const double ca = rk_alpha(rkstep) * dt;
-  const double cb = rk_beta(rkstep) * dt;
-  const double cg = rk_gamma(rkstep) * dt;
-  const bool use_old = rkstep != 0;
   const bool ix = bc.implicit[0], iy = bc.implicit[1], iz = bc.implicit[2];
-
-#define UXv(I, J, K) LD(ux + fidx(g, (I), (J), (K)))
-#define UYv(I, J, K) LD(uy + cidx(g, (I), (J), (K)))
-#define UZv(I, J, K) LD(uz + cidx(g, (I), (J), (K)))
-#define Pv(I, J, K)  LD(p + cidx(g, (I), (J), (K)))
-#define Tv(I, J, K)  LD(t + cidx(g, (I), (J), (K)))
-#define CF(name, I) LD(cf.name + (I))
+  dl[0] = 0.;
+  // neighbours from base pointers: (di, dj, dk) offsets with the row and
+  // plane strides of the face (ux) and centre arrays
+  const int sjf = nx + 1, skf = (nx + 1) * (g.ny + 2);
+  const int sjc = nx + 2, skc = (nx + 2) * (g.ny + 2);
+  const double * __restrict__ bx = ux + fidx(g, i, j, k);
+  const double * __restrict__ by = uy + cidx(g, i, j, k);
+  const double * __restrict__ bz = uz + cidx(g, i, j, k);
+  const double * __restrict__ bp = p + cidx(g, i, j, k);
+  const double * __restrict__ bt = t + cidx(g, i, j, k);
+  const double * __restrict__ bc_ = cf.tab + i;
+#define UXv(DI, DJ, DK) LD(bx + ((DI) + (DJ) * sjf + (DK) * skf))
+#define UYv(DI, DJ, DK) LD(by + ((DI) + (DJ) * sjc + (DK) * skc))
+#define UZv(DI, DJ, DK) LD(bz + ((DI) + (DJ) * sjc + (DK) * skc))
+#define Pv(DI, DJ, DK)  LD(bp + ((DI) + (DJ) * sjc + (DK) * skc))
+#define Tv(DI, DJ, DK)  LD(bt + ((DI) + (DJ) * sjc + (DK) * skc))
+#define CF(T, D) LD(bc_ + ((T) * CSTRIDE + (D)))
 
   // ---------------------------------------------------------------- ux at face i
   if (i >= 2) {
     double e = 0., gi = 0.;
-    const double ux_m = UXv(i - 1, j, k), ux_0 = UXv(i, j, k), ux_p = UXv(i + 1, j, k);
-    const double invj = CF(f_invjd, i);
+    const double ux_m = UXv(-1, 0, 0), ux_0 = UXv(0, 0, 0), ux_p = UXv(+1, 0, 0);
+    const double invj = CF(F_INVJD, 0);
     {  // advection_x, predict/ux.c:92-121
-      const double a1 = CF(f_a1, i), a2 = CF(f_a2, i), a3 = CF(f_a3, i);
+      const double a1 = CF(F_A1, 0), a2 = CF(F_A2, 0), a3 = CF(F_A3, 0);
       const double ux_xm = a1 * ux_m + a2 * ux_0;
       const double ux_xp = a2 * ux_0 + a3 * ux_p;
       const double l = -0.5 * ux_xm, u = 0.5 * ux_xp, c = -l - u;
       e -= invj * (l * ux_m + c * ux_0 + u * ux_p);
     }
-    const double uy_m0 = UYv(i - 1, j, k), uy_00 = UYv(i, j, k);
-    const double uy_m1 = UYv(i - 1, j + 1, k), uy_01 = UYv(i, j + 1, k);
-    const double ux_jm = UXv(i, j - 1, k), ux_jp = UXv(i, j + 1, k);
+    const double uy_m0 = UYv(-1, 0, 0), uy_00 = UYv(0, 0, 0);
+    const double uy_m1 = UYv(-1, +1, 0), uy_01 = UYv(0, +1, 0);
+    const double ux_jm = UXv(0, -1, 0), ux_jp = UXv(0, +1, 0);
     {  // advection_y :123-155
-      const double b1 = CF(f_b1, i), b2 = CF(f_b2, i);
+      const double b1 = CF(F_B1, 0), b2 = CF(F_B2, 0);
       const double uy_ym = b1 * uy_m0 + b2 * uy_00;
       const double uy_yp = b1 * uy_m1 + b2 * uy_01;
       const double l = -0.5 * uy_ym, u = 0.5 * uy_yp, c = -l - u;
       e -= invj * (l * ux_jm + c * ux_0 + u * ux_jp);
     }
-    const double uz_m0 = UZv(i - 1, j, k), uz_00 = UZv(i, j, k);
-    const double uz_m1 = UZv(i - 1, j, k + 1), uz_01 = UZv(i, j, k + 1);
-    const double ux_km = UXv(i, j, k - 1), ux_kp = UXv(i, j, k + 1);
+    const double uz_m0 = UZv(-1, 0, 0), uz_00 = UZv(0, 0, 0);
+    const double uz_m1 = UZv(-1, 0, +1), uz_01 = UZv(0, 0, +1);
+    const double ux_km = UXv(0, 0, -1), ux_kp = UXv(0, 0, +1);
     {  // advection_z :157-186
-      const double c1 = CF(f_c1, i), c2 = CF(f_c2, i);
+      const double c1 = CF(F_C1, 0), c2 = CF(F_C2, 0);
       const double uz_zm = c1 * uz_m0 + c2 * uz_00;
       const double uz_zp = c1 * uz_m1 + c2 * uz_01;
       const double l = -0.5 * uz_zm, u = 0.5 * uz_zp, c = -l - u;
@@ -89,24 +93,24 @@ rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
     {  // advection_1 (centrifugal) :194-226
       const double uy_xm = 0.5 * uy_m0 + 0.5 * uy_m1;
       const double uy_xp = 0.5 * uy_00 + 0.5 * uy_01;
-      e += invj * (CF(f_hd1, i) * uy_xm * uy_xm + CF(f_hd2, i) * uy_xp * uy_xp);
+      e += invj * (CF(F_HD1, 0) * uy_xm * uy_xm + CF(F_HD2, 0) * uy_xp * uy_xp);
     }
     {  // diffusion_x :228-245
-      const double v = 2. * nu * (CF(f_lxl, i) * ux_m + CF(f_lxc, i) * ux_0 + CF(f_lxu, i) * ux_p);
+      const double v = 2. * nu * (CF(F_LXL, 0) * ux_m + CF(F_LXC, 0) * ux_0 + CF(F_LXU, 0) * ux_p);
       if (ix) gi += v; else e += v;
     }
     {  // diffusion_y0 :247-264
-      const double v = nu * (CF(f_lyl, i) * ux_jm + CF(f_lyc, i) * ux_0 + CF(f_lyu, i) * ux_jp);
+      const double v = nu * (CF(F_LYL, 0) * ux_jm + CF(F_LYC, 0) * ux_0 + CF(F_LYU, 0) * ux_jp);
       if (iy) gi += v; else e += v;
     }
     const double njd = nu * invj;
     {  // diffusion_y1 :266-290, with lyx1 (lyx.c:64-83) and lxy (lxy.c:28-34)
-      const double F = CF(c_lyx1f, i), wm = CF(c_wm, i), wp = CF(c_wp, i), ih = CF(c_invhxxf, i);
+      const double F = CF(C_LYX1F, 0), wm = CF(C_WM, 0), wp = CF(C_WP, 0), ih = CF(C_INVHXXF, 0);
       const double lyx1_m = F * (wm * uy_m0 + wp * uy_00);
       const double lyx1_p = F * (wm * uy_m1 + wp * uy_01);
       const double lxy_m = ih * (-uy_m0 + uy_00);
       const double lxy_p = ih * (-uy_m1 + uy_01);
-      const double jh = CF(f_e1, i);
+      const double jh = CF(F_E1, 0);
       e += njd * (-jh * (lyx1_m + lxy_m) + jh * (lyx1_p + lxy_p));
     }
     {  // diffusion_z0 :292-309
@@ -114,53 +118,56 @@ rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
       if (iz) gi += v; else e += v;
     }
     {  // diffusion_z1 :311-332, lxz (lxz.c:19-27)
-      const double ih = CF(c_invhxxf, i), jh = CF(f_e2, i);
+      const double ih = CF(C_INVHXXF, 0), jh = CF(F_E2, 0);
       const double lxz_m = ih * (-uz_m0 + uz_00);
       const double lxz_p = ih * (-uz_m1 + uz_01);
       e += njd * (-jh * lxz_m + jh * lxz_p);
     }
     {  // diffusion_a :344-375, lyy0/lyy1 (lyy.c) at centres i-1 and i
-      const double lyy_xm = CF(c_invhyxc, i - 1) * (-uy_m0 + uy_m1) + CF(c_lyy1, i - 1) * (0.5 * ux_m + 0.5 * ux_0);
-      const double lyy_xp = CF(c_invhyxc, i) * (-uy_00 + uy_01) + CF(c_lyy1, i) * (0.5 * ux_0 + 0.5 * ux_p);
-      e -= 2. * njd * (CF(f_hd1, i) * lyy_xm + CF(f_hd2, i) * lyy_xp);
+      const double lyy_xm = CF(C_INVHYXC, -1) * (-uy_m0 + uy_m1) + CF(C_LYY1, -1) * (0.5 * ux_m + 0.5 * ux_0);
+      const double lyy_xp = CF(C_INVHYXC, 0) * (-uy_00 + uy_01) + CF(C_LYY1, 0) * (0.5 * ux_0 + 0.5 * ux_p);
+      e -= 2. * njd * (CF(F_HD1, 0) * lyy_xm + CF(F_HD2, 0) * lyy_xp);
     }
     // pressure :377-394
-    gi -= CF(c_invhxxf, i) * (-Pv(i - 1, j, k) + Pv(i, j, k));
+    gi -= CF(C_INVHXXF, 0) * (-Pv(-1, 0, 0) + Pv(0, 0, 0));
     const size_t q = pidx(nx - 1, g.ny, i - 2, j, k);
     const double old = use_old ? s_old0[q] : 0.;
     s_new0[q] = e;
-    d0[q] = ca * e + cb * old + cg * gi;
+    dl[0] = ca * e + cb * old + cg * gi;
   }
 
   // ---------------------------------------------------------------- uy at centre i
-  const double uy_0 = UYv(i, j, k);
-  const double uy_im = UYv(i - 1, j, k), uy_ip = UYv(i + 1, j, k);
-  const double uy_jm = UYv(i, j - 1, k), uy_jp = UYv(i, j + 1, k);
-  const double uy_km = UYv(i, j, k - 1), uy_kp = UYv(i, j, k + 1);
-  const double ux_0 = UXv(i, j, k), ux_1 = UXv(i + 1, j, k);          // faces i, i+1 at j
-  const double ux_0m = UXv(i, j - 1, k), ux_1m = UXv(i + 1, j - 1, k); // at j-1
-  const double ux_0k = UXv(i, j, k - 1), ux_1k = UXv(i + 1, j, k - 1); // at k-1
-  const double uz_0 = UZv(i, j, k), uz_kp = UZv(i, j, k + 1);
-  const double uz_jm = UZv(i, j - 1, k), uz_jmkp = UZv(i, j - 1, k + 1);
-  const double invjc = CF(c_invjdxc, i);
+  const double uy_0 = UYv(0, 0, 0);
+  const double uy_im = UYv(-1, 0, 0), uy_ip = UYv(+1, 0, 0);
+  const double uy_jm = UYv(0, -1, 0), uy_jp = UYv(0, +1, 0);
+  const double uy_km = UYv(0, 0, -1), uy_kp = UYv(0, 0, +1);
+  const double ux_0 = UXv(0, 0, 0), ux_1 = UXv(+1, 0, 0);          // faces i, i+1 at j
+  const double ux_0m = UXv(0, -1, 0), ux_1m = UXv(+1, -1, 0); // at j-1
+  const double ux_0k = UXv(0, 0, -1), ux_1k = UXv(+1, 0, -1); // at k-1
+  const double uz_0 = UZv(0, 0, 0), uz_kp = UZv(0, 0, +1);
+  const double uz_jm = UZv(0, -1, 0), uz_jmkp = UZv(0, -1, +1);
+  const double invjc = CF(C_INVJDXC, 0);
   const double njc = nu * invjc;
+  u0[0] = ux_0;
+  u0[1] = uy_0;
+  u0[2] = uz_0;
   {
     double e = 0., gi = 0.;
-    const double a1 = CF(c_a1, i), a2 = CF(c_a2, i);
+    const double a1 = CF(C_A1, 0), a2 = CF(C_A2, 0);
     {  // advection_x, predict/uy.c:93-123
       const double ux_xm = a1 * ux_0m + a1 * ux_0;
       const double ux_xp = a2 * ux_1m + a2 * ux_1;
       const double l = -0.5 * ux_xm, u = 0.5 * ux_xp, c = -l - u;
       e -= invjc * (l * uy_im + c * uy_0 + u * uy_ip);
     }
-    const double b = CF(c_b, i);
+    const double b = CF(C_B, 0);
     {  // advection_y :125-151
       const double uy_ym = b * uy_jm + b * uy_0;
       const double uy_yp = b * uy_0 + b * uy_jp;
       const double l = -0.5 * uy_ym, u = 0.5 * uy_yp, c = -l - u;
       e -= invjc * (l * uy_jm + c * uy_0 + u * uy_jp);
     }
-    const double cz = CF(c_cz, i);
+    const double cz = CF(C_CZ, 0);
     {  // advection_z :153-180
       const double uz_zm = cz * uz_jm + cz * uz_0;
       const double uz_zp = cz * uz_jmkp + cz * uz_kp;
@@ -172,32 +179,32 @@ rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
       const double uy_yp = 0.5 * uy_0 + 0.5 * uy_jp;
       const double ux_ym = 0.5 * ux_0m + 0.5 * ux_1m;
       const double ux_yp = 0.5 * ux_0 + 0.5 * ux_1;
-      const double hd = CF(c_hd, i);
+      const double hd = CF(C_HD, 0);
       e -= invjc * (hd * uy_ym * ux_ym + hd * uy_yp * ux_yp);
     }
     {  // diffusion_x0
-      const double v = nu * (CF(c_lxl, i) * uy_im + CF(c_lxc, i) * uy_0 + CF(c_lxu, i) * uy_ip);
+      const double v = nu * (CF(C_LXL, 0) * uy_im + CF(C_LXC, 0) * uy_0 + CF(C_LXU, 0) * uy_ip);
       if (ix) gi += v; else e += v;
     }
     // lyx0 (lyx.c:33-39), lyx1 (:64-83), lxy (lxy.c) at faces i and i+1
-    const double lyx0_m = CF(c_invhyxf, i) * (-ux_0m + ux_0);
-    const double lyx0_p = CF(c_invhyxf, i + 1) * (-ux_1m + ux_1);
-    const double lyx1_m = CF(c_lyx1f, i) * (CF(c_wm, i) * uy_im + CF(c_wp, i) * uy_0);
-    const double lyx1_p = CF(c_lyx1f, i + 1) * (CF(c_wm, i + 1) * uy_0 + CF(c_wp, i + 1) * uy_ip);
+    const double lyx0_m = CF(C_INVHYXF, 0) * (-ux_0m + ux_0);
+    const double lyx0_p = CF(C_INVHYXF, +1) * (-ux_1m + ux_1);
+    const double lyx1_m = CF(C_LYX1F, 0) * (CF(C_WM, 0) * uy_im + CF(C_WP, 0) * uy_0);
+    const double lyx1_p = CF(C_LYX1F, +1) * (CF(C_WM, +1) * uy_0 + CF(C_WP, +1) * uy_ip);
     const double lyx_xm = lyx0_m + lyx1_m;
     const double lyx_xp = lyx0_p + lyx1_p;
-    const double jfm = CF(c_jf, i), jfp = CF(c_jf, i + 1);
+    const double jfm = CF(C_JF, 0), jfp = CF(C_JF, +1);
     // diffusion_x1
     e += njc * (-jfm * lyx_xm + jfp * lyx_xp);
     {  // diffusion_y0
-      const double v = 2. * nu * (CF(c_lyl, i) * uy_jm + CF(c_lyc, i) * uy_0 + CF(c_lyu, i) * uy_jp);
+      const double v = 2. * nu * (CF(C_LYL, 0) * uy_jm + CF(C_LYC, 0) * uy_0 + CF(C_LYU, 0) * uy_jp);
       if (iy) gi += v; else e += v;
     }
     {  // diffusion_y1, lyy1 (lyy.c:64-83) at j-1 and j
-      const double K = CF(c_lyy1, i);
+      const double K = CF(C_LYY1, 0);
       const double lyy1_m = K * (0.5 * ux_0m + 0.5 * ux_1m);
       const double lyy1_0 = K * (0.5 * ux_0 + 0.5 * ux_1);
-      const double jh = CF(c_e1, i);
+      const double jh = CF(C_E1, 0);
       e += 2. * njc * (-jh * lyy1_m + jh * lyy1_0);
     }
     {  // diffusion_z0
@@ -205,116 +212,117 @@ rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
       if (iz) gi += v; else e += v;
     }
     {  // diffusion_z1, lyz (lyz.c:19-27) at k and k+1
-      const double ih = CF(c_invhyxc, i);
+      const double ih = CF(C_INVHYXC, 0);
       const double lyz_0 = ih * (-uz_jm + uz_0);
       const double lyz_p = ih * (-uz_jmkp + uz_kp);
-      const double jh = CF(c_e2, i);
+      const double jh = CF(C_E2, 0);
       e += njc * (-jh * lyz_0 + jh * lyz_p);
     }
     {  // diffusion_a :367-400
-      const double lxy_m = CF(c_invhxxf, i) * (-uy_im + uy_0);
-      const double lxy_p = CF(c_invhxxf, i + 1) * (-uy_0 + uy_ip);
-      e += njc * (CF(c_hda1, i) * (lyx_xm + lxy_m) + CF(c_hda2, i) * (lyx_xp + lxy_p));
+      const double lxy_m = CF(C_INVHXXF, 0) * (-uy_im + uy_0);
+      const double lxy_p = CF(C_INVHXXF, +1) * (-uy_0 + uy_ip);
+      e += njc * (CF(C_HDA1, 0) * (lyx_xm + lxy_m) + CF(C_HDA2, 0) * (lyx_xp + lxy_p));
     }
-    gi -= CF(c_invhyxc, i) * (-Pv(i, j - 1, k) + Pv(i, j, k));
+    gi -= CF(C_INVHYXC, 0) * (-Pv(0, -1, 0) + Pv(0, 0, 0));
     const size_t q = pidx(nx, g.ny, i - 1, j, k);
     const double old = use_old ? s_old1[q] : 0.;
     s_new1[q] = e;
-    d1[q] = ca * e + cb * old + cg * gi;
+    dl[1] = ca * e + cb * old + cg * gi;
   }
 
   // ---------------------------------------------------------------- uz at centre i
   {
     double e = 0., gi = 0.;
-    const double uz_im = UZv(i - 1, j, k), uz_ip = UZv(i + 1, j, k);
-    const double uz_jp = UZv(i, j + 1, k), uz_km = UZv(i, j, k - 1);
-    const double uy_jpkm = UYv(i, j + 1, k - 1);
+    const double uz_im = UZv(-1, 0, 0), uz_ip = UZv(+1, 0, 0);
+    const double uz_jp = UZv(0, +1, 0), uz_km = UZv(0, 0, -1);
+    const double uy_jpkm = UYv(0, +1, -1);
     {  // advection_x, predict/uz.c:88-118
-      const double a1 = CF(c_a1, i), a2 = CF(c_a2, i);
+      const double a1 = CF(C_A1, 0), a2 = CF(C_A2, 0);
       const double ux_xm = a1 * ux_0k + a1 * ux_0;
       const double ux_xp = a2 * ux_1k + a2 * ux_1;
       const double l = -0.5 * ux_xm, u = 0.5 * ux_xp, c = -l - u;
       e -= invjc * (l * uz_im + c * uz_0 + u * uz_ip);
     }
     {  // advection_y
-      const double b = CF(c_b, i);
+      const double b = CF(C_B, 0);
       const double uy_ym = b * uy_km + b * uy_0;
       const double uy_yp = b * uy_jpkm + b * uy_jp;
       const double l = -0.5 * uy_ym, u = 0.5 * uy_yp, c = -l - u;
       e -= invjc * (l * uz_jm + c * uz_0 + u * uz_jp);
     }
     {  // advection_z
-      const double cz = CF(c_cz, i);
+      const double cz = CF(C_CZ, 0);
       const double uz_zm = cz * uz_km + cz * uz_0;
       const double uz_zp = cz * uz_0 + cz * uz_kp;
       const double l = -0.5 * uz_zm, u = 0.5 * uz_zp, c = -l - u;
       e -= invjc * (l * uz_km + c * uz_0 + u * uz_kp);
     }
     {  // diffusion_x0
-      const double v = nu * (CF(c_lxl, i) * uz_im + CF(c_lxc, i) * uz_0 + CF(c_lxu, i) * uz_ip);
+      const double v = nu * (CF(C_LXL, 0) * uz_im + CF(C_LXC, 0) * uz_0 + CF(C_LXU, 0) * uz_ip);
       if (ix) gi += v; else e += v;
     }
     {  // diffusion_x1, lzx (lzx.c) at faces i, i+1
       const double ihz = cf.inv_hz;
       const double lzx_m = ihz * (-ux_0k + ux_0);
       const double lzx_p = ihz * (-ux_1k + ux_1);
-      e += njc * (-CF(c_jf, i) * lzx_m + CF(c_jf, i + 1) * lzx_p);
+      e += njc * (-CF(C_JF, 0) * lzx_m + CF(C_JF, +1) * lzx_p);
     }
     {  // diffusion_y0
-      const double v = nu * (CF(c_lyl, i) * uz_jm + CF(c_lyc, i) * uz_0 + CF(c_lyu, i) * uz_jp);
+      const double v = nu * (CF(C_LYL, 0) * uz_jm + CF(C_LYC, 0) * uz_0 + CF(C_LYU, 0) * uz_jp);
       if (iy) gi += v; else e += v;
     }
     {  // diffusion_y1, lzy (lzy.c) at j, j+1
       const double ihz = cf.inv_hz;
       const double lzy_0 = ihz * (-uy_km + uy_0);
       const double lzy_p = ihz * (-uy_jpkm + uy_jp);
-      const double jh = CF(c_e1, i);
+      const double jh = CF(C_E1, 0);
       e += njc * (-jh * lzy_0 + jh * lzy_p);
     }
     {  // diffusion_z
       const double v = 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp);
       if (iz) gi += v; else e += v;
     }
-    gi -= cf.inv_hz * (-Pv(i, j, k - 1) + Pv(i, j, k));
+    gi -= cf.inv_hz * (-Pv(0, 0, -1) + Pv(0, 0, 0));
     const size_t q = pidx(nx, g.ny, i - 1, j, k);
     const double old = use_old ? s_old2[q] : 0.;
     s_new2[q] = e;
-    d2[q] = ca * e + cb * old + cg * gi;
+    dl[2] = ca * e + cb * old + cg * gi;
   }
 
   // ---------------------------------------------------------------- t at centre i
   {
     double e = 0., gi = 0.;
-    const double t0 = Tv(i, j, k);
-    const double tim = Tv(i - 1, j, k), tip = Tv(i + 1, j, k);
-    const double tjm = Tv(i, j - 1, k), tjp = Tv(i, j + 1, k);
-    const double tkm = Tv(i, j, k - 1), tkp = Tv(i, j, k + 1);
+    const double t0 = Tv(0, 0, 0);
+    const double tim = Tv(-1, 0, 0), tip = Tv(+1, 0, 0);
+    const double tjm = Tv(0, -1, 0), tjp = Tv(0, +1, 0);
+    const double tkm = Tv(0, 0, -1), tkp = Tv(0, 0, +1);
+    u0[3] = t0;
     {  // advection_x, predict/t.c:88-116
-      const double ux_xm = CF(c_jf, i) * ux_0;
-      const double ux_xp = CF(c_jf, i + 1) * ux_1;
+      const double ux_xm = CF(C_JF, 0) * ux_0;
+      const double ux_xp = CF(C_JF, +1) * ux_1;
       const double l = -0.5 * ux_xm, u = 0.5 * ux_xp, c = -l - u;
       e -= invjc * (l * tim + c * t0 + u * tip);
     }
     {  // advection_y
-      const double jh = CF(c_e1, i);
+      const double jh = CF(C_E1, 0);
       const double uy_ym = jh * uy_0;
       const double uy_yp = jh * uy_jp;
       const double l = -0.5 * uy_ym, u = 0.5 * uy_yp, c = -l - u;
       e -= invjc * (l * tjm + c * t0 + u * tjp);
     }
     {  // advection_z
-      const double jh = CF(c_e2, i);
+      const double jh = CF(C_E2, 0);
       const double uz_zm = jh * uz_0;
       const double uz_zp = jh * uz_kp;
       const double l = -0.5 * uz_zm, u = 0.5 * uz_zp, c = -l - u;
       e -= invjc * (l * tkm + c * t0 + u * tkp);
     }
     {
-      const double v = kappa * (CF(c_lxl, i) * tim + CF(c_lxc, i) * t0 + CF(c_lxu, i) * tip);
+      const double v = kappa * (CF(C_LXL, 0) * tim + CF(C_LXC, 0) * t0 + CF(C_LXU, 0) * tip);
       if (ix) gi += v; else e += v;
     }
     {
-      const double v = kappa * (CF(c_lyl, i) * tjm + CF(c_lyc, i) * t0 + CF(c_lyu, i) * tjp);
+      const double v = kappa * (CF(C_LYL, 0) * tjm + CF(C_LYC, 0) * t0 + CF(C_LYU, 0) * tjp);
       if (iy) gi += v; else e += v;
     }
     {
@@ -324,7 +332,7 @@ rhs_delta_kernel(Geo g, Bc bc, Coefs cf, double nu, double kappa,
     const size_t q = pidx(nx, g.ny, i - 1, j, k);
     const double old = use_old ? s_old3[q] : 0.;
     s_new3[q] = e;
-    d3[q] = ca * e + cb * old + cg * gi;
+    dl[3] = ca * e + cb * old + cg * gi;
   }
 #undef UXv
 #undef UYv
@@ -379,169 +387,223 @@ __global__ void xfactor_kernel(XFactors xf, const double * __restrict__ dtp, dou
   }
 }
 
-// ------------------------------------------------------------ radial solve + update
-// Affine map composition q -> A q + B. compose(first, then).
+// ------------------------------------------------------------ fused predict
+// Affine map q -> a q + b; compositions of the Thomas recurrences.
 struct Aff { double a, b; };
 
-__device__ inline void shfl_up_aff(Aff & x, int off) {
-  x.a = __shfl_up_sync(0xffffffffu, x.a, off);
-  x.b = __shfl_up_sync(0xffffffffu, x.b, off);
-}
-__device__ inline void shfl_down_aff(Aff & x, int off) {
-  x.a = __shfl_down_sync(0xffffffffu, x.a, off);
-  x.b = __shfl_down_sync(0xffffffffu, x.b, off);
-}
-
 template <int E>
-__device__ inline int spad(int e) { return E > 1 ? e + e / E : e; }
+__device__ __forceinline__ int spad(int e) { return E > 1 ? e + e / E : e; }
 
-// One warp per (line, variable). Lines: (j, k) interior; var picks the field.
-// With SOLVE the radial Thomas system is solved first (implicit x). With APPLY
-// the increment is then added and the row's walls and periodic images written;
-// without it the solved increment goes back to the delta buffer (for the y/z
-// solves that follow in the planar configuration, linear_system.c order).
-template <int E, bool SOLVE, bool APPLY>
-__global__ void __launch_bounds__(256)
-xsolve_kernel(Geo g, Bc bc, XFactors xf, int rkstep, int var_lo,
-              double * __restrict__ ux, double * __restrict__ uy,
-              double * __restrict__ uz, double * __restrict__ t,
-              const double * __restrict__ d0, const double * __restrict__ d1,
-              const double * __restrict__ d2, const double * __restrict__ d3) {
-  constexpr int WARPS = 8;
-  constexpr int SLEN = 32 * E + (E > 1 ? 32 : 0);
-  __shared__ double sbuf[WARPS][SLEN];
-  const int lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5;
-  const long long line = (long long)blockIdx.x * WARPS + wid;
-  const int ny = g.ny, nz = g.nz, nx = g.nx;
-  const long long nlines = (long long)ny * nz;
-  const int var = var_lo + blockIdx.y;
-  if (line >= nlines) return;
-  const int j = (int)(line % ny) + 1;
-  const int k = (int)(line / ny) + 1;
+// Radial Thomas solve of one line by one warp (src/tdm.c:24-48), the line held
+// in shared memory (padded by one slot per E elements against bank
+// conflicts). Lane t owns elements tE .. tE+E-1: it composes their affine maps,
+// a 5-level shuffle scan supplies the value entering its chunk, then the
+// recurrence runs in the reference's form q = w (r - l q_prev) (forward) and
+// x = q - v x_next (backward).
+template <int E>
+__device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int rkstep, int var, int lane) {
   const int n = xf.n[var];
-  double * dsrc = const_cast<double *>(var == VUX ? d0 : var == VUY ? d1 : var == VUZ ? d2 : d3);
-  double * drow = dsrc + (size_t)n * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
-  double * sb = sbuf[wid];
-  for (int r = 0; r < E; r++) {
-    const int e = lane + 32 * r;
-    if (e < n) sb[spad<E>(e)] = drow[e];
+  const size_t fo = (size_t)(rkstep * 4 + var) * xf.stride;
+  const double * __restrict__ lo = xf.lo + fo;
+  const double * __restrict__ w = xf.w + fo;
+  const double * __restrict__ v = xf.v + fo;
+  double q[E], ll[E], ww[E];
+#pragma unroll
+  for (int m = 0; m < E; m++) {
+    const int e = lane * E + m;
+    const bool el = e < n;
+    q[m] = el ? sb[spad<E>(e)] : 0.;
+    ll[m] = el ? LD(lo + e) : 0.;
+    ww[m] = el ? LD(w + e) : 0.;
   }
-  __syncwarp();
-  if (SOLVE) {
-    const size_t fo = (size_t)(rkstep * 4 + var) * xf.stride;
-    const double * lo = xf.lo + fo;
-    const double * w = xf.w + fo;
-    const double * v = xf.v + fo;
-    double q[E];
+  Aff acc{1., 0.};
 #pragma unroll
-    for (int m = 0; m < E; m++) {
-      const int e = lane * E + m;
-      q[m] = (e < n) ? sb[spad<E>(e)] : 0.;
-    }
-    // forward: q_0 = r_0 / c_0; q_e = w_e (r_e - l_e q_{e-1})
-    Aff acc{1., 0.};
-#pragma unroll
-    for (int m = 0; m < E; m++) {
-      const int e = lane * E + m;
-      Aff f;
-      if (e == 0) { f.a = 0.; f.b = q[m] / LD(w); }
-      else if (e < n) { const double we = LD(w + e); f.a = -we * LD(lo + e); f.b = we * q[m]; }
-      else { f.a = 0.; f.b = 0.; }
-      acc.b = f.a * acc.b + f.b;
-      acc.a = f.a * acc.a;
-    }
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      Aff o = acc;
-      shfl_up_aff(o, off);
-      if (lane >= off) { acc.b = acc.a * o.b + acc.b; acc.a = acc.a * o.a; }
-    }
-    double qin = __shfl_up_sync(0xffffffffu, acc.b, 1);
-    if (lane == 0) qin = 0.;
-#pragma unroll
-    for (int m = 0; m < E; m++) {
-      const int e = lane * E + m;
-      double r;
-      if (e == 0) r = q[m] / LD(w);
-      else if (e < n) r = LD(w + e) * (q[m] - LD(lo + e) * qin);
-      else r = 0.;
-      q[m] = r;
-      qin = r;
-    }
-    // backward: x_e = q_e - v_e x_{e+1}
-    Aff bac{1., 0.};
-#pragma unroll
-    for (int m = E - 1; m >= 0; m--) {
-      const int e = lane * E + m;
-      Aff f;
-      if (e < n) { f.a = -LD(v + e); f.b = q[m]; } else { f.a = 0.; f.b = 0.; }
-      bac.b = f.a * bac.b + f.b;
-      bac.a = f.a * bac.a;
-    }
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      Aff o = bac;
-      shfl_down_aff(o, off);
-      if (lane + off < 32) { bac.b = bac.a * o.b + bac.b; bac.a = bac.a * o.a; }
-    }
-    double xin = __shfl_down_sync(0xffffffffu, bac.b, 1);
-    if (lane == 31) xin = 0.;
-#pragma unroll
-    for (int m = E - 1; m >= 0; m--) {
-      const int e = lane * E + m;
-      double x = 0.;
-      if (e < n) x = q[m] - LD(v + e) * xin;
-      q[m] = x;
-      xin = x;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int m = 0; m < E; m++) {
-      const int e = lane * E + m;
-      if (e < n) sb[spad<E>(e)] = q[m];
-    }
-    __syncwarp();
+  for (int m = 0; m < E; m++) {
+    const int e = lane * E + m;
+    double fa, fb;
+    if (e == 0) { fa = 0.; fb = q[m] / ww[m]; }          // w[0] holds c[0]
+    else if (e < n) { fa = -ww[m] * ll[m]; fb = ww[m] * q[m]; }
+    else { fa = 0.; fb = 0.; }
+    acc.b = fa * acc.b + fb;
+    acc.a = fa * acc.a;
   }
-  if (!APPLY) {
-    for (int r = 0; r < E; r++) {
-      const int e = lane + 32 * r;
-      if (e < n) drow[e] = sb[spad<E>(e)];
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double oa = __shfl_up_sync(0xffffffffu, acc.a, off);
+    const double ob = __shfl_up_sync(0xffffffffu, acc.b, off);
+    if (lane >= off) { acc.b = acc.a * ob + acc.b; acc.a = acc.a * oa; }
+  }
+  double qin = __shfl_up_sync(0xffffffffu, acc.b, 1);
+  if (lane == 0) qin = 0.;
+#pragma unroll
+  for (int m = 0; m < E; m++) {
+    const int e = lane * E + m;
+    double r;
+    if (e == 0) r = q[m] / ww[m];
+    else if (e < n) r = ww[m] * (q[m] - ll[m] * qin);
+    else r = 0.;
+    q[m] = r;
+    qin = r;
+  }
+  double vv[E];
+  Aff bac{1., 0.};
+#pragma unroll
+  for (int m = E - 1; m >= 0; m--) {
+    const int e = lane * E + m;
+    vv[m] = (e < n) ? LD(v + e) : 0.;
+    const double fa = (e < n) ? -vv[m] : 0.;
+    const double fb = (e < n) ? q[m] : 0.;
+    bac.b = fa * bac.b + fb;
+    bac.a = fa * bac.a;
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double oa = __shfl_down_sync(0xffffffffu, bac.a, off);
+    const double ob = __shfl_down_sync(0xffffffffu, bac.b, off);
+    if (lane + off < 32) { bac.b = bac.a * ob + bac.b; bac.a = bac.a * oa; }
+  }
+  double xin = __shfl_down_sync(0xffffffffu, bac.b, 1);
+  if (lane == 31) xin = 0.;
+#pragma unroll
+  for (int m = E - 1; m >= 0; m--) {
+    const int e = lane * E + m;
+    const double x = (e < n) ? q[m] - vv[m] * xin : 0.;
+    if (e < n) sb[spad<E>(e)] = x;
+    xin = x;
+  }
+}
+
+// One CTA row per radial line (j, k), one thread per radial index i. Each
+// thread computes the four right-hand sides and increments of its cell; the
+// increments are staged in shared memory and the radial implicit systems of
+// the CTA's lines are solved one per warp (line-independent factors from
+// xfactor_kernel). The new fields go to the other buffer of the pair (the old
+// ones are still read by neighbouring lines), walls and periodic images
+// included. PREDICT_DELTA writes the radially solved increments instead, for
+// the y and z solves of the planar configuration.
+#ifndef TC_PREDICT_MIN_BLOCKS
+#define TC_PREDICT_MIN_BLOCKS 4
+#endif
+template <int NW>   // warps per line; also the elements per lane of the solves
+__global__ void __launch_bounds__(256, TC_PREDICT_MIN_BLOCKS)
+predict_kernel(Geo g, Bc bc, Coefs cf, XFactors xf, double nu, double kappa,
+               Fields in, Fields out, SrcSet ss, DeltaSet ds, const double * __restrict__ dtp,
+               int rkstep, int mode) {
+  constexpr int NT = 32 * NW;
+  constexpr int LPB = 256 / NT;
+  constexpr int E = NW;
+  constexpr int SL = 32 * E + (E > 1 ? 32 : 0);
+  __shared__ double sd[LPB][4][SL];
+  const int tx = threadIdx.x;
+  const int ly = threadIdx.y;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const long long nlines = (long long)ny * nz;
+  const long long line = (long long)blockIdx.x * LPB + ly;
+  const bool vline = line < nlines;
+  const int j = vline ? (int)(line % ny) + 1 : 1;
+  const int k = vline ? (int)(line / ny) + 1 : 1;
+  const int i = tx + 1;
+  const bool cell = vline && i <= nx;
+  const double dt = *dtp;
+  const double ca = rk_alpha(rkstep) * dt;
+  const double cb = rk_beta(rkstep) * dt;
+  const double cg = rk_gamma(rkstep) * dt;
+  double dl[4] = {0., 0., 0., 0.}, u0[4] = {0., 0., 0., 0.};
+  if (cell) {
+    cell_rhs_delta(g, bc, cf, nu, kappa, in.ux, in.uy, in.uz, in.p, in.t,
+                   ss.old_[0], ss.old_[1], ss.old_[2], ss.old_[3], ss.new_[0], ss.new_[1], ss.new_[2], ss.new_[3],
+                   i, j, k, ca, cb, cg, rkstep != 0, dl, u0);
+  }
+  if (bc.implicit[0]) {
+    if (cell) {
+      if (i >= 2) sd[ly][VUX][spad<E>(i - 2)] = dl[VUX];
+      sd[ly][VUY][spad<E>(i - 1)] = dl[VUY];
+      sd[ly][VUZ][spad<E>(i - 1)] = dl[VUZ];
+      sd[ly][VT][spad<E>(i - 1)] = dl[VT];
     }
+    __syncthreads();
+    const int wid = (ly * NT + tx) >> 5;
+    const int lane = tx & 31;
+    for (int s = wid; s < 4 * LPB; s += 8) {
+      const int l = s >> 2, v = s & 3;
+      if ((long long)blockIdx.x * LPB + l >= nlines) continue;
+      solve_line<E>(sd[l][v], xf, rkstep, v, lane);
+    }
+    __syncthreads();
+    if (cell) {
+      dl[VUX] = (i >= 2) ? sd[ly][VUX][spad<E>(i - 2)] : 0.;
+      dl[VUY] = sd[ly][VUY][spad<E>(i - 1)];
+      dl[VUZ] = sd[ly][VUZ][spad<E>(i - 1)];
+      dl[VT] = sd[ly][VT][spad<E>(i - 1)];
+    }
+  }
+  if (!cell) return;
+  if (mode == PREDICT_DELTA) {
+    if (i >= 2) ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] = dl[VUX];
+    const size_t qc = pidx(nx, ny, i - 1, j, k);
+    ds.d[VUY][qc] = dl[VUY];
+    ds.d[VUZ][qc] = dl[VUZ];
+    ds.d[VT][qc] = dl[VT];
     return;
   }
-  // u += delta over the row, walls, periodic images
-  if (var == VUX) {
-    double * row = ux + fidx(g, 1, j, k);
-    for (int r = 0; r < E + 1; r++) {
-      const int e = lane + 32 * r;          // e -> i = e + 1, i = 1..nx+1
-      if (e > nx) break;
-      double val;
-      if (e == 0 || e == nx) val = 0.;      // boundary/ux.c:24-26
-      else val = row[e] + sb[spad<E>(e - 1)];
-      row[e] = val;
-      for_images(j, k, ny, nz, [&](int jj, int kk) {
-        ux[fidx(g, 1, jj, kk) + e] = val;
-      });
+  // u += delta into the other buffer, walls (boundary/*.c) and images (halo.c)
+  const double vx = (i >= 2) ? u0[VUX] + dl[VUX] : 0.;
+  const double vy = u0[VUY] + dl[VUY];
+  const double vz = u0[VUZ] + dl[VUZ];
+  const double vt = u0[VT] + dl[VT];
+  auto put = [&](int jj, int kk) {
+    out.ux[fidx(g, i, jj, kk)] = vx;
+    out.uy[cidx(g, i, jj, kk)] = vy;
+    out.uz[cidx(g, i, jj, kk)] = vz;
+    out.t[cidx(g, i, jj, kk)] = vt;
+    if (i == 1) {
+      out.uy[cidx(g, 0, jj, kk)] = bc.uy_xm;
+      out.uz[cidx(g, 0, jj, kk)] = 0.;
+      out.t[cidx(g, 0, jj, kk)] = bc.t_xm;
     }
-  } else {
-    double * arr = var == VUY ? uy : var == VUZ ? uz : t;
-    const double wm = var == VUY ? bc.uy_xm : var == VUZ ? 0. : bc.t_xm;
-    const double wp = var == VUY ? bc.uy_xp : var == VUZ ? 0. : bc.t_xp;
-    double * row = arr + cidx(g, 0, j, k);
-    for (int r = 0; r < E + 1; r++) {
-      const int e = lane + 32 * r;          // e = i, 0..nx+1
-      if (e > nx + 1) break;
-      double val;
-      if (e == 0) val = wm;
-      else if (e == nx + 1) val = wp;
-      else val = row[e] + sb[spad<E>(e - 1)];
-      row[e] = val;
-      for_images(j, k, ny, nz, [&](int jj, int kk) {
-        arr[cidx(g, 0, jj, kk) + e] = val;
-      });
+    if (i == nx) {
+      out.ux[fidx(g, nx + 1, jj, kk)] = 0.;
+      out.uy[cidx(g, nx + 1, jj, kk)] = bc.uy_xp;
+      out.uz[cidx(g, nx + 1, jj, kk)] = 0.;
+      out.t[cidx(g, nx + 1, jj, kk)] = bc.t_xp;
     }
-  }
+  };
+  put(j, k);
+  for_images(j, k, ny, nz, put);
+}
+
+// out = in + delta for every cell, walls and images (after the y / z solves)
+__global__ void __launch_bounds__(256)
+apply_kernel(Geo g, Bc bc, Fields in, Fields out, DeltaSet ds) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  if (i > nx || j > ny) return;
+  const size_t qc = pidx(nx, ny, i - 1, j, k);
+  const double vx = (i >= 2) ? in.ux[fidx(g, i, j, k)] + ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] : 0.;
+  const double vy = in.uy[cidx(g, i, j, k)] + ds.d[VUY][qc];
+  const double vz = in.uz[cidx(g, i, j, k)] + ds.d[VUZ][qc];
+  const double vt = in.t[cidx(g, i, j, k)] + ds.d[VT][qc];
+  auto put = [&](int jj, int kk) {
+    out.ux[fidx(g, i, jj, kk)] = vx;
+    out.uy[cidx(g, i, jj, kk)] = vy;
+    out.uz[cidx(g, i, jj, kk)] = vz;
+    out.t[cidx(g, i, jj, kk)] = vt;
+    if (i == 1) {
+      out.uy[cidx(g, 0, jj, kk)] = bc.uy_xm;
+      out.uz[cidx(g, 0, jj, kk)] = 0.;
+      out.t[cidx(g, 0, jj, kk)] = bc.t_xm;
+    }
+    if (i == nx) {
+      out.ux[fidx(g, nx + 1, jj, kk)] = 0.;
+      out.uy[cidx(g, nx + 1, jj, kk)] = bc.uy_xp;
+      out.uz[cidx(g, nx + 1, jj, kk)] = 0.;
+      out.t[cidx(g, nx + 1, jj, kk)] = bc.t_xp;
+    }
+  };
+  put(j, k);
+  for_images(j, k, ny, nz, put);
 }
 
 // ------------------------------------------------------------ periodic y / z solves
@@ -685,62 +747,57 @@ void launch_yzfactors(const Geo & g, const YZFactors & yf, const double * dtp, d
 }
 
 // ------------------------------------------------------------ launchers
-void launch_rhs_delta(const Geo & g, const Bc & bc, const Coefs & cf, double nu, double kappa,
-                      const Fields & f, double * const s_old[4], double * const s_new[4],
-                      double * const d[4], const double * dtp, int rkstep, cudaStream_t st) {
-  dim3 block(32, 8, 1);
-  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
-  rhs_delta_kernel<<<grid, block, 0, st>>>(g, bc, cf, nu, kappa, f.ux, f.uy, f.uz, f.p, f.t,
-      s_old[0], s_old[1], s_old[2], s_old[3], s_new[0], s_new[1], s_new[2], s_new[3],
-      d[0], d[1], d[2], d[3], dtp, rkstep);
+template <int NW>
+static void launch_predict_nw(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
+                              double kappa, const Fields & in, const Fields & out, const SrcSet & ss,
+                              const DeltaSet & ds, const double * dtp, int rkstep, int mode, cudaStream_t st) {
+  constexpr int NT = 32 * NW;
+  constexpr int LPB = 256 / NT;
+  const long long nlines = (long long)g.ny * g.nz;
+  dim3 block(NT, LPB, 1);
+  dim3 grid((unsigned)((nlines + LPB - 1) / LPB), 1, 1);
+  predict_kernel<NW><<<grid, block, 0, st>>>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode);
+}
+
+int predict_warps(int nx) {
+  int w = 1;
+  while (32 * w < nx) w *= 2;
+  return w;
+}
+
+void launch_predict(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu, double kappa,
+                    const Fields & in, const Fields & out, const SrcSet & ss, const DeltaSet & ds,
+                    const double * dtp, int rkstep, int mode, cudaStream_t st) {
+  switch (predict_warps(g.nx)) {
+    case 1: launch_predict_nw<1>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, st); break;
+    case 2: launch_predict_nw<2>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, st); break;
+    case 4: launch_predict_nw<4>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, st); break;
+    default: launch_predict_nw<8>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, st); break;
+  }
 }
 
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st) {
   xfactor_kernel<<<1, 32, 0, st>>>(xf, dtp, nu, kappa);
 }
 
-template <int E>
-static void launch_xsolve_e(const Geo & g, const Bc & bc, const XFactors & xf, int rkstep, int mode,
-                            const Fields & f, double * const d[4], cudaStream_t st) {
-  const long long nlines = (long long)g.ny * g.nz;
-  dim3 grid((unsigned)((nlines + 7) / 8), 4, 1);
-  if (mode == XS_SOLVE_APPLY) {
-    xsolve_kernel<E, true, true><<<grid, 256, 0, st>>>(g, bc, xf, rkstep, 0, f.ux, f.uy, f.uz, f.t, d[0], d[1], d[2], d[3]);
-  } else if (mode == XS_SOLVE) {
-    xsolve_kernel<E, true, false><<<grid, 256, 0, st>>>(g, bc, xf, rkstep, 0, f.ux, f.uy, f.uz, f.t, d[0], d[1], d[2], d[3]);
-  } else {
-    xsolve_kernel<E, false, true><<<grid, 256, 0, st>>>(g, bc, xf, rkstep, 0, f.ux, f.uy, f.uz, f.t, d[0], d[1], d[2], d[3]);
-  }
+void launch_apply(const Geo & g, const Bc & bc, const Fields & in, const Fields & out, const DeltaSet & ds,
+                  cudaStream_t st) {
+  dim3 block(32, 8, 1);
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  apply_kernel<<<grid, block, 0, st>>>(g, bc, in, out, ds);
 }
 
-int xsolve_elems(int nx) {
-  int e = 1;
-  while (32 * e < nx) e *= 2;
-  return e;
-}
-
-void launch_xsolve(const Geo & g, const Bc & bc, const XFactors & xf, int rkstep, int mode,
-                   const Fields & f, double * const d[4], cudaStream_t st) {
-  switch (xsolve_elems(g.nx)) {
-    case 1: launch_xsolve_e<1>(g, bc, xf, rkstep, mode, f, d, st); break;
-    case 2: launch_xsolve_e<2>(g, bc, xf, rkstep, mode, f, d, st); break;
-    case 4: launch_xsolve_e<4>(g, bc, xf, rkstep, mode, f, d, st); break;
-    case 8: launch_xsolve_e<8>(g, bc, xf, rkstep, mode, f, d, st); break;
-    default: launch_xsolve_e<16>(g, bc, xf, rkstep, mode, f, d, st); break;
-  }
-}
-
-void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st) {
+void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st) {
   for (int v = 0; v < 4; v++) {
     const long long n = (long long)yf.n_i[v] * g.nz;
-    ysolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, d[v]);
+    ysolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, ds.d[v]);
   }
 }
 
-void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, double * const d[4], cudaStream_t st) {
+void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st) {
   for (int v = 0; v < 4; v++) {
     const long long n = (long long)yf.n_i[v] * g.ny;
-    zsolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, d[v]);
+    zsolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, ds.d[v]);
   }
 }
 
