@@ -241,6 +241,28 @@ int tcgpu_set_device(int device);
  * tensors of the current fields. */
 int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]);
 
+/* Allocation-free variant of tdm.solve(). No counterpart in the reference.
+ * For callers that cannot allocate device memory or let a library do it
+ * (inside CUDA graph capture, under a framework that owns the device memory
+ * pool, or on hosts that reserve all device memory at start-up): the
+ * elimination factors go to a fixed static device array of
+ * 4 * TCGPU_TDM_NOALLOC_MAX_SIZE doubles (256 KiB) that every GPU which loads
+ * this library holds until the process exits; nothing is cudaMalloc'd or freed.
+ * l, c, u: host arrays of length size (lower, centre, upper diagonals as in
+ * tdm.get_l/get_c/get_u); data: device memory with nrhs right-hand sides of
+ * length size, contiguous (interleaved re/im when is_complex), solved in place
+ * with the same arithmetic as tdm.solve(). size must lie in
+ * [1, TCGPU_TDM_NOALLOC_MAX_SIZE] ([3, ...] when periodic); larger systems are
+ * rejected with a non-zero return. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture. All calls share the one
+ * array and each rewrites every entry it reads; calls whose kernels could
+ * overlap on the GPU (other threads, other streams) would race on it, so this
+ * library serialises its own calls and synchronises before returning. */
+#define TCGPU_TDM_NOALLOC_MAX_SIZE 8192
+int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, bool is_complex, const double * l,
+                            const double * c, const double * u, double * data);
+
 /* free the device state that belongs to this fluid_t */
 int tcgpu_release(fluid_t * fluid);
 

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "tcgpu.h"
@@ -231,3 +232,90 @@ int destruct(tdm_info_t * info) {
 extern "C" const tdm_t tdm = {
     construct, get_l, get_c, get_u, get_size, get_nrhs, solve, destruct,
 };
+
+// ---------------------------------------------------------------- allocation-free solve
+// For callers that must not allocate device memory themselves or have the
+// library do it: code running inside a CUDA graph capture or a memory-pool-
+// managed framework, embedded/real-time hosts that pre-reserve all device
+// memory up front, or plugins whose allocator belongs to someone else. The
+// elimination-factor table that tdm.solve() keeps in cudaMalloc'd memory lives
+// here in a fixed static device array instead; the caller supplies the
+// coefficients (host) and the right-hand sides (device memory, solved in place).
+namespace {
+
+constexpr int kNoAllocMax = TCGPU_TDM_NOALLOC_MAX_SIZE;
+// [l | v | w | q1], kNoAllocMax each; every loaded GPU holds it until exit
+static __device__ __align__(256) double g_noalloc_factors[4 * kNoAllocMax];
+static double g_noalloc_host[4 * kNoAllocMax];     // staging of the factors
+static double * g_noalloc_dev[128];                // device address per device ordinal
+static std::mutex g_noalloc_mutex;
+
+}  // namespace
+
+extern "C" int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, bool is_complex, const double * l,
+                                       const double * c, const double * u, double * data) {
+  if (size < 1 || size > kNoAllocMax || (is_periodic && size < 3))
+    return tcgpu_report_error(is_periodic && size < 3 && size >= 1
+                                  ? "tcgpu_tdm_solve_noalloc: periodic systems need size >= 3"
+                                  : "tcgpu_tdm_solve_noalloc: size outside [1, TCGPU_TDM_NOALLOC_MAX_SIZE]");
+  if (nrhs < 1) return tcgpu_report_error("tcgpu_tdm_solve_noalloc: nrhs must be positive");
+  if (l == nullptr || c == nullptr || u == nullptr || data == nullptr)
+    return tcgpu_report_error("tcgpu_tdm_solve_noalloc: NULL argument");
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, data) != cudaSuccess ||
+      (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)) {
+    cudaGetLastError();
+    return tcgpu_report_error("tcgpu_tdm_solve_noalloc: data must be device memory");
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+    return tcgpu_report_error("tcgpu_tdm_solve_noalloc: no current device");
+  if (g_noalloc_dev[dev] == nullptr) {
+    // set-up once per device, with that device current: the symbol's device
+    // address (the name itself is only a host-side stand-in)
+    double * p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noalloc_factors);
+    if (e != cudaSuccess) {
+      char msg[256];
+      snprintf(msg, sizeof(msg), "tcgpu_tdm_solve_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return tcgpu_report_error(msg);
+    }
+    g_noalloc_dev[dev] = p;
+  }
+  const int n = size;
+  const int m = is_periodic ? n - 1 : n;
+  double * hl = g_noalloc_host;
+  double * hv = hl + n;
+  double * hw = hl + 2 * n;
+  double * hq1 = hl + 3 * n;
+  // every entry the kernel reads is rewritten here; nothing from an earlier call survives
+  for (int i = 0; i < 4 * n; i++) hl[i] = 0.;
+  memcpy(hl, l, n * sizeof(double));
+  Plan pl{};
+  pl.m = m;
+  factors(m, l, c, u, hv, hw, pl);
+  if (is_periodic) {
+    for (int i = 0; i < n - 1; i++) hq1[i] = i == 0 ? -l[i] : i == n - 2 ? -u[i] : 0.;
+    host_gtsv(m, l, c, u, hv, hw, pl, hq1);
+    pl.u_last = u[n - 1];
+    pl.l_last = l[n - 1];
+    pl.den = c[n - 1] + u[n - 1] * hq1[0] + l[n - 1] * hq1[n - 2];
+    pl.den_zero = fabs(pl.den) < kEps;
+  }
+  double * dcoef = g_noalloc_dev[dev];
+  cudaError_t e = cudaMemcpy(dcoef, hl, 4 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const int comps = is_complex ? 2 : 1;
+    const int threads = nrhs * comps;
+    tdm_kernel<<<(threads + 127) / 128, 128>>>(n, nrhs, comps, is_periodic ? 1 : 0, dcoef, pl, data);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  if (e != cudaSuccess) {
+    char msg[256];
+    snprintf(msg, sizeof(msg), "tcgpu_tdm_solve_noalloc: %s", cudaGetErrorString(e));
+    return tcgpu_report_error(msg);
+  }
+  return 0;
+}
