@@ -392,16 +392,16 @@ static int build_tables(Ctx & c, const domain_t * d) {
   CK(cudaMemcpy(c.tab_y, ty.data(), ty.size() * sizeof(double), cudaMemcpyHostToDevice));
   c.ps.tl = dtl;
   c.ps.tu = dtu;
-  // twiddles exp(-2 pi i m / N), m < N/2, from libm
+  // twiddles exp(-2 pi i m / N), m < N, from libm
   auto twiddles = [&](int N) -> double2 * {
-    std::vector<double> tw(N);  // N/2 complex
-    for (int k = 0; k < N / 2; k++) {
+    std::vector<double> tw(2 * (size_t)N);
+    for (int k = 0; k < N; k++) {
       const double a = 2. * g_pi * k / N;
       tw[2 * k] = cos(a);
       tw[2 * k + 1] = -sin(a);
     }
-    double * p = dalloc(c, N);
-    if (p) cudaMemcpy(p, tw.data(), N * sizeof(double), cudaMemcpyHostToDevice);
+    double * p = dalloc(c, 2 * (size_t)N);
+    if (p) cudaMemcpy(p, tw.data(), 2 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice);
     return reinterpret_cast<double2 *>(p);
   };
   c.ps.tw_y = twiddles(ny);

@@ -122,8 +122,8 @@ struct Poisson {
   int nyh;                  // ny/2 + 1
   double2 * spec;           // [nx][nz][nyh] complex spectra
   double * vscr;            // [nx][nz][nyh] elimination factors
-  const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny/2
-  const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz/2
+  const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny
+  const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz
   const double * tl;        // radial l_i (compute_potential.c:197-200), length nx
   const double * tu;        // radial u_i
   const double * ihy2;      // 1 / HYXC(i)^2 as (1/HYXC)/HYXC, length nx (index i-1)

@@ -14,8 +14,10 @@
 //                    Neumann x ghosts and periodic images (extract_output, :427-443)
 //
 // Transforms are unnormalised like FFTW's; the 1/(ny nz) factor sits in the
-// right-hand side as in the reference. FFTs are radix-2 Stockham passes in shared
-// memory with twiddles exp(-2 pi i m / N) tabulated on the host from libm.
+// right-hand side as in the reference. FFTs are in-place Stockham passes over
+// lines held in shared memory, 16 elements per thread, radix-16 butterflies in
+// registers (N = 1024: passes of 16, 16, 4), twiddles exp(-2 pi i m / N)
+// tabulated on the host from libm.
 //
 // Spectral layout: spec[i][kz][ky] (ky fastest), so the y and z transforms read
 // and write rows of contiguous wavenumbers and the radial solve, one thread per
@@ -23,53 +25,154 @@
 #include "tc_common.cuh"
 #include "tc_kernels.h"
 
+// resident CTAs per SM requested from the register allocator (measured best:
+// 2 for the divergence + FFT kernel, 3 for the pure transforms)
+#ifndef TC_FFT_MIN_BLOCKS
+#define TC_FFT_MIN_BLOCKS 3
+#endif
+#ifndef TC_DIVFFT_MIN_BLOCKS
+#define TC_DIVFFT_MIN_BLOCKS 2
+#endif
+
 namespace tcgpu {
 
 __device__ inline double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// radix-2 Stockham autosort over P lines of length N held in a; b is scratch.
-// Returns the buffer that holds the result (natural order).
+// Shared-memory lines are padded by one slot per 16 complex values so that the
+// strided stores of the first pass and the unit-stride accesses of the others
+// are both free of bank conflicts.
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4) + 1; }
+
 template <int SIGN>
-__device__ double2 * fft_lines(double2 * a, double2 * b, int N, int P, const double2 * __restrict__ tw) {
-  const int half = N >> 1;
-  for (int Ns = 1; Ns < N; Ns <<= 1) {
-    const int tws = N / (2 * Ns);
-    for (int idx = threadIdx.x; idx < P * half; idx += blockDim.x) {
-      const int p = idx / half;
-      const int jj = idx - p * half;
-      const double2 * x = a + (size_t)p * N;
-      double2 * y = b + (size_t)p * N;
-      const int kk = jj & (Ns - 1);
-      double2 w = __ldg(tw + kk * tws);
-      if (SIGN > 0) w.y = -w.y;
-      const double2 u0 = x[jj];
-      const double2 t = cmul(x[jj + half], w);
-      const int o = ((jj - kk) << 1) + kk;
-      y[o] = make_double2(u0.x + t.x, u0.y + t.y);
-      y[o + Ns] = make_double2(u0.x - t.x, u0.y - t.y);
+__device__ __forceinline__ double2 twid(const double2 * __restrict__ tw, int m) {
+  double2 w = __ldg(tw + m);
+  if (SIGN > 0) w.y = -w.y;
+  return w;
+}
+
+// multiply by exp(SIGN i pi / 2) = SIGN i
+template <int SIGN>
+__device__ __forceinline__ double2 quarter(double2 z) {
+  return SIGN < 0 ? make_double2(z.y, -z.x) : make_double2(-z.y, z.x);
+}
+
+template <int R>
+__host__ __device__ constexpr int brev(int a) {
+  int b = 0;
+  for (int m = 1; m < R; m <<= 1) b = (b << 1) | ((a & m) ? 1 : 0);
+  return b;
+}
+
+// In-register DFT of R points: v[s] <- sum_r v[r] exp(SIGN 2 pi i r s / R),
+// iterative radix-2 decimation in time; twiddles exp(SIGN 2 pi i k / len) are
+// tw[k N / len] of the length-N table.
+template <int R, int SIGN>
+__device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict__ tw, int N) {
+#pragma unroll
+  for (int a = 0; a < R; a++) {
+    const int b = brev<R>(a);
+    if (a < b) {
+      const double2 t = v[a];
+      v[a] = v[b];
+      v[b] = t;
     }
-    __syncthreads();
-    double2 * s = a;
-    a = b;
-    b = s;
   }
-  return a;
+#pragma unroll
+  for (int len = 2; len <= R; len <<= 1) {
+    const int half = len >> 1;
+#pragma unroll
+    for (int k = 0; k < half; k++) {
+      double2 w = make_double2(1., 0.);
+      if (k != 0 && 4 * k != len) w = twid<SIGN>(tw, k * (N / len));
+#pragma unroll
+      for (int s = 0; s < R; s += len) {
+        const double2 a = v[s + k];
+        double2 b = v[s + k + half];
+        if (4 * k == len) b = quarter<SIGN>(b);
+        else if (k != 0) b = cmul(b, w);
+        v[s + k] = make_double2(a.x + b.x, a.y + b.y);
+        v[s + k + half] = make_double2(a.x - b.x, a.y - b.y);
+      }
+    }
+  }
+}
+
+// One in-place Stockham pass of radix R over a padded line x of length N: the
+// thread owns butterflies j = t + b TPL (b < B); Ns is the product of the
+// radices already applied. All inputs are read before anything is written.
+template <int R, int B, int SIGN>
+__device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t, int TPL,
+                                              const double2 * __restrict__ tw) {
+  double2 v[B][R];
+  const int NR = N / R;
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * TPL;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[b][r] = x[pad(j + r * NR)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * TPL;
+    const int k = j & (Ns - 1);
+    if (Ns > 1) {
+      const int step = k * (N / (Ns * R));
+#pragma unroll
+      for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], twid<SIGN>(tw, r * step));
+    }
+    dft_reg<R, SIGN>(v[b], tw, N);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) x[pad(base + r * Ns)] = v[b][r];
+  }
+  __syncthreads();
+}
+
+// Full transform of the CTA's lines (N = 2^lg): EPT elements per thread,
+// radix-16 passes then the remainder; natural-order output in place.
+template <int EPT, int SIGN>
+__device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const double2 * __restrict__ tw) {
+  int Ns = 1;
+  int left = lg;
+  while (left > 0) {
+    const int rl = left >= 4 ? 4 : left;
+    if (EPT == 16) {
+      if (rl == 4) stockham_pass<16, 1, SIGN>(x, N, Ns, t, TPL, tw);
+      else if (rl == 3) stockham_pass<8, 2, SIGN>(x, N, Ns, t, TPL, tw);
+      else if (rl == 2) stockham_pass<4, 4, SIGN>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 8, SIGN>(x, N, Ns, t, TPL, tw);
+    } else if (EPT == 8) {
+      if (rl == 3) stockham_pass<8, 1, SIGN>(x, N, Ns, t, TPL, tw);
+      else if (rl == 2) stockham_pass<4, 2, SIGN>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 4, SIGN>(x, N, Ns, t, TPL, tw);
+    } else {
+      if (rl == 2) stockham_pass<4, 1, SIGN>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 2, SIGN>(x, N, Ns, t, TPL, tw);
+    }
+    Ns <<= rl;
+    left -= rl;
+  }
 }
 
 // --------------------------------------------------------------- forward y
-__global__ void __launch_bounds__(256)
-div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P,
+// CTA: P complex lines (radial indices i0 .. i0+2P-1) x all j at one k;
+// TPL = ny / EPT threads per line.
+template <int EPT>
+__global__ void __launch_bounds__(256, TC_DIVFFT_MIN_BLOCKS)
+div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
                 const double * __restrict__ ux, const double * __restrict__ uy,
                 const double * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz;
   const int TI = 2 * P;
+  const int TPL = ny / EPT;
+  const int LS = padded_len(ny);
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
-  double2 * a = smem;
-  double2 * b = smem + (size_t)P * ny;
   const double norm = 1. * ny * nz;
   const double prefactor = 1. / (rk_gamma(rkstep) * (*dtp)) / norm;
   for (int idx = threadIdx.x; idx < TI * ny; idx += blockDim.x) {
@@ -92,11 +195,12 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P,
           - jz * uz_zm + jz * uz_zp);
       val = prefactor * div;
     }
-    double * line = reinterpret_cast<double *>(a + (size_t)(ii >> 1) * ny);
-    line[2 * (j - 1) + (ii & 1)] = val;
+    double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
+    line[2 * pad(j - 1) + (ii & 1)] = val;
   }
   __syncthreads();
-  double2 * r = fft_lines<-1>(a, b, ny, P, ps.tw_y);
+  const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  fft_inplace<EPT, -1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
   // separate the two real transforms and store the ny/2+1 non-negative wavenumbers
   const int nyh = ps.nyh;
   for (int idx = threadIdx.x; idx < TI * nyh; idx += blockDim.x) {
@@ -104,9 +208,9 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P,
     const int ii = idx / nyh;
     const int i = i0 + ii;
     if (i > nx) continue;
-    const double2 * z = r + (size_t)(ii >> 1) * ny;
-    const double2 zm = z[m];
-    const double2 zn = z[(ny - m) & (ny - 1)];
+    const double2 * z = smem + (size_t)(ii >> 1) * LS;
+    const double2 zm = z[pad(m)];
+    const double2 zn = z[pad((ny - m) & (ny - 1))];
     double2 out;
     if ((ii & 1) == 0) out = make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y - zn.y));
     else out = make_double2(0.5 * (zm.y + zn.y), -0.5 * (zm.x - zn.x));
@@ -115,29 +219,31 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P,
 }
 
 // --------------------------------------------------------------- z transforms
-template <int SIGN>
-__global__ void __launch_bounds__(256)
-fftz_kernel(Geo g, Poisson ps, int TM) {
+// CTA: P lines (wavenumbers m0 .. m0+P-1) of one radial index, all kz.
+template <int EPT, int SIGN>
+__global__ void __launch_bounds__(256, TC_FFT_MIN_BLOCKS)
+fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   extern __shared__ double2 smem[];
   const int nz = g.nz, nyh = ps.nyh;
+  const int TPL = nz / EPT;
+  const int LS = padded_len(nz);
   const int i = blockIdx.x;          // 0..nx-1
-  const int m0 = blockIdx.y * TM;
-  double2 * a = smem;
-  double2 * b = smem + (size_t)TM * nz;
+  const int m0 = blockIdx.y * P;
   double2 * base = ps.spec + (size_t)i * nz * nyh;
-  for (int idx = threadIdx.x; idx < TM * nz; idx += blockDim.x) {
-    const int mm = idx % TM;
-    const int kz = idx / TM;
+  for (int idx = threadIdx.x; idx < P * nz; idx += blockDim.x) {
+    const int mm = idx % P;
+    const int kz = idx / P;
     const int m = m0 + mm;
-    a[(size_t)mm * nz + kz] = (m < nyh) ? base[(size_t)kz * nyh + m] : make_double2(0., 0.);
+    smem[(size_t)mm * LS + pad(kz)] = (m < nyh) ? base[(size_t)kz * nyh + m] : make_double2(0., 0.);
   }
   __syncthreads();
-  double2 * r = fft_lines<SIGN>(a, b, nz, TM, ps.tw_z);
-  for (int idx = threadIdx.x; idx < TM * nz; idx += blockDim.x) {
-    const int mm = idx % TM;
-    const int kz = idx / TM;
+  const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  fft_inplace<EPT, SIGN>(smem + (size_t)p * LS, nz, lg, t, TPL, ps.tw_z);
+  for (int idx = threadIdx.x; idx < P * nz; idx += blockDim.x) {
+    const int mm = idx % P;
+    const int kz = idx / P;
     const int m = m0 + mm;
-    if (m < nyh) base[(size_t)kz * nyh + m] = r[(size_t)mm * nz + kz];
+    if (m < nyh) base[(size_t)kz * nyh + m] = smem[(size_t)mm * LS + pad(kz)];
   }
 }
 
@@ -208,15 +314,16 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
 }
 
 // --------------------------------------------------------------- inverse y
-__global__ void __launch_bounds__(256)
-iffty_kernel(Geo g, Poisson ps, int P, double * __restrict__ psi) {
+template <int EPT>
+__global__ void __launch_bounds__(256, TC_FFT_MIN_BLOCKS)
+iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh;
   const int TI = 2 * P;
+  const int TPL = ny / EPT;
+  const int LS = padded_len(ny);
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
-  double2 * a = smem;
-  double2 * b = smem + (size_t)P * ny;
   // Hermitian extension of the two packed real lines
   for (int idx = threadIdx.x; idx < P * ny; idx += blockDim.x) {
     const int m = idx % ny;
@@ -230,16 +337,17 @@ iffty_kernel(Geo g, Poisson ps, int P, double * __restrict__ psi) {
     double2 z;
     if (m <= ny / 2) z = make_double2(xa.x - xb.y, xa.y + xb.x);
     else z = make_double2(xa.x + xb.y, -xa.y + xb.x);
-    a[(size_t)pp * ny + m] = z;
+    smem[(size_t)pp * LS + pad(m)] = z;
   }
   __syncthreads();
-  double2 * r = fft_lines<+1>(a, b, ny, P, ps.tw_y);
+  const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  fft_inplace<EPT, +1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
   for (int idx = threadIdx.x; idx < TI * ny; idx += blockDim.x) {
     const int ii = idx % TI;
     const int j = idx / TI + 1;
     const int i = i0 + ii;
     if (i > nx) continue;
-    const double2 z = r[(size_t)(ii >> 1) * ny + (j - 1)];
+    const double2 z = smem[(size_t)(ii >> 1) * LS + pad(j - 1)];
     const double val = (ii & 1) ? z.y : z.x;
     auto put = [&](int jj, int kk) {
       psi[cidx(g, i, jj, kk)] = val;
@@ -251,41 +359,86 @@ iffty_kernel(Geo g, Poisson ps, int P, double * __restrict__ psi) {
   }
 }
 
-static int pick_lines(int n, int maxlines) {
-  int p = 1;
-  while (p * 2 * n <= 2048 && p * 2 <= maxlines) p *= 2;
-  return p;
+// --------------------------------------------------------------- launchers
+static int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) l++;
+  return l;
+}
+
+// lines per CTA: ceil-free power of two, TPL threads each, at most 256 threads,
+// at most `cap` lines
+static int lines_per_cta(int n, int cap) {
+  const int ept = n < 16 ? n : 16;
+  const int tpl = n / ept;
+  int p = 256 / tpl;
+  while (p > 1 && p > cap) p >>= 1;
+  return p < 1 ? 1 : p;
+}
+
+template <int EPTY, int EPTZ>
+static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+                             const double * tab_y, const double * tab_z, const double * base,
+                             const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
+  auto mark = [&](int kk) { if (pm.mark) pm.mark(kk, 1); };
+  const int lgy = ilog2(g.ny), lgz = ilog2(g.nz);
+  const int Py = lines_per_cta(g.ny, (g.nx + 1) / 2);
+  const int tply = g.ny / EPTY;
+  const size_t smy = sizeof(double2) * (size_t)Py * padded_len(g.ny);
+  dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
+  div_ffty_kernel<EPTY><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
+  mark(pm.k_div);
+  const int Pz = lines_per_cta(g.nz, ps.nyh);
+  const int tplz = g.nz / EPTZ;
+  const size_t smz = sizeof(double2) * (size_t)Pz * padded_len(g.nz);
+  dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
+  fftz_kernel<EPTZ, -1><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  mark(pm.k_fwd);
+  const long long nl = (long long)ps.nyh * g.nz;
+  tdm_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+  mark(pm.k_tdm);
+  fftz_kernel<EPTZ, +1><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  mark(pm.k_inv);
+  iffty_kernel<EPTY><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
+  mark(pm.k_ify);
+}
+
+template <int EPTY>
+static void launch_poisson_z(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+                             const double * tab_y, const double * tab_z, const double * base,
+                             const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
+  if (g.nz >= 16) launch_poisson_t<EPTY, 16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.nz == 8) launch_poisson_t<EPTY, 8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else launch_poisson_t<EPTY, 4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
 }
 
 void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
                     const double * tab_y, const double * tab_z, const double * base,
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
-  auto mark = [&](int k) { if (pm.mark) pm.mark(k, 1); };
-  const int P = pick_lines(g.ny, 8);
-  const size_t smy = sizeof(double2) * 2 * (size_t)P * g.ny;
-  dim3 gy((g.nx + 2 * P - 1) / (2 * P), g.nz);
-  div_ffty_kernel<<<gy, 256, smy, st>>>(g, cf, ps, P, f.ux, f.uy, f.uz, dtp, rkstep);
-  mark(pm.k_div);
-  const int TM = pick_lines(g.nz, 16);
-  const size_t smz = sizeof(double2) * 2 * (size_t)TM * g.nz;
-  dim3 gz(g.nx, (ps.nyh + TM - 1) / TM);
-  fftz_kernel<-1><<<gz, 256, smz, st>>>(g, ps, TM);
-  mark(pm.k_fwd);
-  const long long nl = (long long)ps.nyh * g.nz;
-  tdm_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
-  mark(pm.k_tdm);
-  fftz_kernel<+1><<<gz, 256, smz, st>>>(g, ps, TM);
-  mark(pm.k_inv);
-  iffty_kernel<<<gy, 256, smy, st>>>(g, ps, P, f.psi);
-  mark(pm.k_ify);
+  if (g.ny >= 16) launch_poisson_z<16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.ny == 8) launch_poisson_z<8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else launch_poisson_z<4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+}
+
+template <typename K>
+static void allow_dyn_smem(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
 }
 
 void poisson_smem_limits() {
-  // 2 buffers x 2048 complex doubles = 64 KB of dynamic shared memory
-  cudaFuncSetAttribute(div_ffty_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
-  cudaFuncSetAttribute(iffty_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
-  cudaFuncSetAttribute(fftz_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
-  cudaFuncSetAttribute(fftz_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536);
+  // up to 256 threads x 16 elements of 16 bytes, padded: < 74 KB of dynamic shared memory
+  allow_dyn_smem(div_ffty_kernel<16>);
+  allow_dyn_smem(div_ffty_kernel<8>);
+  allow_dyn_smem(div_ffty_kernel<4>);
+  allow_dyn_smem(iffty_kernel<16>);
+  allow_dyn_smem(iffty_kernel<8>);
+  allow_dyn_smem(iffty_kernel<4>);
+  allow_dyn_smem(fftz_kernel<16, -1>);
+  allow_dyn_smem(fftz_kernel<16, +1>);
+  allow_dyn_smem(fftz_kernel<8, -1>);
+  allow_dyn_smem(fftz_kernel<8, +1>);
+  allow_dyn_smem(fftz_kernel<4, -1>);
+  allow_dyn_smem(fftz_kernel<4, +1>);
 }
 
 }  // namespace tcgpu
