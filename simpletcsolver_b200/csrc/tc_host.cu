@@ -1,6 +1,7 @@
 // Host runtime of tcgpu: per-fluid device contexts, the step schedule (one
 // CUDA stream, the full time step captured once as a CUDA graph), host<->device
 // coherence, and the exported C entry points of include/tcgpu.h.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -319,16 +320,19 @@ static int build_tables(Ctx & c, const domain_t * d) {
   double * dP = dalloc(c, P.size());
   if (!dP) return fail("cudaMalloc failed");
   CK(cudaMemcpy(dP, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice));
-  c.xf.stride = L;
+  // factor rows cover every element a solving warp touches (32 lanes x
+  // elements per lane) and start on 16-byte boundaries for paired loads
+  const size_t LX = ((std::max(L, (size_t)32 * predict_warps(nx)) + 1) / 2) * 2;
+  c.xf.stride = LX;
   for (int v = 0; v < 4; v++) {
     c.xf.n[v] = (v == VUX) ? nx - 1 : nx;
     c.xf.lap_l[v] = dP + (size_t)v * 6 * L;
     c.xf.lap_c[v] = dP + (size_t)v * 6 * L + L;
     c.xf.lap_u[v] = dP + (size_t)v * 6 * L + 2 * L;
   }
-  c.xf.lo = dalloc(c, 12 * L);
-  c.xf.w = dalloc(c, 12 * L);
-  c.xf.v = dalloc(c, 12 * L);
+  c.xf.lo = dalloc(c, 12 * LX);
+  c.xf.w = dalloc(c, 12 * LX);
+  c.xf.v = dalloc(c, 12 * LX);
   if (c.bc.implicit[1] || c.bc.implicit[2]) {
     YZFactors & yf = c.yf;
     yf.max_i = nx;

@@ -25,10 +25,14 @@
 #include "tc_common.cuh"
 #include "tc_kernels.h"
 
-// resident CTAs per SM requested from the register allocator (measured best:
-// 2 for the divergence + FFT kernel, 3 for the pure transforms)
-#ifndef TC_FFT_MIN_BLOCKS
-#define TC_FFT_MIN_BLOCKS 3
+// resident CTAs per SM requested from the register allocator (measured best
+// at 256 x 1024 x 512: 2 for the divergence + y transform and for the z
+// transforms, 3 for the inverse y transform)
+#ifndef TC_FFTZ_MIN_BLOCKS
+#define TC_FFTZ_MIN_BLOCKS 2
+#endif
+#ifndef TC_IFFTY_MIN_BLOCKS
+#define TC_IFFTY_MIN_BLOCKS 3
 #endif
 #ifndef TC_DIVFFT_MIN_BLOCKS
 #define TC_DIVFFT_MIN_BLOCKS 2
@@ -175,28 +179,67 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
   const int k = blockIdx.y + 1;
   const double norm = 1. * ny * nz;
   const double prefactor = 1. / (rk_gamma(rkstep) * (*dtp)) / norm;
-  for (int idx = threadIdx.x; idx < TI * ny; idx += blockDim.x) {
-    const int ii = idx % TI;
-    const int j = idx / TI + 1;
+  // When TI divides the block size (ny >= 2 EPT) each thread keeps one radial
+  // index and visits rows j = j0, j0 + blockDim / TI, ... (2 EPT of them);
+  // otherwise (short lines) the plain element loop.
+  if (blockDim.x % TI != 0) {
+    for (int idx = threadIdx.x; idx < TI * ny; idx += blockDim.x) {
+      const int ii = idx % TI;
+      const int j = idx / TI + 1;
+      const int i = i0 + ii;
+      double val = 0.;
+      if (i <= nx) {
+        const double ux_xm = __ldg(ux + fidx(g, i, j, k));
+        const double ux_xp = __ldg(ux + fidx(g, i + 1, j, k));
+        const double uy_ym = __ldg(uy + cidx(g, i, j, k));
+        const double uy_yp = __ldg(uy + cidx(g, i, j + 1, k));
+        const double uz_zm = __ldg(uz + cidx(g, i, j, k));
+        const double uz_zp = __ldg(uz + cidx(g, i, j, k + 1));
+        const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
+        const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i);
+        const double div = __ldg(cf.c_invjdxc + i) * (
+            -jxm * ux_xm + jxp * ux_xp
+            - jy * uy_ym + jy * uy_yp
+            - jz * uz_zm + jz * uz_zp);
+        val = prefactor * div;
+      }
+      double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
+      line[2 * pad(j - 1) + (ii & 1)] = val;
+    }
+  } else {
+    const int ii = threadIdx.x % TI;
+    const int j0 = threadIdx.x / TI + 1;
+    const int jstep = blockDim.x / TI;
     const int i = i0 + ii;
-    double val = 0.;
+    double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
     if (i <= nx) {
-      const double ux_xm = __ldg(ux + fidx(g, i, j, k));
-      const double ux_xp = __ldg(ux + fidx(g, i + 1, j, k));
-      const double uy_ym = __ldg(uy + cidx(g, i, j, k));
-      const double uy_yp = __ldg(uy + cidx(g, i, j + 1, k));
-      const double uz_zm = __ldg(uz + cidx(g, i, j, k));
-      const double uz_zp = __ldg(uz + cidx(g, i, j, k + 1));
       const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
       const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i);
-      const double div = __ldg(cf.c_invjdxc + i) * (
-          -jxm * ux_xm + jxp * ux_xp
-          - jy * uy_ym + jy * uy_yp
-          - jz * uz_zm + jz * uz_zp);
-      val = prefactor * div;
+      const double ijd = __ldg(cf.c_invjdxc + i);
+      const double * __restrict__ pxm = ux + fidx(g, i, 0, k);
+      const double * __restrict__ pym = uy + cidx(g, i, 0, k);
+      const double * __restrict__ pzm = uz + cidx(g, i, 0, k);
+      const double * __restrict__ pzp = uz + cidx(g, i, 0, k + 1);
+      const int sf = nx + 1, sc = nx + 2;
+#pragma unroll 8
+      for (int r = 0; r < 2 * EPT; r++) {
+        const int j = j0 + r * jstep;
+        const double ux_xm = __ldg(pxm + (size_t)j * sf);
+        const double ux_xp = __ldg(pxm + (size_t)j * sf + 1);
+        const double uy_ym = __ldg(pym + (size_t)j * sc);
+        const double uy_yp = __ldg(pym + (size_t)(j + 1) * sc);
+        const double uz_zm = __ldg(pzm + (size_t)j * sc);
+        const double uz_zp = __ldg(pzp + (size_t)j * sc);
+        const double div = ijd * (
+            -jxm * ux_xm + jxp * ux_xp
+            - jy * uy_ym + jy * uy_yp
+            - jz * uz_zm + jz * uz_zp);
+        line[2 * pad(j - 1) + (ii & 1)] = prefactor * div;
+      }
+    } else {
+#pragma unroll 8
+      for (int r = 0; r < 2 * EPT; r++) line[2 * pad(j0 + r * jstep - 1) + (ii & 1)] = 0.;
     }
-    double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
-    line[2 * pad(j - 1) + (ii & 1)] = val;
   }
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
@@ -221,7 +264,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
 // --------------------------------------------------------------- z transforms
 // CTA: P lines (wavenumbers m0 .. m0+P-1) of one radial index, all kz.
 template <int EPT, int SIGN>
-__global__ void __launch_bounds__(256, TC_FFT_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, TC_FFTZ_MIN_BLOCKS)
 fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   extern __shared__ double2 smem[];
   const int nz = g.nz, nyh = ps.nyh;
@@ -230,25 +273,33 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   const int i = blockIdx.x;          // 0..nx-1
   const int m0 = blockIdx.y * P;
   double2 * base = ps.spec + (size_t)i * nz * nyh;
-  for (int idx = threadIdx.x; idx < P * nz; idx += blockDim.x) {
-    const int mm = idx % P;
-    const int kz = idx / P;
-    const int m = m0 + mm;
-    smem[(size_t)mm * LS + pad(kz)] = (m < nyh) ? base[(size_t)kz * nyh + m] : make_double2(0., 0.);
-  }
+  // P nz = blockDim EPT: each thread moves EPT values of one wavenumber m
+  // (P divides the block size), all loads in flight together
+  const int mm = threadIdx.x % P;
+  const int kz0 = threadIdx.x / P;
+  const int kstep = blockDim.x / P;
+  const int m = m0 + mm;
+#pragma unroll
+  for (int r = 0; r < EPT; r++)
+    smem[(size_t)mm * LS + pad(kz0 + r * kstep)] =
+        (m < nyh) ? base[(size_t)(kz0 + r * kstep) * nyh + m] : make_double2(0., 0.);
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
   fft_inplace<EPT, SIGN>(smem + (size_t)p * LS, nz, lg, t, TPL, ps.tw_z);
-  for (int idx = threadIdx.x; idx < P * nz; idx += blockDim.x) {
-    const int mm = idx % P;
-    const int kz = idx / P;
-    const int m = m0 + mm;
-    if (m < nyh) base[(size_t)kz * nyh + m] = smem[(size_t)mm * LS + pad(kz)];
+  if (m < nyh) {
+#pragma unroll
+    for (int r = 0; r < EPT; r++)
+      base[(size_t)(kz0 + r * kstep) * nyh + m] = smem[(size_t)mm * LS + pad(kz0 + r * kstep)];
   }
 }
 
 // --------------------------------------------------------------- radial solve
-__global__ void __launch_bounds__(128)
+// rows fetched ahead of the recurrence (measured at 256 x 1024 x 512: 2 rows
+// 0.89 ms, 4 rows 0.92 ms, none 1.00 ms)
+#ifndef TC_TDM_PREFETCH
+#define TC_TDM_PREFETCH 2
+#endif
+__global__ void __launch_bounds__(128, 8)
 tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * __restrict__ tab_z,
            const double * __restrict__ base) {
   const int nyh = ps.nyh, nz = g.nz, n = g.nx;
@@ -281,14 +332,32 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
   double2 qprev = q[0];
   qprev = make_double2(qprev.x / c0, qprev.y / c0);
   q[0] = qprev;
-  for (int i = 1; i < n - 1; i++) {
-    const double l = __ldg(ps.tl + i);
-    const double val = 1. / (cdiag(i) - l * vprev);
-    vprev = val * __ldg(ps.tu + i);
-    v[(size_t)i * st] = vprev;
-    const double2 r = q[(size_t)i * st];
-    qprev = make_double2(val * (r.x - l * qprev.x), val * (r.y - l * qprev.y));
-    q[(size_t)i * st] = qprev;
+  // rows are fetched G at a time ahead of the recurrence, so G loads per
+  // thread are in flight together
+  constexpr int G = TC_TDM_PREFETCH;
+  for (int ib = 1; ib < n - 1; ib += G) {
+    double2 r[G];
+    double cd[G];
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int i = ib + u;
+      if (i < n - 1) {
+        r[u] = q[(size_t)i * st];
+        cd[u] = cdiag(i);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int i = ib + u;
+      if (i < n - 1) {
+        const double l = __ldg(ps.tl + i);
+        const double val = 1. / (cd[u] - l * vprev);
+        vprev = val * __ldg(ps.tu + i);
+        v[(size_t)i * st] = vprev;
+        qprev = make_double2(val * (r[u].x - l * qprev.x), val * (r[u].y - l * qprev.y));
+        q[(size_t)i * st] = qprev;
+      }
+    }
   }
   {
     const int i = n - 1;
@@ -305,17 +374,31 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
     qprev = x;
   }
   // back substitution
-  for (int i = n - 2; i >= 0; i--) {
-    const double vi = v[(size_t)i * st];
-    const double2 r = q[(size_t)i * st];
-    qprev = make_double2(r.x - vi * qprev.x, r.y - vi * qprev.y);
-    q[(size_t)i * st] = qprev;
+  for (int ib = n - 2; ib >= 0; ib -= G) {
+    double2 r[G];
+    double vi[G];
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int i = ib - u;
+      if (i >= 0) {
+        vi[u] = v[(size_t)i * st];
+        r[u] = q[(size_t)i * st];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < G; u++) {
+      const int i = ib - u;
+      if (i >= 0) {
+        qprev = make_double2(r[u].x - vi[u] * qprev.x, r[u].y - vi[u] * qprev.y);
+        q[(size_t)i * st] = qprev;
+      }
+    }
   }
 }
 
 // --------------------------------------------------------------- inverse y
 template <int EPT>
-__global__ void __launch_bounds__(256, TC_FFT_MIN_BLOCKS)
+__global__ void __launch_bounds__(256, TC_IFFTY_MIN_BLOCKS)
 iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh;
@@ -325,7 +408,9 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
   // Hermitian extension of the two packed real lines
-  for (int idx = threadIdx.x; idx < P * ny; idx += blockDim.x) {
+#pragma unroll 8
+  for (int r = 0; r < EPT; r++) {
+    const int idx = threadIdx.x + r * blockDim.x;
     const int m = idx % ny;
     const int pp = idx / ny;
     const int ia = i0 + 2 * pp, ib = ia + 1;
@@ -342,9 +427,16 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
   fft_inplace<EPT, +1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
-  for (int idx = threadIdx.x; idx < TI * ny; idx += blockDim.x) {
+  // one radial index per thread when TI divides the block size (ny >= 2 EPT),
+  // else the plain element loop
+  const bool fixed_i = blockDim.x % TI == 0;
+  const int nr = fixed_i ? 2 * EPT : (TI * ny + blockDim.x - 1) / blockDim.x;
+#pragma unroll 4
+  for (int r = 0; r < nr; r++) {
+    const int idx = fixed_i ? threadIdx.x : threadIdx.x + r * blockDim.x;
+    if (idx >= TI * ny) break;
     const int ii = idx % TI;
-    const int j = idx / TI + 1;
+    const int j = fixed_i ? idx / TI + 1 + r * (blockDim.x / TI) : idx / TI + 1;
     const int i = i0 + ii;
     if (i > nx) continue;
     const double2 z = smem[(size_t)(ii >> 1) * LS + pad(j - 1)];
