@@ -70,6 +70,6 @@ __device__ inline void for_images(int j, int k, int ny, int nz, F && f) {
 }
 
 // device-side status word: set by kernels, read by the host after a step
-enum : unsigned { ST_NONFINITE = 1u, ST_BADDT = 2u };
+enum : unsigned { ST_NONFINITE = 1u, ST_BADDT = 2u, ST_TIMEOUT = 4u };
 
 }  // namespace tcgpu

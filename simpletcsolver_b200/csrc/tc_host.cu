@@ -257,6 +257,58 @@ static int build_tables(Ctx & c, const domain_t * d) {
     col(C_PYL)[i] = JDXC(i) / HYXC(i) / HYXC(i);
     col(C_PZL)[i] = JDXC(i) / hz / hz;
   }
+  // products for the marching predict kernel (tc_march.cu); each term's
+  // derivation is beside its use there
+  for (int i = 2; i <= nx; i++) {
+    const double invj = col(F_INVJD)[i];
+    col(P_XA1)[i] = 0.5 * invj * col(F_A1)[i];
+    col(P_XA2)[i] = 0.5 * invj * col(F_A2)[i];
+    col(P_XA3)[i] = 0.5 * invj * col(F_A3)[i];
+    col(P_YB1)[i] = 0.5 * invj * col(F_B1)[i];
+    col(P_YB2)[i] = 0.5 * invj * col(F_B2)[i];
+    col(P_ZC1)[i] = 0.5 * invj * col(F_C1)[i];
+    col(P_ZC2)[i] = 0.5 * invj * col(F_C2)[i];
+    col(P_H1)[i] = 0.25 * invj * col(F_HD1)[i];
+    col(P_H2)[i] = 0.25 * invj * col(F_HD2)[i];
+    const double jh = col(F_E1)[i], F = col(C_LYX1F)[i], wm = col(C_WM)[i], wp = col(C_WP)[i];
+    const double ih = col(C_INVHXXF)[i];
+    const double hm = col(C_INVHYXC)[i - 1], h0 = col(C_INVHYXC)[i];
+    const double km = col(C_LYY1)[i - 1], k0 = col(C_LYY1)[i];
+    const double hd1 = col(F_HD1)[i], hd2 = col(F_HD2)[i];
+    col(P_CY1)[i] = invj * (jh * (F * wm - ih) - 2. * hd1 * hm);
+    col(P_CY2)[i] = invj * (jh * (F * wp + ih) - 2. * hd2 * h0);
+    col(P_CA1)[i] = -invj * hd1 * km;
+    col(P_CA2)[i] = -invj * hd2 * k0;
+    col(P_CZ1)[i] = invj * col(F_E2)[i] * ih;
+  }
+  for (int i = 1; i <= nx; i++) {
+    const double invjc = col(C_INVJDXC)[i];
+    col(P_TX0)[i] = 0.5 * invjc * col(C_JF)[i];
+    col(P_TX1)[i] = 0.5 * invjc * col(C_JF)[i + 1];
+    col(P_TY)[i] = 0.5 * invjc * col(C_E1)[i];
+    col(P_TZ)[i] = 0.5 * invjc * col(C_E2)[i];
+    col(P_UA1)[i] = 0.5 * invjc * col(C_A1)[i];
+    col(P_UA2)[i] = 0.5 * invjc * col(C_A2)[i];
+    col(P_UB)[i] = 0.5 * invjc * col(C_B)[i];
+    col(P_UC)[i] = 0.5 * invjc * col(C_CZ)[i];
+    col(P_UH)[i] = 0.25 * invjc * col(C_HD)[i];
+    const double hf0 = col(C_INVHYXF)[i], hf1 = col(C_INVHYXF)[i + 1];
+    const double F0 = col(C_LYX1F)[i], F1 = col(C_LYX1F)[i + 1];
+    const double wm0 = col(C_WM)[i], wp0 = col(C_WP)[i], wm1 = col(C_WM)[i + 1], wp1 = col(C_WP)[i + 1];
+    const double jf0 = col(C_JF)[i], jf1 = col(C_JF)[i + 1];
+    const double hx0 = col(C_INVHXXF)[i], hx1 = col(C_INVHXXF)[i + 1];
+    const double a1 = col(C_HDA1)[i] - jf0, a2 = col(C_HDA2)[i] + jf1;
+    col(P_P1)[i] = invjc * a1 * hf0;
+    col(P_P2)[i] = invjc * a2 * hf1;
+    col(P_QM)[i] = invjc * (a1 * F0 * wm0 - col(C_HDA1)[i] * hx0);
+    col(P_Q0)[i] = invjc * (a1 * F0 * wp0 + a2 * F1 * wm1 + col(C_HDA1)[i] * hx0 - col(C_HDA2)[i] * hx1);
+    col(P_QP)[i] = invjc * (a2 * F1 * wp1 + col(C_HDA2)[i] * hx1);
+    col(P_YK)[i] = invjc * col(C_E1)[i] * col(C_LYY1)[i];
+    col(P_YZ)[i] = invjc * col(C_E2)[i] * col(C_INVHYXC)[i];
+    col(P_ZX0)[i] = invjc * jf0 / hz;
+    col(P_ZX1)[i] = invjc * jf1 / hz;
+    col(P_ZY)[i] = invjc * col(C_E1)[i] / hz;
+  }
   double * dT = dalloc(c, T.size());
   if (!dT) return fail("cudaMalloc of coefficient tables failed");
   CK(cudaMemcpy(dT, T.data(), T.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -264,12 +316,16 @@ static int build_tables(Ctx & c, const domain_t * d) {
   for (int n = 0; n < NCOL; n++) cols[n] = dT + (size_t)n * CSTRIDE;
   Coefs & cf = c.cf;
   cf.tab = dT;
-  const double ** dst[NCOL] = {&cf.f_invjd, &cf.f_a1, &cf.f_a2, &cf.f_a3, &cf.f_b1, &cf.f_b2, &cf.f_c1, &cf.f_c2,
+  // tables reached through named pointers: F_INVJD .. C_PZL (the P_* tables
+  // are read from tab with their offsets)
+  constexpr int NNAMED = C_PZL + 1;
+  const double ** dst[] = {&cf.f_invjd, &cf.f_a1, &cf.f_a2, &cf.f_a3, &cf.f_b1, &cf.f_b2, &cf.f_c1, &cf.f_c2,
       &cf.f_hd1, &cf.f_hd2, &cf.f_lxl, &cf.f_lxc, &cf.f_lxu, &cf.f_lyl, &cf.f_lyc, &cf.f_lyu, &cf.f_e1, &cf.f_e2,
       &cf.c_lyx1f, &cf.c_wm, &cf.c_wp, &cf.c_invhxxf, &cf.c_invhyxc, &cf.c_invhyxf, &cf.c_lyy1, &cf.c_invjdxc,
       &cf.c_a1, &cf.c_a2, &cf.c_b, &cf.c_cz, &cf.c_hd, &cf.c_lxl, &cf.c_lxc, &cf.c_lxu, &cf.c_lyl, &cf.c_lyc,
       &cf.c_lyu, &cf.c_jf, &cf.c_e1, &cf.c_e2, &cf.c_hda1, &cf.c_hda2, &cf.c_pxl, &cf.c_pxu, &cf.c_pyl, &cf.c_pzl};
-  for (int n = 0; n < NCOL; n++) *dst[n] = cols[n];
+  static_assert(sizeof(dst) / sizeof(dst[0]) == NNAMED, "one named pointer per table F_INVJD .. C_PZL");
+  for (int n = 0; n < NNAMED; n++) *dst[n] = cols[n];
   const double lz = 1. / hz / hz;
   cf.lz_l = lz;
   cf.lz_c = -lz - lz;
@@ -490,6 +546,7 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   if (cudaMallocHost(&c->h_status, sizeof(unsigned) * 4) != cudaSuccess) return bad("cudaMallocHost failed");
   if (build_tables(*c, d)) { destroy_ctx(c); return nullptr; }
   poisson_smem_limits();
+  march_smem_limits();
   c->nu = 0.;
   if (set_physics(*c, fl, d)) { destroy_ctx(c); return nullptr; }
   return c;
@@ -559,11 +616,14 @@ static void enqueue_predict(Ctx & c, int rk) {
   const Fields in = c.fb[c.cur];
   const Fields out = c.fb[c.cur ^ 1];
   const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
+  auto predict = [&](int mode) {
+    launch_predict_march(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, mode, c.status, c.st);
+  };
   if (!iy && !iz) {
-    launch_predict(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, PREDICT_APPLY, c.st);
+    predict(PREDICT_APPLY);
     mark(TCGPU_K_PREDICT);
   } else {
-    launch_predict(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, PREDICT_DELTA, c.st);
+    predict(PREDICT_DELTA);
     mark(TCGPU_K_PREDICT);
     if (iy) { launch_ysolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
     if (iz) { launch_zsolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
@@ -643,6 +703,7 @@ static int finish(Ctx & c, const char * what) {
     cudaStreamSynchronize(c.st);
     if (s & ST_NONFINITE) return fail("%s: non-finite velocity in the field", what);
     if (s & ST_BADDT) return fail("%s: invalid time step size", what);
+    if (s & ST_TIMEOUT) return fail("%s: a device copy did not complete within its wait limit", what);
   }
   return 0;
 }

@@ -26,6 +26,25 @@ enum CoefTable {
   F_INVJD, F_A1, F_A2, F_A3, F_B1, F_B2, F_C1, F_C2, F_HD1, F_HD2, F_LXL, F_LXC, F_LXU, F_LYL, F_LYC, F_LYU,
   F_E1, F_E2, C_LYX1F, C_WM, C_WP, C_INVHXXF, C_INVHYXC, C_INVHYXF, C_LYY1, C_INVJDXC, C_A1, C_A2, C_B, C_CZ,
   C_HD, C_LXL, C_LXC, C_LXU, C_LYL, C_LYC, C_LYU, C_JF, C_E1, C_E2, C_HDA1, C_HDA2, C_PXL, C_PXU, C_PYL, C_PZL,
+  // Products of the tables above, one per stencil term of the marching
+  // predict kernel (the viscosity factor stays out, applied in the kernel).
+  // ux at face i:
+  P_XA1, P_XA2, P_XA3,   // 0.5 F_INVJD F_A1..3        advection in x
+  P_YB1, P_YB2,          // 0.5 F_INVJD F_B1..2        advection in y
+  P_ZC1, P_ZC2,          // 0.5 F_INVJD F_C1..2        advection in z
+  P_H1, P_H2,            // 0.25 F_INVJD F_HD1..2      centrifugal term
+  P_CY1, P_CY2,          // uy differences of diffusion_y1 + diffusion_a, / nu
+  P_CA1, P_CA2,          // ux sums of diffusion_a, / nu
+  P_CZ1,                 // uz differences of diffusion_z1, / nu
+  // t at centre i:
+  P_TX0, P_TX1, P_TY, P_TZ,  // 0.5 C_INVJDXC {C_JF(i), C_JF(i+1), C_E1, C_E2}
+  // uy, uz at centre i:
+  P_UA1, P_UA2, P_UB, P_UC,  // 0.5 C_INVJDXC {C_A1, C_A2, C_B, C_CZ}
+  P_UH,                      // 0.25 C_INVJDXC C_HD
+  P_P1, P_P2,                // uy: ux differences of diffusion_x1 + diffusion_a, / nu
+  P_QM, P_Q0, P_QP,          // uy: uy values of diffusion_x1 + diffusion_a, / nu
+  P_YK, P_YZ,                // uy: diffusion_y1, diffusion_z1, / nu
+  P_ZX0, P_ZX1, P_ZY,        // uz: diffusion_x1, diffusion_y1, / nu
   NCOEF_TABLES
 };
 struct Coefs {
@@ -79,7 +98,6 @@ struct Coefs {
   double lz_l, lz_c, lz_u; // Laplacian in z
   double inv_hz;
 };
-constexpr int NCOEF_ARRAYS = NCOEF_TABLES;
 
 // Radial Thomas factors for the three substeps x four variables.
 struct XFactors {
@@ -142,10 +160,14 @@ struct DeltaSet {
   double * d[4];
 };
 enum { PREDICT_APPLY = 0, PREDICT_DELTA = 1 };
-void launch_predict(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu, double kappa,
-                    const Fields & in, const Fields & out, const SrcSet & ss, const DeltaSet & ds,
-                    const double * dtp, int rkstep, int mode, cudaStream_t st);
 int predict_warps(int nx);
+// marching form of the predict stage (tc_march.cu); sets ST_TIMEOUT in
+// *status if a plane's copy does not arrive within its wait limit
+void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
+                          double kappa, const Fields & in, const Fields & out, const SrcSet & ss,
+                          const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
+                          cudaStream_t st);
+void march_smem_limits();
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);
 void launch_apply(const Geo & g, const Bc & bc, const Fields & in, const Fields & out, const DeltaSet & ds,
                   cudaStream_t st);

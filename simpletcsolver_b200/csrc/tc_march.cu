@@ -1,0 +1,764 @@
+// Predict stage: fluid_predict_field (src/fluid/predict/main.c:35-110) for JT
+// neighbouring radial lines (j .. j+JT-1) per CTA, marching through a chunk of
+// KC planes in z. One pass over the fields per substep: right-hand sides of ux
+// (face i), uy, uz, t (centre i), the new explicit source terms, the RK
+// increment delta = dt (alpha srcA + beta srcA_prev + gamma srcG) with srcG
+// (implicit diffusion + pressure gradient) kept in registers, the radial
+// implicit solve (src/tdm.c:17-50), and u + delta into the other buffer of the
+// pair with walls and periodic images (boundary/*.c, halo.c).
+//
+// Per CTA, a ring of three plane slots in shared memory holds the rows
+// j-1 .. j+JT of ux, uy, uz, t, j-1 .. j+JT-1 of p and the previous
+// substep's source terms of the CTA's lines for planes k and k+1, while plane
+// k+2 streams in: one bulk asynchronous copy (cp.async.bulk, completion counted
+// in bytes on an mbarrier) per row, issued one plane ahead by one thread.
+// Values a cell needs from plane k-1 (ux at faces i, i+1; uy at rows j, j+1;
+// uz, p, t at j) are the ones the same thread read one plane earlier and stay
+// in registers; the metric coefficients depend on i only, are folded into one
+// product per stencil term on the host (the P_* tables) and are loaded once
+// per thread. The radial systems of the JT lines are solved one per warp with
+// shuffle scans of affine maps.
+//
+// Row copies start and end on 16-byte boundaries as bulk copies require: a row
+// of n doubles starting at element s is copied from s & ~1 up to the even
+// bound above s + n, and read at offset s & 1. The parity of s depends only on
+// the row's j (ny + 2 is even), so each row keeps one offset for the whole
+// march. Every array holds an even number of doubles, so the widened copies
+// stay inside their allocations. The packed source-term rows of JT (even)
+// consecutive lines start and end on 16-byte boundaries as they are.
+#include <type_traits>
+
+#include "tc_common.cuh"
+#include "tc_kernels.h"
+
+namespace tcgpu {
+namespace {
+
+#define LD(p) __ldg(p)
+
+constexpr int NSLOT = 3;
+// wait limit on a plane's arrival, in SM clock cycles (about two seconds)
+constexpr long long kWaitCycles = 4000000000LL;
+
+__device__ __forceinline__ unsigned smem_u32(const void * p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long * bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long * bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long * bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false if the phase did not complete within kWaitCycles
+__device__ __forceinline__ bool mbar_wait(unsigned long long * bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void bulk_g2s(void * dst, const void * src, unsigned bytes, unsigned long long * bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// fields of a slot, in row-block order
+enum SlotField { SF_UX = 0, SF_UY = 1, SF_UZ = 2, SF_T = 3, SF_P = 4 };
+
+// Two thread groups per radial line: group A (ux at face i, t at centre i)
+// and group B (uy, uz at centre i), each with the coefficients of its own
+// variables in registers, loaded once (they depend on i only). The
+// coefficients are products of the metric tables taken once on the host
+// (P_* tables); each is spelled out below where it is used.
+struct CoefA {
+  double xa1, xa2, xa3, yb1, yb2, zc1, zc2, h1, h2;   // ux advection
+  double lxl, lxc, lxu, lyl, lyc, lyu;                // ux Laplacian, x and y
+  double cy1, cy2, ca1, ca2, cz1, px;                 // ux cross diffusion, pressure gradient
+  double tx0, tx1, ty, tz;                            // t advection
+  double clxl, clxc, clxu, clyl, clyc, clyu;          // t Laplacian, x and y
+};
+struct CoefB {
+  double a1, a2, b, c, h;                             // uy / uz advection
+  double lxl, lxc, lxu, lyl, lyc, lyu;                // centred Laplacian, x and y
+  double p1, p2, qm, q0, qp, yk, yz, py;              // uy cross diffusion, pressure gradient
+  double zx0, zx1, zy;                                // uz cross diffusion
+};
+
+__device__ __forceinline__ void load_coefs(CoefA & q, const Coefs & cf, int i) {
+  const double * __restrict__ b = cf.tab + i;
+#define CF(T) LD(b + (T) * CSTRIDE)
+  q.xa1 = CF(P_XA1); q.xa2 = CF(P_XA2); q.xa3 = CF(P_XA3); q.yb1 = CF(P_YB1); q.yb2 = CF(P_YB2);
+  q.zc1 = CF(P_ZC1); q.zc2 = CF(P_ZC2); q.h1 = CF(P_H1); q.h2 = CF(P_H2);
+  q.lxl = CF(F_LXL); q.lxc = CF(F_LXC); q.lxu = CF(F_LXU); q.lyl = CF(F_LYL); q.lyc = CF(F_LYC); q.lyu = CF(F_LYU);
+  q.cy1 = CF(P_CY1); q.cy2 = CF(P_CY2); q.ca1 = CF(P_CA1); q.ca2 = CF(P_CA2); q.cz1 = CF(P_CZ1);
+  q.px = CF(C_INVHXXF);
+  q.tx0 = CF(P_TX0); q.tx1 = CF(P_TX1); q.ty = CF(P_TY); q.tz = CF(P_TZ);
+  q.clxl = CF(C_LXL); q.clxc = CF(C_LXC); q.clxu = CF(C_LXU); q.clyl = CF(C_LYL); q.clyc = CF(C_LYC);
+  q.clyu = CF(C_LYU);
+#undef CF
+}
+__device__ __forceinline__ void load_coefs(CoefB & q, const Coefs & cf, int i) {
+  const double * __restrict__ b = cf.tab + i;
+#define CF(T) LD(b + (T) * CSTRIDE)
+  q.a1 = CF(P_UA1); q.a2 = CF(P_UA2); q.b = CF(P_UB); q.c = CF(P_UC); q.h = CF(P_UH);
+  q.lxl = CF(C_LXL); q.lxc = CF(C_LXC); q.lxu = CF(C_LXU); q.lyl = CF(C_LYL); q.lyc = CF(C_LYC); q.lyu = CF(C_LYU);
+  q.p1 = CF(P_P1); q.p2 = CF(P_P2); q.qm = CF(P_QM); q.q0 = CF(P_Q0); q.qp = CF(P_QP);
+  q.yk = CF(P_YK); q.yz = CF(P_YZ); q.py = CF(C_INVHYXC);
+  q.zx0 = CF(P_ZX0); q.zx1 = CF(P_ZX1); q.zy = CF(P_ZY);
+#undef CF
+}
+
+// values of plane k-1 a cell needs, carried from the previous plane
+struct PrevA { double ux0, t0; };
+struct PrevB { double ux0, ux1, uy0, uyjp, uz0, p0; };
+
+// A cell's view of two plane slots (k and k+1): base pointers already moved to
+// the cell's radial index (centre arrays at element i, ux at element i - 1,
+// face i sitting at element i - 1 of its row) and, for rows of odd parity, to
+// the widened copy's offset.
+struct SlotView {
+  const double * cb;   // plane k, centre arrays
+  const double * cbo;  // plane k, centre arrays, odd rows
+  const double * fb;   // plane k, ux
+  const double * fbo;  // plane k, ux, odd rows
+  const double * nb;   // plane k+1, centre arrays
+  const double * nbo;
+  const double * nf;   // plane k+1, ux
+  const double * nfo;
+};
+
+// Slot rows: field f, row r (j - 1 + r for the CTA's first line j) starts at
+// (f (JT + 2) + r) RL; odd rows read at the widened copy's offset. JL is the
+// cell's line within the CTA.
+#define ROW_(F, DJ) (((F) * (JT + 2) + JL + 1 + (DJ)) * RL)
+#define ODD_(DJ) (((JL + 1 + (DJ)) & 1) != 0)
+#define UX(DI, DJ) (ODD_(DJ) ? V.fbo : V.fb)[ROW_(SF_UX, DJ) + (DI)]
+#define UY(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_UY, DJ) + (DI)]
+#define UZ(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_UZ, DJ) + (DI)]
+#define TT(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_T, DJ) + (DI)]
+#define PP(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_P, DJ) + (DI)]
+#define NUX(DI) (ODD_(0) ? V.nfo : V.nf)[ROW_(SF_UX, 0) + (DI)]
+#define NUY(DI) (ODD_(0) ? V.nbo : V.nb)[ROW_(SF_UY, 0) + (DI)]
+#define NUZ(DI, DJ) (ODD_(DJ) ? V.nbo : V.nb)[ROW_(SF_UZ, DJ) + (DI)]
+#define NTT(DI) (ODD_(0) ? V.nbo : V.nb)[ROW_(SF_T, 0) + (DI)]
+// diffusion in direction D goes to the implicit part when D is implicit
+#define ROUTE(D, V_) do { if (D) gi += (V_); else e += (V_); } while (0)
+
+// Group A: right-hand sides of ux at face i (src/fluid/predict/ux.c) and t at
+// centre i (t.c) of cell (i, j, k); new source terms to ss.new_, increments
+// dl[0] (ux, 0 at i = 1 where ux has no unknown) and dl[1] (t), current
+// values u0[0] (ux) and u0[1] (t).
+template <int JT, int RL, int JL, int IMPL>
+__device__ __forceinline__ void cell_a(const CoefA & q, const SlotView & V, PrevA & pv, const Bc & bc,
+                                       const Coefs & cf, double nu, double kappa, int i, size_t qf, size_t qc,
+                                       const SrcSet & ss, double ca, double cb, double cg, double old_x,
+                                       double old_t, double dl[2], double u0[2]) {
+  const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
+  const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
+  const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
+  const double ux_0 = UX(0, 0), ux_p = UX(1, 0);
+  const double uy_00 = UY(0, 0), uy_01 = UY(0, 1);
+  const double uz_00 = UZ(0, 0), uz_01 = NUZ(0, 0);
+  dl[0] = 0.;
+  if (i >= 2) {
+    const double ux_m = UX(-1, 0);
+    const double ux_jm = UX(0, -1), ux_jp = UX(0, 1);
+    const double ux_km = pv.ux0, ux_kp = NUX(0);
+    const double uy_m0 = UY(-1, 0), uy_m1 = UY(-1, 1);
+    const double uz_m0 = UZ(-1, 0), uz_m1 = NUZ(-1, 0);
+    double e, gi;
+    // advection (ux.c:92-186): invj (l q_m + c q_0 + u q_p) with c = -l - u,
+    // l = -0.5 (a q_m' + a' q_0'), u = 0.5 (...), as differences from q_0
+    e = (q.xa1 * ux_m + q.xa2 * ux_0) * (ux_m - ux_0) - (q.xa2 * ux_0 + q.xa3 * ux_p) * (ux_p - ux_0);
+    e += (q.yb1 * uy_m0 + q.yb2 * uy_00) * (ux_jm - ux_0) - (q.yb1 * uy_m1 + q.yb2 * uy_01) * (ux_jp - ux_0);
+    e += (q.zc1 * uz_m0 + q.zc2 * uz_00) * (ux_km - ux_0) - (q.zc1 * uz_m1 + q.zc2 * uz_01) * (ux_kp - ux_0);
+    // centrifugal term (:194-226): invj hd (uy averaged to the face)^2
+    const double sm = uy_m0 + uy_m1, sp = uy_00 + uy_01;
+    e += q.h1 * sm * sm + q.h2 * sp * sp;
+    // cross diffusion (:266-375): diffusion_y1 and the uy part of diffusion_a
+    // as differences of uy across j, the ux part of diffusion_a, diffusion_z1
+    e += nu * (q.cy1 * (uy_m1 - uy_m0) + q.cy2 * (uy_01 - uy_00) + q.ca1 * (ux_m + ux_0) +
+               q.ca2 * (ux_0 + ux_p) + q.cz1 * ((uz_01 - uz_m1) - (uz_00 - uz_m0)));
+    // pressure gradient (:377-394)
+    gi = -q.px * (PP(0, 0) - PP(-1, 0));
+    ROUTE(ix, 2. * nu * (q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p));
+    ROUTE(iy, nu * (q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp));
+    ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
+    ss.new_[VUX][qf] = e;
+    dl[0] = ca * e + cb * old_x + cg * gi;
+  }
+  {
+    const double t_0 = TT(0, 0);
+    const double tim = TT(-1, 0), tip = TT(1, 0), tjm = TT(0, -1), tjp = TT(0, 1);
+    const double tkm = pv.t0, tkp = NTT(0);
+    double e, gi = 0.;
+    // advection (t.c:88-116) with face velocities ux_0, ux_p, uy_00, uy_01, uz_00, uz_01
+    e = q.tx0 * ux_0 * (tim - t_0) - q.tx1 * ux_p * (tip - t_0);
+    e += q.ty * uy_00 * (tjm - t_0) - q.ty * uy_01 * (tjp - t_0);
+    e += q.tz * uz_00 * (tkm - t_0) - q.tz * uz_01 * (tkp - t_0);
+    ROUTE(ix, kappa * (q.clxl * tim + q.clxc * t_0 + q.clxu * tip));
+    ROUTE(iy, kappa * (q.clyl * tjm + q.clyc * t_0 + q.clyu * tjp));
+    ROUTE(iz, kappa * (cf.lz_l * tkm + cf.lz_c * t_0 + cf.lz_u * tkp));
+    ss.new_[VT][qc] = e;
+    dl[1] = ca * e + cb * old_t + cg * gi;
+    u0[1] = t_0;
+    pv.t0 = t_0;
+  }
+  u0[0] = ux_0;
+  pv.ux0 = ux_0;
+}
+
+// Group B: right-hand sides of uy (src/fluid/predict/uy.c) and uz (uz.c) at
+// centre i of cell (i, j, k); increments dl[0] (uy), dl[1] (uz), current
+// values u0[0], u0[1].
+template <int JT, int RL, int JL, int IMPL>
+__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView & V, PrevB & pv, const Bc & bc,
+                                       const Coefs & cf, double nu, int i, size_t qc, const SrcSet & ss,
+                                       double ca, double cb, double cg, double old_y, double old_z, double dl[2],
+                                       double u0[2]) {
+  const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
+  const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
+  const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
+  const double ux_0 = UX(0, 0), ux_1 = UX(1, 0);
+  const double uy_0 = UY(0, 0), uy_jp = UY(0, 1);
+  const double uz_0 = UZ(0, 0), uz_kp = NUZ(0, 0);
+  const double p_0 = PP(0, 0);
+  {  // uy
+    const double uy_im = UY(-1, 0), uy_ip = UY(1, 0), uy_jm = UY(0, -1);
+    const double uy_km = pv.uy0, uy_kp = NUY(0);
+    const double ux_0m = UX(0, -1), ux_1m = UX(1, -1);
+    const double uz_jm = UZ(0, -1), uz_jmkp = NUZ(0, -1);
+    double e, gi;
+    // advection (uy.c:93-180), as differences from uy_0
+    e = q.a1 * (ux_0m + ux_0) * (uy_im - uy_0) - q.a2 * (ux_1m + ux_1) * (uy_ip - uy_0);
+    e += q.b * (uy_jm + uy_0) * (uy_jm - uy_0) - q.b * (uy_0 + uy_jp) * (uy_jp - uy_0);
+    e += q.c * (uz_jm + uz_0) * (uy_km - uy_0) - q.c * (uz_jmkp + uz_kp) * (uy_kp - uy_0);
+    // advection_1 (:188-223): -invjc hd (uy ux averaged to j -/+ 1/2)
+    e -= q.h * ((uy_jm + uy_0) * (ux_0m + ux_1m) + (uy_0 + uy_jp) * (ux_0 + ux_1));
+    // diffusion_x1 + diffusion_a (lyx at faces i, i+1 and lxy), diffusion_y1
+    // (lyy1 at j-1, j), diffusion_z1 (lyz at k, k+1)
+    e += nu * (q.p1 * (ux_0 - ux_0m) + q.p2 * (ux_1 - ux_1m) + q.qm * uy_im + q.q0 * uy_0 + q.qp * uy_ip +
+               q.yk * ((ux_0 + ux_1) - (ux_0m + ux_1m)) + q.yz * ((uz_kp - uz_jmkp) - (uz_0 - uz_jm)));
+    gi = -q.py * (p_0 - PP(0, -1));
+    ROUTE(ix, nu * (q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip));
+    ROUTE(iy, 2. * nu * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
+    ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
+    ss.new_[VUY][qc] = e;
+    dl[0] = ca * e + cb * old_y + cg * gi;
+  }
+  {  // uz
+    const double uz_im = UZ(-1, 0), uz_ip = UZ(1, 0), uz_jm = UZ(0, -1), uz_jp = UZ(0, 1);
+    const double uz_km = pv.uz0;
+    const double uy_km = pv.uy0, uy_jpkm = pv.uyjp;
+    const double ux_0k = pv.ux0, ux_1k = pv.ux1;
+    double e, gi;
+    // advection (uz.c:88-180), as differences from uz_0
+    e = q.a1 * (ux_0k + ux_0) * (uz_im - uz_0) - q.a2 * (ux_1k + ux_1) * (uz_ip - uz_0);
+    e += q.b * (uy_km + uy_0) * (uz_jm - uz_0) - q.b * (uy_jpkm + uy_jp) * (uz_jp - uz_0);
+    e += q.c * (uz_km + uz_0) * (uz_km - uz_0) - q.c * (uz_0 + uz_kp) * (uz_kp - uz_0);
+    // diffusion_x1 (lzx at faces i, i+1), diffusion_y1 (lzy at j, j+1)
+    e += nu * (q.zx1 * (ux_1 - ux_1k) - q.zx0 * (ux_0 - ux_0k) + q.zy * ((uy_jp - uy_jpkm) - (uy_0 - uy_km)));
+    gi = -cf.inv_hz * (p_0 - pv.p0);
+    ROUTE(ix, nu * (q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip));
+    ROUTE(iy, nu * (q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp));
+    ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
+    ss.new_[VUZ][qc] = e;
+    dl[1] = ca * e + cb * old_z + cg * gi;
+  }
+  u0[0] = uy_0;
+  u0[1] = uz_0;
+  pv.ux0 = ux_0;
+  pv.ux1 = ux_1;
+  pv.uy0 = uy_0;
+  pv.uyjp = uy_jp;
+  pv.uz0 = uz_0;
+  pv.p0 = p_0;
+}
+#undef ROW_
+#undef ODD_
+#undef UX
+#undef UY
+#undef UZ
+#undef TT
+#undef PP
+#undef NUX
+#undef NUY
+#undef NUZ
+#undef NTT
+#undef ROUTE
+
+template <int E>
+__device__ __forceinline__ int spad(int e) { return E > 1 ? e + e / E : e; }
+
+struct Aff { double a, b; };
+
+// Lane's chunk of a factor row: E consecutive values, as 16-byte pairs when
+// E > 1 (rows start 16-byte aligned and hold at least 32 E values).
+template <int E>
+__device__ __forceinline__ void load_chunk(double (&r)[E], const double * __restrict__ row, int lane) {
+  if constexpr (E == 1) {
+    r[0] = LD(row + lane);
+  } else {
+    const double2 * p2 = reinterpret_cast<const double2 *>(row + lane * E);
+#pragma unroll
+    for (int m = 0; m < E / 2; m++) {
+      const double2 t = __ldg(p2 + m);
+      r[2 * m] = t.x;
+      r[2 * m + 1] = t.y;
+    }
+  }
+}
+
+// Radial Thomas solve of one line by one warp (src/tdm.c:24-48): lane t owns
+// elements tE .. tE+E-1, composes their affine maps, a 5-level shuffle scan
+// supplies the value entering its chunk, then the recurrences run in the
+// reference's form q = w (r - l q_prev) and x = q - v x_next. The factor rows
+// hold w[0] = 1 / c[0] and l[0] = 0, and zeros from n on; the staging line is
+// zero from n on as well, so elements past the end map to zero without tests.
+template <int E>
+__device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int rkstep, int var, int lane) {
+  const size_t fo = (size_t)(rkstep * 4 + var) * xf.stride;
+  double q[E], ll[E], ww[E];
+  load_chunk<E>(ll, xf.lo + fo, lane);
+  load_chunk<E>(ww, xf.w + fo, lane);
+#pragma unroll
+  for (int m = 0; m < E; m++) q[m] = sb[spad<E>(lane * E + m)];
+  Aff acc{1., 0.};
+#pragma unroll
+  for (int m = 0; m < E; m++) {
+    const double fa = -ww[m] * ll[m], fb = ww[m] * q[m];
+    acc.b = fa * acc.b + fb;
+    acc.a = fa * acc.a;
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double oa = __shfl_up_sync(0xffffffffu, acc.a, off);
+    const double ob = __shfl_up_sync(0xffffffffu, acc.b, off);
+    if (lane >= off) { acc.b = acc.a * ob + acc.b; acc.a = acc.a * oa; }
+  }
+  double qin = __shfl_up_sync(0xffffffffu, acc.b, 1);
+  if (lane == 0) qin = 0.;
+#pragma unroll
+  for (int m = 0; m < E; m++) {
+    const double r = ww[m] * (q[m] - ll[m] * qin);
+    q[m] = r;
+    qin = r;
+  }
+  double vv[E];
+  load_chunk<E>(vv, xf.v + fo, lane);
+  Aff bac{1., 0.};
+#pragma unroll
+  for (int m = E - 1; m >= 0; m--) {
+    bac.b = -vv[m] * bac.b + q[m];
+    bac.a = -vv[m] * bac.a;
+  }
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double oa = __shfl_down_sync(0xffffffffu, bac.a, off);
+    const double ob = __shfl_down_sync(0xffffffffu, bac.b, off);
+    if (lane + off < 32) { bac.b = bac.a * ob + bac.b; bac.a = bac.a * oa; }
+  }
+  double xin = __shfl_down_sync(0xffffffffu, bac.b, 1);
+  if (lane == 31) xin = 0.;
+#pragma unroll
+  for (int m = E - 1; m >= 0; m--) {
+    const double x = q[m] - vv[m] * xin;
+    sb[spad<E>(lane * E + m)] = x;
+    xin = x;
+  }
+}
+
+// Shared-memory layout in doubles, shared by the kernel and its launcher. Row
+// buffers are sized for the widest radial line of the warp count (nx <= 32 NW),
+// so every stencil offset is a compile-time constant.
+template <int NW, int JT>
+struct MarchLayout {
+  static_assert(JT == 2 || JT == 4, "line groups start at odd j, so rows of even index have even j");
+  static constexpr int E = NW;
+  static constexpr int RL = 32 * NW + 4;                 // >= nx + 4, even
+  static constexpr int NROW = 4 * (JT + 2) + (JT + 1);   // ux, uy, uz, t: JT + 2 rows; p: JT + 1
+  static constexpr int OLD = NROW * RL;                  // then the previous substep's source terms:
+  static constexpr int SLOT = OLD + 4 * JT * RL;         // JT packed lines per variable, at OLD + v JT RL
+  static constexpr int SL = 32 * E + (E > 1 ? 32 : 0);   // staging line (padded for the solves)
+  static constexpr int STAGE = NSLOT * SLOT;             // [2][JT][4][SL] after the ring
+  static constexpr int BAR = STAGE + 2 * JT * 4 * SL;    // NSLOT mbarriers after the staging
+  static constexpr size_t BYTES = sizeof(double) * (size_t)BAR + NSLOT * sizeof(unsigned long long);
+};
+
+// Everything a group's march needs besides its coefficients.
+struct MarchArgs {
+  Geo g;
+  Bc bc;
+  Coefs cf;
+  XFactors xf;
+  double nu, kappa;
+  Fields in, out;
+  SrcSet ss;
+  DeltaSet ds;
+  int rkstep, mode, KC;
+  unsigned * status;
+};
+
+// The plane loop of one thread group: G = 0 computes ux and t, G = 1 uy and
+// uz, G = 2 all four (one group per line). With two groups both pass the same
+// barriers in the same order.
+template <int NW, int JT, int IMPL, int G>
+__device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, double * stage,
+                                            unsigned long long * bar, int j0, int k0, int k1, double dt) {
+  using L = MarchLayout<NW, JT>;
+  constexpr int E = L::E, RL = L::RL, SL = L::SL, NT = 32 * NW;
+  constexpr bool GA = G != 1, GB = G != 0;   // group computes ux and t / uy and uz
+  constexpr int NGRP = G == 2 ? 1 : 2;
+  const Geo & g = A.g;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int tx = threadIdx.x;
+  const int lane = tx & 31, wid = tx >> 5;
+  const int i = tx - (G == 1 ? NT : 0) + 1;
+  const bool act = i <= nx;
+  const int of = (nx + 1) & 1, oc = (nx + 2) & 1;
+  const size_t sjc = (size_t)ny + 2;
+
+  // Copies of plane kp into slot sl: the field rows and, for planes that are
+  // computed in a substep with beta != 0, the source terms of the previous
+  // substep at the JT lines (consecutive in the packed layout, 16-byte
+  // aligned as JT is even).
+  const bool use_old = A.rkstep != 0;
+  auto issue = [&](int kp, int sl) {
+    double * base = ring + (size_t)sl * L::SLOT;
+    const double * src[5] = {A.in.ux, A.in.uy, A.in.uz, A.in.t, A.in.p};
+    const bool olds = use_old && kp >= k0 && kp < k1;
+    unsigned total = 0;
+    for (int f = 0; f < 5; f++) {
+      const size_t n = (f == SF_UX) ? (size_t)nx + 1 : (size_t)nx + 2;
+      for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
+        const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
+        const size_t a = s0 & ~(size_t)1, b = (s0 + n + 1) & ~(size_t)1;
+        total += (unsigned)((b - a) * sizeof(double));
+      }
+    }
+    if (olds) total += (unsigned)(JT * (4 * nx - 1) * sizeof(double));
+    mbar_expect_tx(&bar[sl], total);
+    if (olds) {
+      for (int v = 0; v < 4; v++) {
+        const int ni = (v == VUX) ? nx - 1 : nx;
+        bulk_g2s(base + L::OLD + (size_t)v * JT * RL, A.ss.old_[v] + pidx(ni, ny, 0, j0, kp),
+                 (unsigned)(JT * ni * sizeof(double)), &bar[sl]);
+      }
+    }
+    for (int f = 0; f < 5; f++) {
+      const size_t n = (f == SF_UX) ? (size_t)nx + 1 : (size_t)nx + 2;
+      for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
+        const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
+        const size_t a = s0 & ~(size_t)1, b = (s0 + n + 1) & ~(size_t)1;
+        bulk_g2s(base + (size_t)(f * (JT + 2) + r) * RL, src[f] + a, (unsigned)((b - a) * sizeof(double)),
+                 &bar[sl]);
+      }
+    }
+  };
+  if (tx == 0) {
+    issue(k0 - 1, 0);
+    issue(k0, 1);
+    issue(k0 + 1, 2);
+  }
+  unsigned par[NSLOT] = {0u, 0u, 0u};
+  bool late = false;
+  auto wait_slot = [&](int sl) {
+    if (!mbar_wait(&bar[sl], par[sl])) late = true;
+    par[sl] ^= 1u;
+  };
+
+  CoefA qa;
+  CoefB qb;
+  if constexpr (GA) load_coefs(qa, A.cf, act ? i : 1);
+  if constexpr (GB) load_coefs(qb, A.cf, act ? i : 1);
+  const int rk = A.rkstep;
+  const double ca = rk_alpha(rk) * dt, cb = rk_beta(rk) * dt, cg = rk_gamma(rk) * dt;
+
+  // plane k0 - 1: the carried values
+  wait_slot(0);
+  wait_slot(1);
+  PrevA pa[JT];
+  PrevB pb[JT];
+  if (act) {
+    const double * cbs = ring + i, * fbs = ring + i - 1;
+#pragma unroll
+    for (int jl = 0; jl < JT; jl++) {
+      const int r1 = jl + 1, r2 = jl + 2;   // rows j and j + 1
+      const int o1c = (r1 & 1) ? oc : 0, o1f = (r1 & 1) ? of : 0, o2c = (r2 & 1) ? oc : 0;
+      if constexpr (GA) {
+        pa[jl].ux0 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f];
+        pa[jl].t0 = cbs[(SF_T * (JT + 2) + r1) * RL + o1c];
+      }
+      if constexpr (GB) {
+        pb[jl].ux0 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f];
+        pb[jl].ux1 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f + 1];
+        pb[jl].uy0 = cbs[(SF_UY * (JT + 2) + r1) * RL + o1c];
+        pb[jl].uyjp = cbs[(SF_UY * (JT + 2) + r2) * RL + o2c];
+        pb[jl].uz0 = cbs[(SF_UZ * (JT + 2) + r1) * RL + o1c];
+        pb[jl].p0 = cbs[(SF_P * (JT + 2) + r1) * RL + o1c];
+      }
+    }
+  }
+  __syncthreads();
+
+  const bool solve_x = IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0;
+  for (int k = k0; k < k1; k++) {
+    const int step = k - k0;
+    const int cur = (step + 1) % NSLOT, nxt = (step + 2) % NSLOT, fre = step % NSLOT;
+    // plane k + 2 into the slot of plane k - 1, which every thread finished
+    // reading before the previous plane's first barrier
+    if (tx == 0 && k + 2 <= k1) {
+      fence_async_smem();
+      issue(k + 2, fre);
+    }
+    wait_slot(nxt);
+    double * sdb = stage + (size_t)(step & 1) * JT * 4 * SL;
+    double dl[JT][4], u0[JT][4];   // indexed by Var
+#pragma unroll
+    for (int jl = 0; jl < JT; jl++)
+#pragma unroll
+      for (int v = 0; v < 4; v++) dl[jl][v] = u0[jl][v] = 0.;
+    if (act) {
+      SlotView V;
+      V.cb = ring + (size_t)cur * L::SLOT + i;
+      V.cbo = V.cb + oc;
+      V.fb = V.cb - 1;
+      V.fbo = V.fb + of;
+      V.nb = ring + (size_t)nxt * L::SLOT + i;
+      V.nbo = V.nb + oc;
+      V.nf = V.nb - 1;
+      V.nfo = V.nf + of;
+      const size_t qf = pidx(nx - 1, ny, i - 2, j0, k), qc = pidx(nx, ny, i - 1, j0, k);
+      const double * ob = ring + (size_t)cur * L::SLOT + L::OLD;   // old source terms of plane k
+      auto cells = [&](auto jlc) {
+        constexpr int JL = decltype(jlc)::value;
+        double d2[2], w2[2];
+        auto old = [&](int v, int e) {
+          return use_old ? ob[v * JT * RL + JL * (v == VUX ? nx - 1 : nx) + e] : 0.;
+        };
+        if constexpr (GA) {
+          cell_a<JT, RL, JL, IMPL>(qa, V, pa[JL], A.bc, A.cf, A.nu, A.kappa, i, qf + (size_t)JL * (nx - 1),
+                                   qc + (size_t)JL * nx, A.ss, ca, cb, cg, i >= 2 ? old(VUX, i - 2) : 0.,
+                                   old(VT, i - 1), d2, w2);
+          dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
+        }
+        if constexpr (GB) {
+          cell_b<JT, RL, JL, IMPL>(qb, V, pb[JL], A.bc, A.cf, A.nu, i, qc + (size_t)JL * nx, A.ss, ca, cb, cg,
+                                   old(VUY, i - 1), old(VUZ, i - 1), d2, w2);
+          dl[JL][VUY] = d2[0]; dl[JL][VUZ] = d2[1]; u0[JL][VUY] = w2[0]; u0[JL][VUZ] = w2[1];
+        }
+      };
+      cells(std::integral_constant<int, 0>());
+      cells(std::integral_constant<int, 1>());
+      if constexpr (JT == 4) {
+        cells(std::integral_constant<int, 2>());
+        cells(std::integral_constant<int, 3>());
+      }
+    }
+    // staging positions: ux unknowns are faces 2..nx (element i - 2), the
+    // centred ones cells 1..nx (element i - 1)
+    if (solve_x) {
+      if (act) {
+#pragma unroll
+        for (int jl = 0; jl < JT; jl++) {
+          double * s = sdb + (size_t)jl * 4 * SL;
+          if constexpr (GA) {
+            if (i >= 2) s[VUX * SL + spad<E>(i - 2)] = dl[jl][VUX];
+            s[VT * SL + spad<E>(i - 1)] = dl[jl][VT];
+          }
+          if constexpr (GB) {
+            s[VUY * SL + spad<E>(i - 1)] = dl[jl][VUY];
+            s[VUZ * SL + spad<E>(i - 1)] = dl[jl][VUZ];
+          }
+        }
+      }
+      __syncthreads();
+      for (int s = wid; s < 4 * JT; s += NGRP * NW) solve_line<E>(sdb + (size_t)s * SL, A.xf, rk, s & 3, lane);
+      __syncthreads();
+      if (act) {
+#pragma unroll
+        for (int jl = 0; jl < JT; jl++) {
+          const double * s = sdb + (size_t)jl * 4 * SL;
+          if constexpr (GA) {
+            dl[jl][VUX] = (i >= 2) ? s[VUX * SL + spad<E>(i - 2)] : 0.;
+            dl[jl][VT] = s[VT * SL + spad<E>(i - 1)];
+          }
+          if constexpr (GB) {
+            dl[jl][VUY] = s[VUY * SL + spad<E>(i - 1)];
+            dl[jl][VUZ] = s[VUZ * SL + spad<E>(i - 1)];
+          }
+        }
+      }
+    } else {
+      // no radial solve: this barrier alone orders the plane's slot reads
+      // before the copy into that slot two planes on
+      __syncthreads();
+    }
+    if (!act) continue;
+#pragma unroll
+    for (int jl = 0; jl < JT; jl++) {
+      const int j = j0 + jl;
+      if (A.mode == PREDICT_DELTA) {
+        const size_t qc = pidx(nx, ny, i - 1, j, k);
+        if constexpr (GA) {
+          if (i >= 2) A.ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] = dl[jl][VUX];
+          A.ds.d[VT][qc] = dl[jl][VT];
+        }
+        if constexpr (GB) {
+          A.ds.d[VUY][qc] = dl[jl][VUY];
+          A.ds.d[VUZ][qc] = dl[jl][VUZ];
+        }
+        continue;
+      }
+      // u += delta into the other buffer, walls (boundary/*.c) and images (halo.c)
+      const double vx = (i < 2) ? 0. : u0[jl][VUX] + dl[jl][VUX];
+      const double vt = u0[jl][VT] + dl[jl][VT];
+      const double vy = u0[jl][VUY] + dl[jl][VUY];
+      const double vz = u0[jl][VUZ] + dl[jl][VUZ];
+      auto put = [&](int jj, int kk) {
+        if constexpr (GA) {
+          A.out.ux[fidx(g, i, jj, kk)] = vx;
+          A.out.t[cidx(g, i, jj, kk)] = vt;
+          if (i == 1) A.out.t[cidx(g, 0, jj, kk)] = A.bc.t_xm;
+          if (i == nx) {
+            A.out.ux[fidx(g, nx + 1, jj, kk)] = 0.;
+            A.out.t[cidx(g, nx + 1, jj, kk)] = A.bc.t_xp;
+          }
+        }
+        if constexpr (GB) {
+          A.out.uy[cidx(g, i, jj, kk)] = vy;
+          A.out.uz[cidx(g, i, jj, kk)] = vz;
+          if (i == 1) {
+            A.out.uy[cidx(g, 0, jj, kk)] = A.bc.uy_xm;
+            A.out.uz[cidx(g, 0, jj, kk)] = 0.;
+          }
+          if (i == nx) {
+            A.out.uy[cidx(g, nx + 1, jj, kk)] = A.bc.uy_xp;
+            A.out.uz[cidx(g, nx + 1, jj, kk)] = 0.;
+          }
+        }
+      };
+      put(j, k);
+      for_images(j, k, ny, nz, put);
+    }
+  }
+  if (late) atomicOr(A.status, ST_TIMEOUT);
+}
+
+// Thread groups per line. With 2, ux and t are computed by one thread and uy
+// and uz by another, so the coefficients of each fit in 128 registers and twice
+// as many warps are resident; measured at 256 x 1024 x 512 the single group
+// (up to 255 registers, 8 warps per SM) is faster (7.9 against 9.4 ms per
+// launch, the two groups waiting on each other at the barriers).
+#ifndef TC_MARCH_GROUPS
+#define TC_MARCH_GROUPS 1
+#endif
+// NG groups of 32 NW threads, one thread per radial index in each; CTA = JT
+// lines (j0 .. j0+JT-1) x KC planes.
+template <int NW, int JT, int IMPL>
+__global__ void __launch_bounds__(32 * NW * TC_MARCH_GROUPS, 1)
+march_predict_kernel(MarchArgs A, const double * __restrict__ dtp) {
+  using L = MarchLayout<NW, JT>;
+  extern __shared__ __align__(16) double sm[];
+  double * ring = sm;
+  double * stage = sm + L::STAGE;
+  unsigned long long * bar = reinterpret_cast<unsigned long long *>(sm + L::BAR);
+  const int tx = threadIdx.x;
+  const int njg = A.g.ny / JT;
+  const int j0 = (int)(blockIdx.x % njg) * JT + 1;   // odd
+  const int k0 = (int)(blockIdx.x / njg) * A.KC + 1;
+  const int k1 = k0 + A.KC;   // planes k0 .. k1-1 are computed; k0-1 .. k1 are read
+  if (tx == 0) {
+    for (int s = 0; s < NSLOT; s++) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  // staging lines are zero past each line's unknowns for the whole march
+  for (int e = tx; e < 2 * JT * 4 * L::SL; e += blockDim.x) stage[e] = 0.;
+  __syncthreads();
+  const double dt = *dtp;
+  if constexpr (TC_MARCH_GROUPS == 1) {
+    march_group<NW, JT, IMPL, 2>(A, ring, stage, bar, j0, k0, k1, dt);
+  } else {
+    if (tx < 32 * NW) march_group<NW, JT, IMPL, 0>(A, ring, stage, bar, j0, k0, k1, dt);
+    else march_group<NW, JT, IMPL, 1>(A, ring, stage, bar, j0, k0, k1, dt);
+  }
+}
+
+#ifndef TC_MARCH_JT
+#define TC_MARCH_JT 2
+#endif
+#ifndef TC_MARCH_KC
+#define TC_MARCH_KC 32
+#endif
+
+template <int NW>
+void launch_march_nw(const MarchArgs & A, const double * dtp, cudaStream_t st) {
+  constexpr int JT = TC_MARCH_JT;   // ny is a power of two >= 4
+  const long long nblk = (long long)(A.g.ny / JT) * (A.g.nz / A.KC);
+  const int mask = (A.bc.implicit[0] ? 1 : 0) | (A.bc.implicit[1] ? 2 : 0) | (A.bc.implicit[2] ? 4 : 0);
+  const unsigned grid = (unsigned)nblk, block = 32 * NW * TC_MARCH_GROUPS;
+  const size_t smem = MarchLayout<NW, JT>::BYTES;
+  switch (mask) {
+    case 1: march_predict_kernel<NW, JT, 1><<<grid, block, smem, st>>>(A, dtp); break;
+    case 7: march_predict_kernel<NW, JT, 7><<<grid, block, smem, st>>>(A, dtp); break;
+    case 0: march_predict_kernel<NW, JT, 0><<<grid, block, smem, st>>>(A, dtp); break;
+    default: march_predict_kernel<NW, JT, -1><<<grid, block, smem, st>>>(A, dtp); break;
+  }
+}
+
+template <int NW>
+void allow_march_smem() {
+  constexpr int JT = TC_MARCH_JT;
+  const int bytes = (int)MarchLayout<NW, JT>::BYTES;
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+}  // namespace
+
+void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
+                          double kappa, const Fields & in, const Fields & out, const SrcSet & ss,
+                          const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
+                          cudaStream_t st) {
+  MarchArgs A{g, bc, cf, xf, nu, kappa, in, out, ss, ds, rkstep, mode, g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC,
+              status};
+  switch (predict_warps(g.nx)) {
+    case 1: launch_march_nw<1>(A, dtp, st); break;
+    case 2: launch_march_nw<2>(A, dtp, st); break;
+    case 4: launch_march_nw<4>(A, dtp, st); break;
+    default: launch_march_nw<8>(A, dtp, st); break;
+  }
+}
+
+void march_smem_limits() {
+  allow_march_smem<1>();
+  allow_march_smem<2>();
+  allow_march_smem<4>();
+  allow_march_smem<8>();
+}
+
+}  // namespace tcgpu
