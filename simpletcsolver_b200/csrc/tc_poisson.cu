@@ -22,6 +22,8 @@
 // Spectral layout: spec[i][kz][ky] (ky fastest), so the y and z transforms read
 // and write rows of contiguous wavenumbers and the radial solve, one thread per
 // (kz, ky) line, walks i with fully coalesced steps.
+#include <type_traits>
+
 #include "tc_common.cuh"
 #include "tc_kernels.h"
 
@@ -70,9 +72,22 @@ __host__ __device__ constexpr int brev(int a) {
   return b;
 }
 
+// exp(-2 pi i m / 16), m = 0 .. 7: the twiddles inside the 16-point DFTs,
+// cos and sin of multiples of pi/8 (sqrt(2 + sqrt 2)/2, sqrt(2)/2,
+// sqrt(2 - sqrt 2)/2), correctly rounded
+__device__ constexpr double kC1 = 0.92387953251128674, kC2 = 0.70710678118654752, kC3 = 0.38268343236508977;
+template <int SIGN>
+__device__ __forceinline__ double2 twid16(int m) {
+  const double c = m == 0 ? 1. : m == 1 ? kC1 : m == 2 ? kC2 : m == 3 ? kC3 : m == 4 ? 0. : m == 5 ? -kC3
+                 : m == 6 ? -kC2 : -kC1;
+  const double sn = m == 0 ? 0. : m == 1 ? kC3 : m == 2 ? kC2 : m == 3 ? kC1 : m == 4 ? 1. : m == 5 ? kC1
+                  : m == 6 ? kC2 : kC3;
+  return make_double2(c, SIGN < 0 ? -sn : sn);
+}
+
 // In-register DFT of R points: v[s] <- sum_r v[r] exp(SIGN 2 pi i r s / R),
 // iterative radix-2 decimation in time; twiddles exp(SIGN 2 pi i k / len) are
-// tw[k N / len] of the length-N table.
+// compile-time constants (R <= 16).
 template <int R, int SIGN>
 __device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict__ tw, int N) {
 #pragma unroll
@@ -90,7 +105,7 @@ __device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict_
 #pragma unroll
     for (int k = 0; k < half; k++) {
       double2 w = make_double2(1., 0.);
-      if (k != 0 && 4 * k != len) w = twid<SIGN>(tw, k * (N / len));
+      if (k != 0 && 4 * k != len) w = twid16<SIGN>(k * (16 / len));
 #pragma unroll
       for (int s = 0; s < R; s += len) {
         const double2 a = v[s + k];
@@ -159,6 +174,87 @@ __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const do
     }
     Ns <<= rl;
     left -= rl;
+  }
+}
+
+// Stockham pass reading its inputs from the global column g (IN) instead of
+// the shared line, and/or writing its outputs there (OUT): the first and last
+// passes of the z transforms, so the data crosses shared memory only between
+// passes. Column element e sits at g[e gs]; gv false (a padding line past the
+// last wavenumber) reads zeros and writes nothing. A pass that reads and
+// writes the shared line synchronises like stockham_pass.
+template <int R, int B, int SIGN, bool IN, bool OUT>
+__device__ __forceinline__ void stockham_pass_io(double2 * x, double2 * g, size_t gs, bool gv, int N, int Ns,
+                                                 int t, int TPL, const double2 * __restrict__ tw) {
+  double2 v[B][R];
+  const int NR = N / R;
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * TPL;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      if (IN) v[b][r] = gv ? g[(size_t)(j + r * NR) * gs] : make_double2(0., 0.);
+      else v[b][r] = x[pad(j + r * NR)];
+    }
+  }
+  if (!IN && !OUT) __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int j = t + b * TPL;
+    const int k = j & (Ns - 1);
+    if (Ns > 1) {
+      const int step = k * (N / (Ns * R));
+#pragma unroll
+      for (int r = 1; r < R; r++) v[b][r] = cmul(v[b][r], twid<SIGN>(tw, r * step));
+    }
+    dft_reg<R, SIGN>(v[b], tw, N);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      if (OUT) {
+        if (gv) g[(size_t)(base + r * Ns) * gs] = v[b][r];
+      } else {
+        x[pad(base + r * Ns)] = v[b][r];
+      }
+    }
+  }
+  if (!OUT) __syncthreads();
+}
+
+// Full transform of one column held in global memory (N = 2^lg), in place:
+// the first pass reads the column, the last writes it, the passes between go
+// through the shared line x.
+template <int EPT, int SIGN>
+__device__ void fft_direct(double2 * x, double2 * g, size_t gs, bool gv, int N, int lg, int t, int TPL,
+                           const double2 * __restrict__ tw) {
+  int Ns = 1;
+  int left = lg;
+  auto pass = [&](auto rc, auto bc) {
+    constexpr int R = decltype(rc)::value, B = decltype(bc)::value;
+    const bool first = Ns == 1, last = left == 0;
+    if (first && last) stockham_pass_io<R, B, SIGN, true, true>(x, g, gs, gv, N, Ns, t, TPL, tw);
+    else if (first) stockham_pass_io<R, B, SIGN, true, false>(x, g, gs, gv, N, Ns, t, TPL, tw);
+    else if (last) stockham_pass_io<R, B, SIGN, false, true>(x, g, gs, gv, N, Ns, t, TPL, tw);
+    else stockham_pass_io<R, B, SIGN, false, false>(x, g, gs, gv, N, Ns, t, TPL, tw);
+  };
+  using I = int;
+  while (left > 0) {
+    const int rl = left >= 4 ? 4 : left;
+    left -= rl;
+    if (EPT == 16) {
+      if (rl == 4) pass(std::integral_constant<I, 16>(), std::integral_constant<I, 1>());
+      else if (rl == 3) pass(std::integral_constant<I, 8>(), std::integral_constant<I, 2>());
+      else if (rl == 2) pass(std::integral_constant<I, 4>(), std::integral_constant<I, 4>());
+      else pass(std::integral_constant<I, 2>(), std::integral_constant<I, 8>());
+    } else if (EPT == 8) {
+      if (rl == 3) pass(std::integral_constant<I, 8>(), std::integral_constant<I, 1>());
+      else if (rl == 2) pass(std::integral_constant<I, 4>(), std::integral_constant<I, 2>());
+      else pass(std::integral_constant<I, 2>(), std::integral_constant<I, 4>());
+    } else {
+      if (rl == 2) pass(std::integral_constant<I, 4>(), std::integral_constant<I, 1>());
+      else pass(std::integral_constant<I, 2>(), std::integral_constant<I, 2>());
+    }
+    Ns <<= rl;
   }
 }
 
@@ -244,13 +340,13 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
   fft_inplace<EPT, -1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
-  // separate the two real transforms and store the ny/2+1 non-negative wavenumbers
-  const int nyh = ps.nyh;
-  for (int idx = threadIdx.x; idx < TI * nyh; idx += blockDim.x) {
-    const int m = idx % nyh;
-    const int ii = idx / nyh;
+  // separate the two real transforms and store the ny/2+1 non-negative
+  // wavenumbers: m < ny/2 for every radial index (power-of-two index
+  // arithmetic), then the Nyquist terms
+  const int nyh = ps.nyh, half = ny >> 1;
+  auto put = [&](int ii, int m) {
     const int i = i0 + ii;
-    if (i > nx) continue;
+    if (i > nx) return;
     const double2 * z = smem + (size_t)(ii >> 1) * LS;
     const double2 zm = z[pad(m)];
     const double2 zn = z[pad((ny - m) & (ny - 1))];
@@ -258,11 +354,16 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
     if ((ii & 1) == 0) out = make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y - zn.y));
     else out = make_double2(0.5 * (zm.y + zn.y), -0.5 * (zm.x - zn.x));
     ps.spec[((size_t)(i - 1) * nz + (k - 1)) * nyh + m] = out;
-  }
+  };
+  for (int idx = threadIdx.x; idx < TI * half; idx += blockDim.x) put(idx >> (lg - 1), idx & (half - 1));
+  if ((int)threadIdx.x < TI) put(threadIdx.x, half);
 }
 
 // --------------------------------------------------------------- z transforms
-// CTA: P lines (wavenumbers m0 .. m0+P-1) of one radial index, all kz.
+// CTA: P lines (wavenumbers m0 .. m0+P-1) of one radial index, all kz. Thread
+// (p, t) = (tid mod P, tid / P): lanes run along the contiguous wavenumbers, so
+// the first pass reads and the last pass writes rows of P values straight from
+// and to the spectral array.
 template <int EPT, int SIGN>
 __global__ void __launch_bounds__(256, TC_FFTZ_MIN_BLOCKS)
 fftz_kernel(Geo g, Poisson ps, int P, int lg) {
@@ -271,26 +372,10 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   const int TPL = nz / EPT;
   const int LS = padded_len(nz);
   const int i = blockIdx.x;          // 0..nx-1
-  const int m0 = blockIdx.y * P;
-  double2 * base = ps.spec + (size_t)i * nz * nyh;
-  // P nz = blockDim EPT: each thread moves EPT values of one wavenumber m
-  // (P divides the block size), all loads in flight together
-  const int mm = threadIdx.x % P;
-  const int kz0 = threadIdx.x / P;
-  const int kstep = blockDim.x / P;
-  const int m = m0 + mm;
-#pragma unroll
-  for (int r = 0; r < EPT; r++)
-    smem[(size_t)mm * LS + pad(kz0 + r * kstep)] =
-        (m < nyh) ? base[(size_t)(kz0 + r * kstep) * nyh + m] : make_double2(0., 0.);
-  __syncthreads();
-  const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  fft_inplace<EPT, SIGN>(smem + (size_t)p * LS, nz, lg, t, TPL, ps.tw_z);
-  if (m < nyh) {
-#pragma unroll
-    for (int r = 0; r < EPT; r++)
-      base[(size_t)(kz0 + r * kstep) * nyh + m] = smem[(size_t)mm * LS + pad(kz0 + r * kstep)];
-  }
+  const int p = threadIdx.x % P, t = threadIdx.x / P;
+  const int m = blockIdx.y * P + p;
+  double2 * col = ps.spec + (size_t)i * nz * nyh + m;
+  fft_direct<EPT, SIGN>(smem + (size_t)p * LS, col, (size_t)nyh, m < nyh, nz, lg, t, TPL, ps.tw_z);
 }
 
 // --------------------------------------------------------------- radial solve
@@ -411,8 +496,8 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
 #pragma unroll 8
   for (int r = 0; r < EPT; r++) {
     const int idx = threadIdx.x + r * blockDim.x;
-    const int m = idx % ny;
-    const int pp = idx / ny;
+    const int m = idx & (ny - 1);
+    const int pp = idx >> lg;
     const int ia = i0 + 2 * pp, ib = ia + 1;
     const int mr = (m <= ny / 2) ? m : ny - m;
     double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
@@ -429,14 +514,16 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   fft_inplace<EPT, +1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
   // one radial index per thread when TI divides the block size (ny >= 2 EPT),
   // else the plain element loop
+  // (TI and the block size are powers of two)
+  const int lgt = __ffs(TI) - 1;
   const bool fixed_i = blockDim.x % TI == 0;
   const int nr = fixed_i ? 2 * EPT : (TI * ny + blockDim.x - 1) / blockDim.x;
 #pragma unroll 4
   for (int r = 0; r < nr; r++) {
     const int idx = fixed_i ? threadIdx.x : threadIdx.x + r * blockDim.x;
     if (idx >= TI * ny) break;
-    const int ii = idx % TI;
-    const int j = fixed_i ? idx / TI + 1 + r * (blockDim.x / TI) : idx / TI + 1;
+    const int ii = idx & (TI - 1);
+    const int j = fixed_i ? (idx >> lgt) + 1 + r * (blockDim.x >> lgt) : (idx >> lgt) + 1;
     const int i = i0 + ii;
     if (i > nx) continue;
     const double2 z = smem[(size_t)(ii >> 1) * LS + pad(j - 1)];
