@@ -58,7 +58,7 @@ BYTES_PER_CELL = {
     "IFFTY": 8 + 8,                            # spectrum read, psi written
     "CORRECT": 9 * 8,                          # psi, ux, uy, uz, p read; ux, uy, uz, p written
 }
-MODEL_BYTES_PER_CELL_STEP = 936.0              # minimum-pass model of the whole step (FP64)
+MODEL_BYTES_PER_CELL_STEP = 912
 
 
 def parse_args(argv=None):

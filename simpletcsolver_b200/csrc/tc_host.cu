@@ -75,6 +75,10 @@ struct Ctx {
   double * dt_caps = nullptr;
   double * dtp = nullptr;
   unsigned long long * dtmin = nullptr;
+  // dtmin holds the advective limit of the current fields, folded in by the
+  // last correction of the previous step (reset to 1.0 whenever that stops
+  // being true)
+  bool dt_ready = false;
   unsigned * status = nullptr;
   double * diag_out = nullptr;
   double * diag_part = nullptr;
@@ -535,13 +539,14 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   }
   c->dt_caps = dalloc(*c, 3);
   c->dtp = dalloc(*c, 1);
-  c->dtmin = reinterpret_cast<unsigned long long *>(dalloc(*c, 1));
+  c->dtmin = reinterpret_cast<unsigned long long *>(dalloc(*c, DT_SLOTS));
   c->status = reinterpret_cast<unsigned *>(dalloc(*c, 1));
   c->diag_out = dalloc(*c, 16);
   c->diag_part = dalloc(*c, (size_t)DIAG_BLOCKS_MAX * 9);
   if (!c->dt_caps || !c->dtp || !c->dtmin || !c->status || !c->diag_out || !c->diag_part) return bad("cudaMalloc failed");
-  const unsigned long long one = 0x3ff0000000000000ull;
-  if (cudaMemcpy(c->dtmin, &one, sizeof(one), cudaMemcpyHostToDevice) != cudaSuccess) return bad("cudaMemcpy failed");
+  const std::vector<unsigned long long> ones(DT_SLOTS, 0x3ff0000000000000ull);   // 1.0
+  if (cudaMemcpy(c->dtmin, ones.data(), DT_SLOTS * sizeof(ones[0]), cudaMemcpyHostToDevice) != cudaSuccess)
+    return bad("cudaMemcpy failed");
   if (cudaMallocHost(&c->h_scalar, 64 * sizeof(double)) != cudaSuccess) return bad("cudaMallocHost failed");
   if (cudaMallocHost(&c->h_status, sizeof(unsigned) * 4) != cudaSuccess) return bad("cudaMallocHost failed");
   if (build_tables(*c, d)) { destroy_ctx(c); return nullptr; }
@@ -644,25 +649,32 @@ static void enqueue_potential(Ctx & c, int rk) {
   launch_poisson(c.g, c.cf, c.ps, c.f(), c.tab_y, c.tab_z, c.base, c.dtp, rk, c.st, pm);
 }
 
-static void enqueue_correct(Ctx & c, int rk, int what) {
-  launch_correct(c.g, c.bc, c.cf, c.f(), c.dtp, rk, c.nu, what, c.st);
+static void enqueue_correct(Ctx & c, int rk, int what, bool cfl = false) {
+  launch_correct(c.g, c.bc, c.cf, c.f(), c.dtp, rk, c.nu, what, cfl ? c.dtmin : nullptr, c.status, c.st);
   mark(TCGPU_K_CORRECT);
 }
 
-static void enqueue_step(Ctx & c) {
+static void enqueue_dtmin(Ctx & c) {
   launch_dtmin(c.g, c.f(), c.dtmin, c.status, c.st);
   mark(TCGPU_K_DTMIN);
+}
+
+// One step (integrate.c:24-70) after the advective limit of the current
+// fields is in dtmin: dt, the factors, three substeps; the last correction
+// leaves the next step's advective limit in dtmin.
+static void enqueue_step(Ctx & c) {
   launch_dtfinal(c.coef_adv, c.dt_caps, c.dtmin, c.dtp, c.status, c.st);
   mark(TCGPU_K_DTFINAL);
   enqueue_factors(c);
   for (int rk = 0; rk < 3; rk++) {
     enqueue_predict(c, rk);
     enqueue_potential(c, rk);
-    enqueue_correct(c, rk, CORRECT_VELOCITY | CORRECT_PRESSURE);
+    enqueue_correct(c, rk, CORRECT_VELOCITY | CORRECT_PRESSURE, rk == 2);
   }
 }
 
 static int launch_step(Ctx & c) {
+  if (!c.dt_ready) enqueue_dtmin(c);
   const int p = c.cur;
   if (c.step_graph[p] == nullptr) {
     cudaGraph_t graph;
@@ -681,6 +693,7 @@ static int launch_step(Ctx & c) {
   }
   CK(cudaGraphLaunch(c.step_graph[p], c.st));
   c.cur = p ^ 1;   // three predicts per step: the state ends in the other buffer
+  c.dt_ready = true;
   return 0;
 }
 
@@ -689,6 +702,14 @@ static int set_dt(Ctx & c, double dt) {
   *c.h_scalar = dt;
   CK(cudaMemcpyAsync(c.dtp, c.h_scalar, sizeof(double), cudaMemcpyHostToDevice, c.st));
   return 0;
+}
+
+// the fields are about to change outside a full step: drop the advective limit
+// the last step left in dtmin
+static void invalidate_dt(Ctx & c) {
+  if (!c.dt_ready) return;
+  launch_dtreset(c.dtmin, c.st);
+  c.dt_ready = false;
 }
 
 static int finish(Ctx & c, const char * what) {
@@ -700,6 +721,7 @@ static int finish(Ctx & c, const char * what) {
   if (*c.h_status) {
     const unsigned s = *c.h_status;
     cudaMemsetAsync(c.status, 0, sizeof(unsigned), c.st);
+    invalidate_dt(c);
     cudaStreamSynchronize(c.st);
     if (s & ST_NONFINITE) return fail("%s: non-finite velocity in the field", what);
     if (s & ST_BADDT) return fail("%s: invalid time step size", what);
@@ -754,6 +776,7 @@ static const char * field_name(unsigned bit) {
 }
 
 static int push_fields(Ctx & c, const fluid_t * fl, unsigned mask) {
+  invalidate_dt(c);
   for (unsigned bit = 1; bit <= TCGPU_T; bit <<= 1) {
     if (!(mask & bit)) continue;
     const array_t * a = host_field(fl, bit);
@@ -931,12 +954,16 @@ int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int in
   CK(cudaStreamSynchronize(c->st));
   CK(cudaEventRecord(e0, c->st));
   if (instrument) rec.mark(TCGPU_K_DTMIN, 0);   // start marker, counts nothing
+  int direct_dtmin = 0;                          // dtmin launches outside the step graphs
   for (int s = 0; s < nsteps; s++) {
     if (instrument) {
       g_rec = &rec;
+      if (!c->dt_ready) enqueue_dtmin(*c);
       enqueue_step(*c);
+      c->dt_ready = true;
       g_rec = nullptr;
     } else {
+      if (!c->dt_ready) direct_dtmin++;
       if (launch_step(*c)) return 1;
     }
     if (dts) CK(cudaMemcpyAsync(c->h_scalar + s, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -959,6 +986,7 @@ int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int in
   }
   if (kernel_launches) {
     for (int k = 0; k < TCGPU_K_COUNT; k++) kernel_launches[k] = instrument ? rec.launches[k] : c->graph_launches[k] * nsteps;
+    if (!instrument) kernel_launches[TCGPU_K_DTMIN] += direct_dtmin;
   }
   return 0;
 }
@@ -993,6 +1021,7 @@ double fluid_compute_scalar_diffusivity(const fluid_t * fluid) { return 1. / flu
 int decide_dt(const domain_t * domain, const fluid_t * fluid, double * dt) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
+  invalidate_dt(*c);
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
   launch_decide_dt(c->g, c->f(), c->coef_adv, c->dt_caps, c->dtmin, c->dtp, c->status, c->st);
   CK(cudaMemcpyAsync(c->h_scalar, c->dtp, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -1005,6 +1034,7 @@ int fluid_predict_field(const domain_t * domain, const size_t rkstep, const doub
   if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
+  invalidate_dt(*c);
   const int rk = (int)rkstep;
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
   if (set_dt(*c, dt)) return 1;
@@ -1022,6 +1052,7 @@ int fluid_compute_potential(const domain_t * domain, const size_t rkstep, const 
   if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
+  invalidate_dt(*c);
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ)) return 1;
   if (set_dt(*c, dt)) return 1;
   enqueue_potential(*c, (int)rkstep);
@@ -1033,6 +1064,7 @@ int fluid_correct_velocity(const domain_t * domain, const size_t rkstep, const d
   if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
+  invalidate_dt(*c);
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_PSI)) return 1;
   if (set_dt(*c, dt)) return 1;
   enqueue_correct(*c, (int)rkstep, CORRECT_VELOCITY);
@@ -1044,6 +1076,7 @@ int fluid_update_pressure(const domain_t * domain, const size_t rkstep, const do
   if (rkstep > 2) return fail("rkstep %zu out of range", rkstep);
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
+  invalidate_dt(*c);
   // inside integrate() this update runs fused with the velocity correction
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_P | TCGPU_PSI)) return 1;
   if (set_dt(*c, dt)) return 1;

@@ -186,8 +186,15 @@ void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const F
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm = PoissonMarks());
 void poisson_smem_limits();
 enum { CORRECT_VELOCITY = 1, CORRECT_PRESSURE = 2 };
+// cfl_dtmin: when non-null (velocity and pressure together), the advective
+// time-step limit of the corrected velocities is folded into it
 void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
-                    int rkstep, double nu, int what, cudaStream_t st);
+                    int rkstep, double nu, int what, unsigned long long * cfl_dtmin, unsigned * status,
+                    cudaStream_t st);
+// the advective limit is gathered in DT_SLOTS accumulators (blocks spread
+// their atomicMin over them); dtfinal takes their minimum and resets them
+constexpr int DT_SLOTS = 256;
+void launch_dtreset(unsigned long long * dtmin, cudaStream_t st);
 
 // decide_dt: dt_caps[0..2] are the diffusive limits (0 when that direction is
 // implicit), written to *dtp together with status bits in *status

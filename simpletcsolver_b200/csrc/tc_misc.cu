@@ -21,145 +21,247 @@
 namespace tcgpu {
 
 // --------------------------------------------------------------- correction
-__global__ void __launch_bounds__(256)
-correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp, int rkstep, double nu, int what) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  const int k = blockIdx.z + 1;
-  if (i > g.nx || j > g.ny) return;
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
-  const double dt = *dtp;
-  const double pf = rk_gamma(rkstep) * dt;          // correct/main.c:21-22
-  const double pp = 0.5 * rk_gamma(rkstep) * dt * nu; // update_pressure.c:161-162
-  const double * psi = f.psi;
-  const double psi0 = __ldg(psi + cidx(g, i, j, k));
-  const double psi_im = __ldg(psi + cidx(g, i - 1, j, k));
-  const double psi_jm = __ldg(psi + cidx(g, i, j - 1, k));
-  const double psi_km = __ldg(psi + cidx(g, i, j, k - 1));
-  // ux, i = 2..nx (correct/ux.c:25-52); walls stay zero
-  if (what & CORRECT_VELOCITY) {
-    double val = 0.;
-    if (i >= 2) {
-      const size_t q = fidx(g, i, j, k);
-      val = f.ux[q] - pf * __ldg(cf.c_invhxxf + i) * (-psi_im + psi0);
-      f.ux[q] = val;
-      for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, i, jj, kk)] = val; });
-    } else {
-      f.ux[fidx(g, 1, j, k)] = 0.;
-      for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, 1, jj, kk)] = 0.; });
-    }
-    if (i == nx) {
-      f.ux[fidx(g, nx + 1, j, k)] = 0.;
-      for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, nx + 1, jj, kk)] = 0.; });
-    }
-  }
-  // uy (correct/uy.c:25-52) with its walls (boundary/uy.c)
-  if (what & CORRECT_VELOCITY) {
-    const size_t q = cidx(g, i, j, k);
-    const double val = f.uy[q] - pf * __ldg(cf.c_invhyxc + i) * (-psi_jm + psi0);
-    auto put = [&](int jj, int kk) {
-      f.uy[cidx(g, i, jj, kk)] = val;
-      if (i == 1) f.uy[cidx(g, 0, jj, kk)] = bc.uy_xm;
-      if (i == nx) f.uy[cidx(g, nx + 1, jj, kk)] = bc.uy_xp;
-    };
-    put(j, k);
-    for_images(j, k, ny, nz, put);
-  }
-  // uz (correct/uz.c:15-44)
-  if (what & CORRECT_VELOCITY) {
-    const size_t q = cidx(g, i, j, k);
-    const double val = f.uz[q] - pf * cf.inv_hz * (-psi_km + psi0);
-    auto put = [&](int jj, int kk) {
-      f.uz[cidx(g, i, jj, kk)] = val;
-      if (i == 1) f.uz[cidx(g, 0, jj, kk)] = 0.;
-      if (i == nx) f.uz[cidx(g, nx + 1, jj, kk)] = 0.;
-    };
-    put(j, k);
-    for_images(j, k, ny, nz, put);
-  }
-  // p += psi, then the implicit-direction corrections (update_pressure.c:23-136)
-  if (what & CORRECT_PRESSURE) {
-    const size_t q = cidx(g, i, j, k);
-    double val = f.p[q] + psi0;
-    const double ijd = __ldg(cf.c_invjdxc + i);
-    if (bc.implicit[0]) {
-      const double l = __ldg(cf.c_pxl + i), u = __ldg(cf.c_pxu + i), c = -l - u;
-      const double psi_ip = __ldg(psi + cidx(g, i + 1, j, k));
-      val -= 2. * pp * ijd * (l * psi_im + c * psi0 + u * psi_ip);
-    }
-    if (bc.implicit[1]) {
-      const double l = __ldg(cf.c_pyl + i), c = -l - l;
-      const double psi_jp = __ldg(psi + cidx(g, i, j + 1, k));
-      val -= 2. * pp * ijd * (l * psi_jm + c * psi0 + l * psi_jp);
-    }
-    if (bc.implicit[2]) {
-      const double l = __ldg(cf.c_pzl + i), c = -l - l;
-      const double psi_kp = __ldg(psi + cidx(g, i, j, k + 1));
-      val -= 2. * pp * ijd * (l * psi_km + c * psi0 + l * psi_kp);
-    }
-    auto put = [&](int jj, int kk) {
-      f.p[cidx(g, i, jj, kk)] = val;
-      if (i == 1) f.p[cidx(g, 0, jj, kk)] = val;
-      if (i == nx) f.p[cidx(g, nx + 1, jj, kk)] = val;
-    };
-    put(j, k);
-    for_images(j, k, ny, nz, put);
-  }
-}
-
-void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
-                    int rkstep, double nu, int what, cudaStream_t st) {
-  dim3 block(32, 8, 1);
-  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
-  correct_kernel<<<grid, block, 0, st>>>(g, bc, cf, f, dtp, rkstep, nu, what);
-}
-
-// --------------------------------------------------------------- decide_dt
 __device__ inline double warp_min(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
+// Advective limit of a (32, 8) block: the largest |v| + 1e-8 per direction
+// over the block's eight rows j of each radial index, one division per index
+// and direction (h depends on i only, and correctly rounded division is
+// monotonic, so h / max(|v| + 1e-8) is the minimum of the per-cell quotients),
+// the minimum over the 32 indices, then an order-independent atomicMin on the
+// bit pattern of the positive double into one of DT_SLOTS accumulators (blocks
+// spread over them). Non-finite velocities raise ST_NONFINITE. Threads without
+// a cell pass a = 0.
+__device__ inline void block_cfl(double ax, double ay, double az, double hx, double hy, double hz, bool bad,
+                                 unsigned long long * dtmin, unsigned * status) {
+  __shared__ double sa[3][8][32];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  sa[0][ty][tx] = ax;
+  sa[1][ty][tx] = ay;
+  sa[2][ty][tx] = az;
+  if (__syncthreads_or(bad) && tx == 0 && ty == 0) atomicOr(status, (unsigned)ST_NONFINITE);
+  if (ty == 0) {
+    double mx = 0., my = 0., mz = 0.;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      mx = fmax(mx, sa[0][r][tx]);
+      my = fmax(my, sa[1][r][tx]);
+      mz = fmax(mz, sa[2][r][tx]);
+    }
+    double m = 1.;
+    if (mx > 0.) m = fmin(m, hx / mx);
+    if (my > 0.) m = fmin(m, hy / my);
+    if (mz > 0.) m = fmin(m, hz / mz);
+    m = warp_min(m);
+    if (tx == 0) {
+      const unsigned b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+      atomicMin(dtmin + (b & (DT_SLOTS - 1)), (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// WHAT: CORRECT_VELOCITY and/or CORRECT_PRESSURE; IMPL: implicit directions
+// as a compile-time mask (bit 0 x, 1 y, 2 z) or -1 to read them from bc. One
+// thread per cell. With CFL the advective limit of decide_dt_adv
+// (src/decide_dt.c:32-80) is taken on the corrected velocities as they are
+// written, for the next step's dt (the reference computes it at the start of
+// that step from the same values).
+// Resident blocks requested from the register allocator; measured at
+// 256 x 1024 x 512 (ms per launch, averaged over a step's three): 6/5 (plain /
+// with CFL) 2.23, 5/4 2.15, 4/4 2.09. With all loads issued up front the
+// registers holding them buy more than the extra warps.
+#ifndef TC_CORRECT_MB
+#define TC_CORRECT_MB 4
+#endif
+#ifndef TC_CORRECT_MB_CFL
+#define TC_CORRECT_MB_CFL 4
+#endif
+template <int WHAT, int IMPL, bool CFL>
+__global__ void __launch_bounds__(256, CFL ? TC_CORRECT_MB_CFL : TC_CORRECT_MB)
+correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp, int rkstep, double nu,
+               unsigned long long * dtmin, unsigned * status) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const bool act = i <= nx && j <= ny;
+  const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
+  const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
+  const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
+  const double small = 1.e-8;
+  double ax = 0., ay = 0., az = 0.;   // |v| + 1e-8 of the corrected velocities (CFL)
+  bool bad = false;
+  if (act) {
+    // every input is loaded before the first store (the arrays are distinct,
+    // which the compiler cannot know), so a thread's loads are in flight together
+    const double * psi = f.psi;
+    const size_t qc = cidx(g, i, j, k), qf = fidx(g, i, j, k);
+    const size_t sj = (size_t)(nx + 2), sk = (size_t)(nx + 2) * (ny + 2);
+    const double psi0 = __ldg(psi + qc);
+    const double psi_im = __ldg(psi + qc - 1);
+    const double psi_jm = __ldg(psi + qc - sj);
+    const double psi_km = __ldg(psi + qc - sk);
+    double psi_ip = 0., psi_jp = 0., psi_kp = 0.;
+    double ux0 = 0., uy0 = 0., uz0 = 0., p0 = 0.;
+    if (WHAT & CORRECT_VELOCITY) {
+      if (i >= 2) ux0 = f.ux[qf];
+      uy0 = f.uy[qc];
+      uz0 = f.uz[qc];
+    }
+    if (WHAT & CORRECT_PRESSURE) {
+      p0 = f.p[qc];
+      if (ix) psi_ip = __ldg(psi + qc + 1);
+      if (iy) psi_jp = __ldg(psi + qc + sj);
+      if (iz) psi_kp = __ldg(psi + qc + sk);
+    }
+    const double dt = *dtp;
+    const double pf = rk_gamma(rkstep) * dt;            // correct/main.c:21-22
+    const double pp = 0.5 * rk_gamma(rkstep) * dt * nu;  // update_pressure.c:161-162
+    if (WHAT & CORRECT_VELOCITY) {
+      // ux, i = 2..nx (correct/ux.c:25-52); walls stay zero
+      const double vx = (i >= 2) ? ux0 - pf * __ldg(cf.c_invhxxf + i) * (-psi_im + psi0) : 0.;
+      f.ux[qf] = vx;
+      for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, i, jj, kk)] = vx; });
+      if (i == nx) {
+        f.ux[qf + 1] = 0.;
+        for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, nx + 1, jj, kk)] = 0.; });
+      }
+      // uy (correct/uy.c:25-52), uz (correct/uz.c:15-44) with their walls
+      const double vy = uy0 - pf * __ldg(cf.c_invhyxc + i) * (-psi_jm + psi0);
+      const double vz = uz0 - pf * cf.inv_hz * (-psi_km + psi0);
+      auto put = [&](int jj, int kk) {
+        const size_t q = cidx(g, i, jj, kk);
+        f.uy[q] = vy;
+        f.uz[q] = vz;
+        if (i == 1) { f.uy[q - 1] = bc.uy_xm; f.uz[q - 1] = 0.; }
+        if (i == nx) { f.uy[q + 1] = bc.uy_xp; f.uz[q + 1] = 0.; }
+      };
+      put(j, k);
+      for_images(j, k, ny, nz, put);
+      if (CFL) {
+        bad = !isfinite(vx) || !isfinite(vy) || !isfinite(vz);
+        if (i >= 2) ax = fabs(vx) + small;
+        ay = fabs(vy) + small;
+        az = fabs(vz) + small;
+      }
+    }
+    // p += psi, then the implicit-direction corrections (update_pressure.c:23-136)
+    if (WHAT & CORRECT_PRESSURE) {
+      double val = p0 + psi0;
+      const double ijd = __ldg(cf.c_invjdxc + i);
+      if (ix) {
+        const double l = __ldg(cf.c_pxl + i), u = __ldg(cf.c_pxu + i), c = -l - u;
+        val -= 2. * pp * ijd * (l * psi_im + c * psi0 + u * psi_ip);
+      }
+      if (iy) {
+        const double l = __ldg(cf.c_pyl + i), c = -l - l;
+        val -= 2. * pp * ijd * (l * psi_jm + c * psi0 + l * psi_jp);
+      }
+      if (iz) {
+        const double l = __ldg(cf.c_pzl + i), c = -l - l;
+        val -= 2. * pp * ijd * (l * psi_km + c * psi0 + l * psi_kp);
+      }
+      auto put = [&](int jj, int kk) {
+        const size_t q = cidx(g, i, jj, kk);
+        f.p[q] = val;
+        if (i == 1) f.p[q - 1] = val;
+        if (i == nx) f.p[q + 1] = val;
+      };
+      put(j, k);
+      for_images(j, k, ny, nz, put);
+    }
+  }
+  if (CFL) {
+    const bool in = i <= nx;
+    block_cfl(ax, ay, az, in ? __ldg(g.hxxf + i) : 1., in ? __ldg(g.hyxc + i) : 1., g.hz, bad, dtmin, status);
+  }
+}
+
+template <int WHAT, int IMPL, bool CFL>
+static void launch_correct_t(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+                             int rkstep, double nu, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
+  dim3 block(32, 8, 1);
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  correct_kernel<WHAT, IMPL, CFL><<<grid, block, 0, st>>>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status);
+}
+
+template <bool CFL>
+static void launch_correct_both(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f,
+                                const double * dtp, int rkstep, double nu, unsigned long long * dtmin,
+                                unsigned * status, cudaStream_t st) {
+  const int mask = (bc.implicit[0] ? 1 : 0) | (bc.implicit[1] ? 2 : 0) | (bc.implicit[2] ? 4 : 0);
+  constexpr int B = CORRECT_VELOCITY | CORRECT_PRESSURE;
+  switch (mask) {
+    case 1: launch_correct_t<B, 1, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    case 7: launch_correct_t<B, 7, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    case 0: launch_correct_t<B, 0, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    default: launch_correct_t<B, -1, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+  }
+}
+
+void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+                    int rkstep, double nu, int what, unsigned long long * cfl_dtmin, unsigned * status,
+                    cudaStream_t st) {
+  if (what == CORRECT_VELOCITY)
+    launch_correct_t<CORRECT_VELOCITY, -1, false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+  else if (what == CORRECT_PRESSURE)
+    launch_correct_t<CORRECT_PRESSURE, -1, false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+  else if (cfl_dtmin)
+    launch_correct_both<true>(g, bc, cf, f, dtp, rkstep, nu, cfl_dtmin, status, st);
+  else
+    launch_correct_both<false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+}
+
+// --------------------------------------------------------------- decide_dt
 __global__ void __launch_bounds__(256)
 dtmin_kernel(Geo g, const double * __restrict__ ux, const double * __restrict__ uy,
              const double * __restrict__ uz, unsigned long long * dtmin, unsigned * status) {
   const double small = 1.e-8;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-  double m = 1.;
   bool bad = false;
+  double ax = 0., ay = 0., az = 0., hx = 1., hy = 1., hz = 1.;
   if (i <= g.nx && j <= g.ny) {
-    const double hx = __ldg(g.hxxf + i), hy = __ldg(g.hyxc + i), hz = g.hz;
+    hx = __ldg(g.hxxf + i);
+    hy = __ldg(g.hyxc + i);
+    hz = g.hz;
     for (int k = blockIdx.z + 1; k <= g.nz; k += gridDim.z) {
       if (i >= 2) {
         const double v = __ldg(ux + fidx(g, i, j, k));
         bad |= !isfinite(v);
-        m = fmin(m, hx / (fabs(v) + small));
+        ax = fmax(ax, fabs(v) + small);
       }
       const double vy = __ldg(uy + cidx(g, i, j, k));
       const double vz = __ldg(uz + cidx(g, i, j, k));
       bad |= !isfinite(vy) || !isfinite(vz);
-      m = fmin(m, hy / (fabs(vy) + small));
-      m = fmin(m, hz / (fabs(vz) + small));
+      ay = fmax(ay, fabs(vy) + small);
+      az = fmax(az, fabs(vz) + small);
     }
   }
-  __shared__ double red[8];
-  m = warp_min(m);
-  const int t = threadIdx.y * blockDim.x + threadIdx.x;
-  const int lane = t & 31, wid = t >> 5;
-  if (lane == 0) red[wid] = m;
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, (unsigned)ST_NONFINITE);
-  __syncthreads();
-  if (wid == 0) {
-    double v = (lane < 8) ? red[lane] : 1.;
-    v = warp_min(v);
-    if (lane == 0) atomicMin(dtmin, (unsigned long long)__double_as_longlong(v));
-  }
+  block_cfl(ax, ay, az, hx, hy, hz, bad, dtmin, status);
 }
 
-__global__ void dtfinal_kernel(double coef_adv, const double * caps, unsigned long long * dtmin,
-                               double * dtp, unsigned * status) {
-  double dt = __longlong_as_double((long long)*dtmin);
+// sets the accumulators of the advective limit back to 1.0, the reference's
+// starting value (src/decide_dt.c:40)
+__global__ void dtreset_kernel(unsigned long long * dtmin) { dtmin[threadIdx.x] = 0x3ff0000000000000ull; }
+
+void launch_dtreset(unsigned long long * dtmin, cudaStream_t st) { dtreset_kernel<<<1, DT_SLOTS, 0, st>>>(dtmin); }
+
+// one thread per accumulator: their minimum, then dt, and each thread resets
+// its accumulator to 1.0
+__global__ void __launch_bounds__(DT_SLOTS)
+dtfinal_kernel(double coef_adv, const double * caps, unsigned long long * dtmin, double * dtp, unsigned * status) {
+  __shared__ double red[DT_SLOTS / 32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  double v = warp_min(__longlong_as_double((long long)dtmin[t]));
+  dtmin[t] = 0x3ff0000000000000ull;  // 1.0
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  if (t != 0) return;
+  double dt = red[0];
+  for (int w = 1; w < DT_SLOTS / 32; w++) dt = fmin(dt, red[w]);
   dt = fmin(1., dt);
   dt *= coef_adv;
   for (int d = 0; d < 3; d++) {
@@ -167,7 +269,6 @@ __global__ void dtfinal_kernel(double coef_adv, const double * caps, unsigned lo
   }
   if (!(dt > 0.) || !isfinite(dt)) atomicOr(status, (unsigned)ST_BADDT);
   *dtp = dt;
-  *dtmin = 0x3ff0000000000000ull;  // 1.0, the reference's starting value
 }
 
 void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
@@ -178,7 +279,7 @@ void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, u
 
 void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,
                     unsigned * status, cudaStream_t st) {
-  dtfinal_kernel<<<1, 1, 0, st>>>(coef_adv, dt_caps, dtmin, dtp, status);
+  dtfinal_kernel<<<1, DT_SLOTS, 0, st>>>(coef_adv, dt_caps, dtmin, dtp, status);
 }
 
 void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,

@@ -356,7 +356,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
     ps.spec[((size_t)(i - 1) * nz + (k - 1)) * nyh + m] = out;
   };
   for (int idx = threadIdx.x; idx < TI * half; idx += blockDim.x) put(idx >> (lg - 1), idx & (half - 1));
-  if ((int)threadIdx.x < TI) put(threadIdx.x, half);
+  for (int ii = threadIdx.x; ii < TI; ii += blockDim.x) put(ii, half);
 }
 
 // --------------------------------------------------------------- z transforms
