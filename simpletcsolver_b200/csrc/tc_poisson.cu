@@ -28,10 +28,20 @@
 #include "tc_kernels.h"
 
 // resident CTAs per SM requested from the register allocator (measured best
-// at 256 x 1024 x 512: 2 for the divergence + y transform and for the z
-// transforms, 3 for the inverse y transform)
+// at 256 x 1024 x 512: 2 for the divergence + y transform, 3 for the inverse y
+// transform)
+// z transforms: elements per thread (the largest radix), threads per CTA and
+// resident CTAs requested from the register allocator. Measured at
+// 256 x 1024 x 512 (ms per launch): 16 / 256 / 2 0.65; 8 / 512 / 2 0.66;
+// 8 / 256 / 3 0.58; 8 / 256 / 4 0.67; 8 / 128 / 6 0.72.
+#ifndef TC_FFTZ_EPT
+#define TC_FFTZ_EPT 8
+#endif
+#ifndef TC_FFTZ_THREADS
+#define TC_FFTZ_THREADS 256
+#endif
 #ifndef TC_FFTZ_MIN_BLOCKS
-#define TC_FFTZ_MIN_BLOCKS 2
+#define TC_FFTZ_MIN_BLOCKS 3
 #endif
 #ifndef TC_IFFTY_MIN_BLOCKS
 #define TC_IFFTY_MIN_BLOCKS 3
@@ -187,7 +197,9 @@ __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const do
   int Ns = 1;
   int left = lg;
   while (left > 0) {
-    const int rl = left >= 4 ? 4 : left;
+    // radix 2^rl, at most EPT (one butterfly's points per thread)
+    constexpr int LGE = EPT >= 16 ? 4 : EPT >= 8 ? 3 : EPT >= 4 ? 2 : 1;
+    const int rl = left >= LGE ? LGE : left;
     if (EPT == 16) {
       if (rl == 4) stockham_pass<16, 1, SIGN>(x, N, Ns, t, TPL, tw);
       else if (rl == 3) stockham_pass<8, 2, SIGN>(x, N, Ns, t, TPL, tw);
@@ -260,7 +272,9 @@ __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg,
   };
   using I = int;
   while (left > 0) {
-    const int rl = left >= 4 ? 4 : left;
+    // radix 2^rl, at most EPT (one butterfly's points per thread)
+    constexpr int LGE = EPT >= 16 ? 4 : EPT >= 8 ? 3 : EPT >= 4 ? 2 : 1;
+    const int rl = left >= LGE ? LGE : left;
     left -= rl;
     if (EPT == 16) {
       if (rl == 4) pass(std::integral_constant<I, 16>(), std::integral_constant<I, 1>());
@@ -386,7 +400,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
 // the first pass reads and the last pass writes rows of P values straight from
 // and to the spectral array.
 template <int EPT, int SIGN>
-__global__ void __launch_bounds__(256, TC_FFTZ_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTZ_THREADS, TC_FFTZ_MIN_BLOCKS)
 fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   extern __shared__ double2 smem[];
   const int nz = g.nz, nyh = ps.nyh;
@@ -571,10 +585,10 @@ static int ilog2(int n) {
 
 // lines per CTA: ceil-free power of two, TPL threads each, at most 256 threads,
 // at most `cap` lines
-static int lines_per_cta(int n, int cap) {
-  const int ept = n < 16 ? n : 16;
+static int lines_per_cta(int n, int cap, int ept_max = 16, int threads = 256) {
+  const int ept = n < ept_max ? n : ept_max;
   const int tpl = n / ept;
-  int p = 256 / tpl;
+  int p = threads / tpl;
   while (p > 1 && p > cap) p >>= 1;
   return p < 1 ? 1 : p;
 }
@@ -591,7 +605,7 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
   div_ffty_kernel<EPTY><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
   mark(pm.k_div);
-  const int Pz = lines_per_cta(g.nz, ps.nyh);
+  const int Pz = lines_per_cta(g.nz, ps.nyh, EPTZ, TC_FFTZ_THREADS);
   const int tplz = g.nz / EPTZ;
   const size_t smz = sizeof(double2) * (size_t)Pz * padded_len(g.nz);
   dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
@@ -610,8 +624,8 @@ template <int EPTY>
 static void launch_poisson_z(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
                              const double * tab_y, const double * tab_z, const double * base,
                              const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
-  if (g.nz >= 16) launch_poisson_t<EPTY, 16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else if (g.nz == 8) launch_poisson_t<EPTY, 8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  if (g.nz >= 16 && TC_FFTZ_EPT == 16) launch_poisson_t<EPTY, 16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.nz >= 8) launch_poisson_t<EPTY, 8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
   else launch_poisson_t<EPTY, 4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
 }
 
