@@ -30,6 +30,15 @@
 // resident CTAs per SM requested from the register allocator (measured best
 // at 256 x 1024 x 512: 2 for the divergence + y transform, 3 for the inverse y
 // transform)
+// y transforms (divergence + forward, inverse): elements per thread and
+// threads per CTA. Measured at 256 x 1024 x 512 (ms, divergence + forward /
+// inverse): 16 / 256 1.32 / 0.96; 8 / 512 1.59-1.68 / 1.02; 8 / 256 1.68 / 0.97.
+#ifndef TC_FFTY_EPT
+#define TC_FFTY_EPT 16
+#endif
+#ifndef TC_FFTY_THREADS
+#define TC_FFTY_THREADS 256
+#endif
 // z transforms: elements per thread (the largest radix), threads per CTA and
 // resident CTAs requested from the register allocator. Measured at
 // 256 x 1024 x 512 (ms per launch): 16 / 256 / 2 0.65; 8 / 512 / 2 0.66;
@@ -297,7 +306,7 @@ __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg,
 // CTA: P complex lines (radial indices i0 .. i0+2P-1) x all j at one k;
 // TPL = ny / EPT threads per line.
 template <int EPT>
-__global__ void __launch_bounds__(256, TC_DIVFFT_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTY_THREADS, TC_DIVFFT_MIN_BLOCKS)
 div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
                 const double * __restrict__ ux, const double * __restrict__ uy,
                 const double * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
@@ -521,7 +530,7 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
 
 // --------------------------------------------------------------- inverse y
 template <int EPT>
-__global__ void __launch_bounds__(256, TC_IFFTY_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTY_THREADS, TC_IFFTY_MIN_BLOCKS)
 iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh;
@@ -599,7 +608,7 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
                              const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
   auto mark = [&](int kk) { if (pm.mark) pm.mark(kk, 1); };
   const int lgy = ilog2(g.ny), lgz = ilog2(g.nz);
-  const int Py = lines_per_cta(g.ny, (g.nx + 1) / 2);
+  const int Py = lines_per_cta(g.ny, (g.nx + 1) / 2, EPTY, TC_FFTY_THREADS);
   const int tply = g.ny / EPTY;
   const size_t smy = sizeof(double2) * (size_t)Py * padded_len(g.ny);
   dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
@@ -632,8 +641,8 @@ static void launch_poisson_z(const Geo & g, const Coefs & cf, const Poisson & ps
 void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
                     const double * tab_y, const double * tab_z, const double * base,
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
-  if (g.ny >= 16) launch_poisson_z<16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else if (g.ny == 8) launch_poisson_z<8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  if (g.ny >= 16 && TC_FFTY_EPT == 16) launch_poisson_z<16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.ny >= 8) launch_poisson_z<8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
   else launch_poisson_z<4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
 }
 
