@@ -234,6 +234,18 @@ int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int in
 /* select the CUDA device used by contexts created afterwards in this thread */
 int tcgpu_set_device(int device);
 
+/* FP32-storage mode. No counterpart in the reference. bytes = 8 (default:
+ * everything in FP64) or 4: contexts created afterwards store ux, uy, uz, t,
+ * the RK source terms and the Poisson spectra in 4-byte floats (in a padded
+ * device layout; host arrays stay the reference's doubles and are converted on
+ * every copy), while p, psi, every coefficient and all arithmetic stay FP64.
+ * An existing context keeps its storage until tcgpu_release(). Returns 0, or
+ * non-zero for other byte counts. */
+int tcgpu_set_storage(int bytes);
+/* bytes per stored value of this fluid's context (the default for new ones
+ * when it has none) */
+int tcgpu_get_storage(const fluid_t * fluid);
+
 /* logging quantities of src/logging/*.c from the device state:
  * out[0] max |div u|, out[1..2] energy injection (momentum, scalar),
  * out[3..4] dissipation (momentum, scalar), out[5..8] total energy

@@ -92,6 +92,8 @@ _EXT_SIGS = {
     "tcgpu_run": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_int, c_double_p]),
     "tcgpu_diagnostics": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 9]),
     "tcgpu_release": (C.c_int, [C.POINTER(FluidT)]),
+    "tcgpu_set_storage": (C.c_int, [C.c_int]),
+    "tcgpu_get_storage": (C.c_int, [C.POINTER(FluidT)]),
     "tcgpu_last_error": (C.c_char_p, []),
 }
 

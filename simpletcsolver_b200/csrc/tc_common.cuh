@@ -57,6 +57,44 @@ __host__ __device__ inline size_t pidx(int n_i, int ny, int ii, int j, int k) {
   return (size_t)ii + (size_t)n_i * ((size_t)(j - 1) + (size_t)ny * (size_t)(k - 1));
 }
 
+// Layout of the state arrays (ux, uy, uz, t) and RK source terms by storage
+// type. double: the reference's layout above (host copies are single
+// memcpys). float (FP32-storage mode, device only, converted on every host
+// copy): rows of P = nx + 2 rounded up to a multiple of 4 values so that every
+// row starts on a 16-byte boundary; ux keeps face i at element i (element 0
+// unused), so all four fields share one index; source-term lines are padded
+// to PS = nx rounded up to a multiple of 4.
+__host__ __device__ constexpr int pitch32(int nx) { return (nx + 2 + 3) & ~3; }
+__host__ __device__ constexpr int spitch32(int nx) { return (nx + 3) & ~3; }
+template <class T>
+__host__ __device__ inline size_t sidx_c(const Geo & g, int i, int j, int k) {
+  if (sizeof(T) == 8) return cidx(g, i, j, k);
+  return (size_t)i + (size_t)pitch32(g.nx) * ((size_t)j + (size_t)(g.ny + 2) * (size_t)k);
+}
+template <class T>
+__host__ __device__ inline size_t sidx_f(const Geo & g, int i, int j, int k) {
+  if (sizeof(T) == 8) return fidx(g, i, j, k);
+  return (size_t)i + (size_t)pitch32(g.nx) * ((size_t)j + (size_t)(g.ny + 2) * (size_t)k);
+}
+// row strides (elements) of the state arrays
+template <class T> __host__ __device__ inline int srow_c(const Geo & g) { return sizeof(T) == 8 ? g.nx + 2 : pitch32(g.nx); }
+template <class T> __host__ __device__ inline int srow_f(const Geo & g) { return sizeof(T) == 8 ? g.nx + 1 : pitch32(g.nx); }
+// element count of a state array
+template <class T> __host__ __device__ inline size_t scount_c(const Geo & g) {
+  return (size_t)srow_c<T>(g) * (g.ny + 2) * (g.nz + 2);
+}
+template <class T> __host__ __device__ inline size_t scount_f(const Geo & g) {
+  return (size_t)srow_f<T>(g) * (g.ny + 2) * (g.nz + 2);
+}
+// packed source-term index (ii from 0; n_i = nx - 1 for ux, nx otherwise)
+template <class T>
+__host__ __device__ inline size_t sidx_s(const Geo & g, int n_i, int ii, int j, int k) {
+  return pidx(sizeof(T) == 8 ? n_i : spitch32(g.nx), g.ny, ii, j, k);
+}
+template <class T> __host__ __device__ inline int sline(const Geo & g, int n_i) {
+  return sizeof(T) == 8 ? n_i : spitch32(g.nx);
+}
+
 // periodic images of interior (j, k) in the one-layer halo, including the
 // corner written by the z exchange after the y exchange (src/halo.c:18-142);
 // ny, nz >= 2 (the FFTs require powers of two >= 4)

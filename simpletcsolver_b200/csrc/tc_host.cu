@@ -65,9 +65,11 @@ struct Ctx {
   XFactors xf{};
   YZFactors yf{};
   Poisson ps{};
-  Fields fb[2]{};       // ux, uy, uz, t double-buffered; p and psi shared
+  int sb = 8;           // bytes per stored value of ux, uy, uz, t, sources, spectra: 8, or 4 (FP32 storage)
+  FieldBufs fb[2]{};    // ux, uy, uz, t double-buffered; p and psi shared
   int cur = 0;          // buffer holding the current state
-  double * src[4][2]{};
+  void * src[4][2]{};
+  double * stage = nullptr;   // FP32 storage: reference-layout doubles between host and device
   DeltaSet ds{};
   double * tab_y = nullptr;
   double * tab_z = nullptr;
@@ -91,7 +93,7 @@ struct Ctx {
   cudaStream_t st = nullptr;
   cudaGraphExec_t step_graph[2] = {nullptr, nullptr};   // one per starting buffer
   int graph_launches[TCGPU_K_COUNT] = {0};
-  Fields & f() { return fb[cur]; }
+  FieldBufs & f() { return fb[cur]; }
   std::vector<void *> pinned;     // caller arrays registered with cudaHostRegister
   double * h_scalar = nullptr;    // pinned: dt in / out
   unsigned * h_status = nullptr;  // pinned
@@ -99,6 +101,15 @@ struct Ctx {
 };
 
 static std::map<const fluid_t *, Ctx *> g_ctx;
+static int g_storage_bytes = 8;   // storage of contexts created from now on
+
+static void * valloc(Ctx & c, size_t bytes) {
+  void * p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, bytes);
+  c.allocs.push_back(p);
+  return p;
+}
 
 static double * dalloc(Ctx & c, size_t n) {
   void * p = nullptr;
@@ -471,7 +482,8 @@ static int build_tables(Ctx & c, const domain_t * d) {
   c.ps.tw_y = twiddles(ny);
   c.ps.tw_z = twiddles(nz);
   const size_t nspec = (size_t)nx * nz * nyh;
-  c.ps.spec = reinterpret_cast<double2 *>(dalloc(c, 2 * nspec));
+  c.ps.spec_bytes = 2 * c.sb;
+  c.ps.spec = valloc(c, nspec * c.ps.spec_bytes);
   c.ps.vscr = dalloc(c, nspec);
   if (!c.ps.tw_y || !c.ps.tw_z || !c.ps.spec || !c.ps.vscr) return fail("cudaMalloc of Poisson buffers failed");
   return 0;
@@ -502,6 +514,10 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   c->nz = (int)d->glsizes[2];
   c->nc = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
   c->nf = (size_t)(c->nx + 1) * (c->ny + 2) * (c->nz + 2);
+  c->g.nx = c->nx;
+  c->g.ny = c->ny;
+  c->g.nz = c->nz;
+  c->sb = g_storage_bytes;
   c->bc.uy_xm = g_params.uy_xm;
   c->bc.uy_xp = g_params.uy_xp;
   c->bc.t_xm = g_params.t_xm;
@@ -515,22 +531,30 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   double * p = dalloc(*c, c->nc);
   double * psi = dalloc(*c, c->nc);
   if (!p || !psi) return bad("cudaMalloc of fields failed");
+  const bool f32 = c->sb == 4;
+  const size_t nsf = f32 ? scount_f<float>(c->g) : c->nf, nsc = f32 ? scount_c<float>(c->g) : c->nc;
   for (int b = 0; b < 2; b++) {
-    Fields & F = c->fb[b];
-    F.ux = dalloc(*c, c->nf);
-    F.uy = dalloc(*c, c->nc);
-    F.uz = dalloc(*c, c->nc);
-    F.t = dalloc(*c, c->nc);
+    FieldBufs & F = c->fb[b];
+    F.ux = valloc(*c, nsf * c->sb);
+    F.uy = valloc(*c, nsc * c->sb);
+    F.uz = valloc(*c, nsc * c->sb);
+    F.t = valloc(*c, nsc * c->sb);
     F.p = p;
     F.psi = psi;
+    F.bytes = c->sb;
     if (!F.ux || !F.uy || !F.uz || !F.t) return bad("cudaMalloc of fields failed");
+  }
+  if (f32) {
+    c->stage = dalloc(*c, c->nc);
+    if (!c->stage) return bad("cudaMalloc of the staging buffer failed");
   }
   const size_t nin = (size_t)c->nx * c->ny * c->nz;
   const bool need_delta = c->bc.implicit[1] || c->bc.implicit[2];
   for (int v = 0; v < 4; v++) {
     const size_t n = (v == VUX) ? (size_t)(c->nx - 1) * c->ny * c->nz : nin;
-    c->src[v][0] = dalloc(*c, n);
-    c->src[v][1] = dalloc(*c, n);
+    const size_t ns = f32 ? (size_t)spitch32(c->nx) * c->ny * c->nz : n;
+    c->src[v][0] = valloc(*c, ns * c->sb);
+    c->src[v][1] = valloc(*c, ns * c->sb);
     if (!c->src[v][0] || !c->src[v][1]) return bad("cudaMalloc of source terms failed");
     if (need_delta) {
       c->ds.d[v] = dalloc(*c, n);
@@ -604,8 +628,8 @@ struct Recorder {
 static thread_local Recorder * g_rec = nullptr;
 static void mark(int k, int n = 1) { if (g_rec) g_rec->mark(k, n); }
 
-static double * s_new(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 1 : 0]; }
-static double * s_old(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 0 : 1]; }
+static void * s_new(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 1 : 0]; }
+static void * s_old(Ctx & c, int v, int rk) { return c.src[v][rk == 1 ? 0 : 1]; }
 
 static void enqueue_factors(Ctx & c) {
   if (c.bc.implicit[0]) { launch_xfactors(c.xf, c.dtp, c.nu, c.kappa, c.st); mark(TCGPU_K_FACTORS); }
@@ -613,13 +637,14 @@ static void enqueue_factors(Ctx & c) {
 }
 
 static void enqueue_predict(Ctx & c, int rk) {
-  SrcSet ss;
+  SrcBufs ss;
+  ss.bytes = c.sb;
   for (int v = 0; v < 4; v++) {
     ss.new_[v] = s_new(c, v, rk);
     ss.old_[v] = s_old(c, v, rk);
   }
-  const Fields in = c.fb[c.cur];
-  const Fields out = c.fb[c.cur ^ 1];
+  const FieldBufs in = c.fb[c.cur];
+  const FieldBufs out = c.fb[c.cur ^ 1];
   const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
   auto predict = [&](int mode) {
     launch_predict_march(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, mode, c.status, c.st);
@@ -733,8 +758,8 @@ static int finish(Ctx & c, const char * what) {
 // ------------------------------------------------------------------ coherence
 static size_t field_count(const Ctx & c, unsigned bit) { return bit == TCGPU_UX ? c.nf : c.nc; }
 
-static double * dev_field(Ctx & c, unsigned bit) {
-  const Fields & f = c.f();
+static void * dev_field(Ctx & c, unsigned bit) {
+  const FieldBufs & f = c.f();
   switch (bit) {
     case TCGPU_UX: return f.ux;
     case TCGPU_UY: return f.uy;
@@ -775,6 +800,18 @@ static const char * field_name(unsigned bit) {
   }
 }
 
+// bytes per stored value of a field: p and psi are always double
+static int field_bytes(const Ctx & c, unsigned bit) { return (bit == TCGPU_P || bit == TCGPU_PSI) ? 8 : c.sb; }
+
+// FP32 storage: reference-layout rows of a field (nref doubles) and their
+// FP32 pitch and shift
+static void rows_of(const Ctx & c, unsigned bit, size_t & rows, int & nref, int & pitch, int & shift) {
+  rows = (size_t)(c.ny + 2) * (c.nz + 2);
+  nref = bit == TCGPU_UX ? c.nx + 1 : c.nx + 2;
+  pitch = pitch32(c.nx);
+  shift = bit == TCGPU_UX ? 1 : 0;
+}
+
 static int push_fields(Ctx & c, const fluid_t * fl, unsigned mask) {
   invalidate_dt(c);
   for (unsigned bit = 1; bit <= TCGPU_T; bit <<= 1) {
@@ -782,7 +819,15 @@ static int push_fields(Ctx & c, const fluid_t * fl, unsigned mask) {
     const array_t * a = host_field(fl, bit);
     const size_t n = field_count(c, bit);
     if (check_host_array(c, a, n, field_name(bit))) return 1;
-    CK(cudaMemcpyAsync(dev_field(c, bit), a->data, n * sizeof(double), cudaMemcpyHostToDevice, c.st));
+    if (field_bytes(c, bit) == 8) {
+      CK(cudaMemcpyAsync(dev_field(c, bit), a->data, n * sizeof(double), cudaMemcpyHostToDevice, c.st));
+    } else {
+      size_t rows;
+      int nref, pitch, shift;
+      rows_of(c, bit, rows, nref, pitch, shift);
+      CK(cudaMemcpyAsync(c.stage, a->data, n * sizeof(double), cudaMemcpyHostToDevice, c.st));
+      launch_pack32(c.stage, static_cast<float *>(dev_field(c, bit)), rows, nref, pitch, shift, c.st);
+    }
   }
   return 0;
 }
@@ -793,7 +838,15 @@ static int pull_fields(Ctx & c, fluid_t * fl, unsigned mask) {
     const array_t * a = host_field(fl, bit);
     const size_t n = field_count(c, bit);
     if (check_host_array(c, a, n, field_name(bit))) return 1;
-    CK(cudaMemcpyAsync(a->data, dev_field(c, bit), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    if (field_bytes(c, bit) == 8) {
+      CK(cudaMemcpyAsync(a->data, dev_field(c, bit), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    } else {
+      size_t rows;
+      int nref, pitch, shift;
+      rows_of(c, bit, rows, nref, pitch, shift);
+      launch_unpack32(static_cast<const float *>(dev_field(c, bit)), c.stage, rows, nref, pitch, shift, c.st);
+      CK(cudaMemcpyAsync(a->data, c.stage, n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    }
   }
   return 0;
 }
@@ -839,10 +892,19 @@ static int mirror_srcs(Ctx & c, fluid_t * fl, int rk) {
   }
   if (!(c.coherence & TCGPU_SYNC_SRCS)) return 0;
   for (int v = 0; v < 4; v++) {
-    const size_t n = (v == VUX) ? (size_t)(c.nx - 1) * c.ny * c.nz : (size_t)c.nx * c.ny * c.nz;
-    if (arrs[v][0].data) CK(cudaMemcpyAsync(arrs[v][0].data, s_new(c, v, rk), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
-    if (arrs[v][1].data && rk != 0)
-      CK(cudaMemcpyAsync(arrs[v][1].data, s_old(c, v, rk), n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    const int ni = (v == VUX) ? c.nx - 1 : c.nx;
+    const size_t n = (size_t)ni * c.ny * c.nz;
+    auto copy = [&](void * host, const void * dev) -> int {
+      if (c.sb == 8) {
+        CK(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+      } else {
+        launch_unpack32(static_cast<const float *>(dev), c.stage, (size_t)c.ny * c.nz, ni, spitch32(c.nx), 0, c.st);
+        CK(cudaMemcpyAsync(host, c.stage, n * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+      }
+      return 0;
+    };
+    if (arrs[v][0].data && copy(arrs[v][0].data, s_new(c, v, rk))) return 1;
+    if (arrs[v][1].data && rk != 0 && copy(arrs[v][1].data, s_old(c, v, rk))) return 1;
   }
   return 0;
 }
@@ -853,7 +915,7 @@ static int apply_bcs(Ctx & c, unsigned mask) {
   const BcKind kinds[6] = {BC_UX, BC_UY, BC_UZ, BC_P, BC_PSI, BC_T};
   for (int s = 0; s < 6; s++) {
     const unsigned bit = 1u << s;
-    if (mask & bit) launch_bc(c.g, c.bc, kinds[s], dev_field(c, bit), c.st);
+    if (mask & bit) launch_bc(c.g, c.bc, kinds[s], dev_field(c, bit), field_bytes(c, bit), c.st);
   }
   return 0;
 }
@@ -989,6 +1051,18 @@ int tcgpu_run_timed(const domain_t * domain, fluid_t * fluid, int nsteps, int in
     if (!instrument) kernel_launches[TCGPU_K_DTMIN] += direct_dtmin;
   }
   return 0;
+}
+
+int tcgpu_set_storage(int bytes) {
+  if (bytes != 8 && bytes != 4) return fail("tcgpu_set_storage: %d bytes per value; 8 or 4 expected", bytes);
+  g_storage_bytes = bytes;
+  return 0;
+}
+
+int tcgpu_get_storage(const fluid_t * fluid) {
+  std::lock_guard<std::mutex> lk(g_mutex);
+  auto it = g_ctx.find(fluid);
+  return it == g_ctx.end() ? g_storage_bytes : it->second->sb;
 }
 
 int tcgpu_set_device(int device) {
@@ -1129,7 +1203,7 @@ static int bc_entry(const domain_t * domain, array_t * array, BcKind kind, const
   CK(cudaMalloc(&dbuf, n * sizeof(double)));
   cudaError_t e = cudaMemcpy(dbuf, array->data, n * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    launch_bc(g, bc, kind, dbuf, 0);
+    launch_bc(g, bc, kind, dbuf, 8, 0);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpy(array->data, dbuf, n * sizeof(double), cudaMemcpyDeviceToHost);

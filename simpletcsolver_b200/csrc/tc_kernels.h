@@ -5,14 +5,33 @@
 
 namespace tcgpu {
 
-// Device pointers of the state fields (reference layout with halos).
-struct Fields {
-  double * ux;
-  double * uy;
-  double * uz;
+// Device pointers of the state fields (reference layout with halos). ux, uy,
+// uz and t are stored in T: double, or float in the FP32-storage mode (all
+// arithmetic stays FP64); p and psi are always double.
+template <class T>
+struct FieldsT {
+  T * ux;
+  T * uy;
+  T * uz;
   double * p;
   double * psi;
-  double * t;
+  T * t;
+};
+using Fields = FieldsT<double>;
+// the host's type-erased form: bytes = 8 or 4 per stored value
+struct FieldBufs {
+  void * ux;
+  void * uy;
+  void * uz;
+  double * p;
+  double * psi;
+  void * t;
+  int bytes;
+  template <class T>
+  FieldsT<T> as() const {
+    return FieldsT<T>{static_cast<T *>(ux), static_cast<T *>(uy), static_cast<T *>(uz), p, psi,
+                      static_cast<T *>(t)};
+  }
 };
 
 // Per-radial-index coefficient tables (length nx+2, indexed by the reference
@@ -138,7 +157,8 @@ struct YZFactors {
 // Poisson solver state.
 struct Poisson {
   int nyh;                  // ny/2 + 1
-  double2 * spec;           // [nx][nz][nyh] complex spectra
+  void * spec;              // [nx][nz][nyh] complex spectra: double2, or float2 (spec_bytes 8)
+  int spec_bytes;           // 16 or 8 per complex value
   double * vscr;            // [nx][nz][nyh] elimination factors
   const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny
   const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz
@@ -150,10 +170,27 @@ struct Poisson {
   const double * eval_z;    // -4 sin^2(pi m / nz), m < nz
 };
 
-// RK source terms of one substep: old_ (srcA of the previous substep) and new_
-struct SrcSet {
-  const double * old_[4];
-  double * new_[4];
+// RK source terms of one substep: old_ (srcA of the previous substep) and new_,
+// stored like the state fields
+template <class T>
+struct SrcSetT {
+  const T * old_[4];
+  T * new_[4];
+};
+using SrcSet = SrcSetT<double>;
+struct SrcBufs {
+  const void * old_[4];
+  void * new_[4];
+  int bytes;
+  template <class T>
+  SrcSetT<T> as() const {
+    SrcSetT<T> s;
+    for (int v = 0; v < 4; v++) {
+      s.old_[v] = static_cast<const T *>(old_[v]);
+      s.new_[v] = static_cast<T *>(new_[v]);
+    }
+    return s;
+  }
 };
 // increments (packed interior layout), used by the planar y / z solves
 struct DeltaSet {
@@ -164,12 +201,12 @@ int predict_warps(int nx);
 // marching form of the predict stage (tc_march.cu); sets ST_TIMEOUT in
 // *status if a plane's copy does not arrive within its wait limit
 void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
-                          double kappa, const Fields & in, const Fields & out, const SrcSet & ss,
+                          double kappa, const FieldBufs & in, const FieldBufs & out, const SrcBufs & ss,
                           const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
                           cudaStream_t st);
 void march_smem_limits();
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);
-void launch_apply(const Geo & g, const Bc & bc, const Fields & in, const Fields & out, const DeltaSet & ds,
+void launch_apply(const Geo & g, const Bc & bc, const FieldBufs & in, const FieldBufs & out, const DeltaSet & ds,
                   cudaStream_t st);
 void launch_yzfactors(const Geo & g, const YZFactors & yf, const double * dtp, double nu, double kappa, cudaStream_t st);
 void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st);
@@ -181,14 +218,14 @@ struct PoissonMarks {
   int k_div = 0, k_fwd = 0, k_tdm = 0, k_inv = 0, k_ify = 0;
 };
 // tab_y[i][ky] = ey/hyxc/hyxc, tab_z[kz] = ez/hz/hz, base[i] = -l_i - u_i
-void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const FieldBufs & f,
                     const double * tab_y, const double * tab_z, const double * base,
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm = PoissonMarks());
 void poisson_smem_limits();
 enum { CORRECT_VELOCITY = 1, CORRECT_PRESSURE = 2 };
 // cfl_dtmin: when non-null (velocity and pressure together), the advective
 // time-step limit of the corrected velocities is folded into it
-void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const FieldBufs & f, const double * dtp,
                     int rkstep, double nu, int what, unsigned long long * cfl_dtmin, unsigned * status,
                     cudaStream_t st);
 // the advective limit is gathered in DT_SLOTS accumulators (blocks spread
@@ -198,24 +235,30 @@ void launch_dtreset(unsigned long long * dtmin, cudaStream_t st);
 
 // decide_dt: dt_caps[0..2] are the diffusive limits (0 when that direction is
 // implicit), written to *dtp together with status bits in *status
-void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,
+void launch_decide_dt(const Geo & g, const FieldBufs & f, double coef_adv, const double * dt_caps,
                       unsigned long long * dtmin, double * dtp, unsigned * status, cudaStream_t st);
-void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st);
+void launch_dtmin(const Geo & g, const FieldBufs & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st);
 void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,
                     unsigned * status, cudaStream_t st);
 
 // boundary conditions + periodic images of a single field (boundary/*.c)
 enum BcKind { BC_UX = 0, BC_UY, BC_UZ, BC_P, BC_PSI, BC_T };
-void launch_bc(const Geo & g, const Bc & bc, BcKind kind, double * a, cudaStream_t st);
+// a: the field, bytes per value 8 or 4 (p and psi are always double)
+void launch_bc(const Geo & g, const Bc & bc, BcKind kind, void * a, int bytes, cudaStream_t st);
 
 // velocity-gradient tensors with halos (predict/l*.c), for logging/statistics
 struct Tensors { double * a[11]; };  // lxx lxy lxz lyx0 lyx1 lyy0 lyy1 lyz lzx lzy lzz
-void launch_tensors(const Geo & g, const Coefs & cf, const Fields & f, const Tensors & tn, cudaStream_t st);
+void launch_tensors(const Geo & g, const Coefs & cf, const FieldBufs & f, const Tensors & tn, cudaStream_t st);
 
 // logging reductions (src/logging/*.c); out: 9 doubles on the device,
 // partial: DIAG_BLOCKS x 9 doubles of scratch
 constexpr int DIAG_BLOCKS_MAX = 296;
-void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const Fields & f, double nu, double kappa,
+void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, double nu, double kappa,
                         double * out, double * partial, cudaStream_t st);
+
+// FP32-storage mode: rows of nref doubles in the reference's layout to and from
+// rows of pitch floats (element e at e + shift)
+void launch_pack32(const double * src, float * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st);
+void launch_unpack32(const float * src, double * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st);
 
 }  // namespace tcgpu

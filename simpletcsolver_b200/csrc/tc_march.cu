@@ -135,30 +135,34 @@ struct PrevA { double ux0, t0; };
 struct PrevB { double ux0, ux1, uy0, uyjp, uz0, p0; };
 
 // A cell's view of two plane slots (k and k+1): base pointers already moved to
-// the cell's radial index (centre arrays at element i, ux at element i - 1,
-// face i sitting at element i - 1 of its row) and, for rows of odd parity, to
-// the widened copy's offset.
+// the cell's radial index and, for rows of odd parity, to the widened copy's
+// offset. Field rows hold the storage type T (ux at element i - 1 in the
+// reference layout, at element i in the FP32 layout); p rows are double.
+template <class T>
 struct SlotView {
-  const double * cb;   // plane k, centre arrays
-  const double * cbo;  // plane k, centre arrays, odd rows
-  const double * fb;   // plane k, ux
-  const double * fbo;  // plane k, ux, odd rows
-  const double * nb;   // plane k+1, centre arrays
-  const double * nbo;
-  const double * nf;   // plane k+1, ux
-  const double * nfo;
+  const T * cb;        // plane k, centre fields
+  const T * cbo;       // plane k, centre fields, odd rows
+  const T * fb;        // plane k, ux
+  const T * fbo;       // plane k, ux, odd rows
+  const T * nb;        // plane k+1, centre fields
+  const T * nbo;
+  const T * nf;        // plane k+1, ux
+  const T * nfo;
+  const double * pb;   // plane k, p
+  const double * pbo;  // plane k, p, odd rows
 };
 
 // Slot rows: field f, row r (j - 1 + r for the CTA's first line j) starts at
-// (f (JT + 2) + r) RL; odd rows read at the widened copy's offset. JL is the
-// cell's line within the CTA.
+// (f (JT + 2) + r) RL values of the field block, p row r at r RL of the p
+// block; odd rows read at the widened copy's offset. JL is the cell's line
+// within the CTA.
 #define ROW_(F, DJ) (((F) * (JT + 2) + JL + 1 + (DJ)) * RL)
 #define ODD_(DJ) (((JL + 1 + (DJ)) & 1) != 0)
 #define UX(DI, DJ) (ODD_(DJ) ? V.fbo : V.fb)[ROW_(SF_UX, DJ) + (DI)]
 #define UY(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_UY, DJ) + (DI)]
 #define UZ(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_UZ, DJ) + (DI)]
 #define TT(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_T, DJ) + (DI)]
-#define PP(DI, DJ) (ODD_(DJ) ? V.cbo : V.cb)[ROW_(SF_P, DJ) + (DI)]
+#define PP(DI, DJ) (ODD_(DJ) ? V.pbo : V.pb)[(JL + 1 + (DJ)) * RL + (DI)]
 #define NUX(DI) (ODD_(0) ? V.nfo : V.nf)[ROW_(SF_UX, 0) + (DI)]
 #define NUY(DI) (ODD_(0) ? V.nbo : V.nb)[ROW_(SF_UY, 0) + (DI)]
 #define NUZ(DI, DJ) (ODD_(DJ) ? V.nbo : V.nb)[ROW_(SF_UZ, DJ) + (DI)]
@@ -170,10 +174,10 @@ struct SlotView {
 // centre i (t.c) of cell (i, j, k); new source terms to ss.new_, increments
 // dl[0] (ux, 0 at i = 1 where ux has no unknown) and dl[1] (t), current
 // values u0[0] (ux) and u0[1] (t).
-template <int JT, int RL, int JL, int IMPL>
-__device__ __forceinline__ void cell_a(const CoefA & q, const SlotView & V, PrevA & pv, const Bc & bc,
+template <int JT, int RL, int JL, int IMPL, class T>
+__device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, PrevA & pv, const Bc & bc,
                                        const Coefs & cf, double nu, double kappa, int i, size_t qf, size_t qc,
-                                       const SrcSet & ss, double ca, double cb, double cg, double old_x,
+                                       const SrcSetT<T> & ss, double ca, double cb, double cg, double old_x,
                                        double old_t, double dl[2], double u0[2]) {
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
   const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
@@ -206,7 +210,7 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView & V, Prev
     ROUTE(ix, 2. * nu * (q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p));
     ROUTE(iy, nu * (q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp));
     ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
-    ss.new_[VUX][qf] = e;
+    ss.new_[VUX][qf] = (T)e;
     dl[0] = ca * e + cb * old_x + cg * gi;
   }
   {
@@ -221,7 +225,7 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView & V, Prev
     ROUTE(ix, kappa * (q.clxl * tim + q.clxc * t_0 + q.clxu * tip));
     ROUTE(iy, kappa * (q.clyl * tjm + q.clyc * t_0 + q.clyu * tjp));
     ROUTE(iz, kappa * (cf.lz_l * tkm + cf.lz_c * t_0 + cf.lz_u * tkp));
-    ss.new_[VT][qc] = e;
+    ss.new_[VT][qc] = (T)e;
     dl[1] = ca * e + cb * old_t + cg * gi;
     u0[1] = t_0;
     pv.t0 = t_0;
@@ -233,9 +237,9 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView & V, Prev
 // Group B: right-hand sides of uy (src/fluid/predict/uy.c) and uz (uz.c) at
 // centre i of cell (i, j, k); increments dl[0] (uy), dl[1] (uz), current
 // values u0[0], u0[1].
-template <int JT, int RL, int JL, int IMPL>
-__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView & V, PrevB & pv, const Bc & bc,
-                                       const Coefs & cf, double nu, int i, size_t qc, const SrcSet & ss,
+template <int JT, int RL, int JL, int IMPL, class T>
+__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, PrevB & pv, const Bc & bc,
+                                       const Coefs & cf, double nu, int i, size_t qc, const SrcSetT<T> & ss,
                                        double ca, double cb, double cg, double old_y, double old_z, double dl[2],
                                        double u0[2]) {
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
@@ -265,7 +269,7 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView & V, Prev
     ROUTE(ix, nu * (q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip));
     ROUTE(iy, 2. * nu * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
     ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
-    ss.new_[VUY][qc] = e;
+    ss.new_[VUY][qc] = (T)e;
     dl[0] = ca * e + cb * old_y + cg * gi;
   }
   {  // uz
@@ -284,7 +288,7 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView & V, Prev
     ROUTE(ix, nu * (q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip));
     ROUTE(iy, nu * (q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp));
     ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
-    ss.new_[VUZ][qc] = e;
+    ss.new_[VUZ][qc] = (T)e;
     dl[1] = ca * e + cb * old_z + cg * gi;
   }
   u0[0] = uy_0;
@@ -390,32 +394,36 @@ __device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int
   }
 }
 
-// Shared-memory layout in doubles, shared by the kernel and its launcher. Row
+// Shared-memory layout in bytes, shared by the kernel and its launcher. Row
 // buffers are sized for the widest radial line of the warp count (nx <= 32 NW),
-// so every stencil offset is a compile-time constant.
-template <int NW, int JT>
+// so every stencil offset is a compile-time constant. A slot holds the field
+// rows (storage type T), the p rows (double) and the previous substep's source
+// terms (T).
+template <int NW, int JT, class T>
 struct MarchLayout {
   static_assert(JT == 2 || JT == 4, "line groups start at odd j, so rows of even index have even j");
   static constexpr int E = NW;
-  static constexpr int RL = 32 * NW + 4;                 // >= nx + 4, even
-  static constexpr int NROW = 4 * (JT + 2) + (JT + 1);   // ux, uy, uz, t: JT + 2 rows; p: JT + 1
-  static constexpr int OLD = NROW * RL;                  // then the previous substep's source terms:
-  static constexpr int SLOT = OLD + 4 * JT * RL;         // JT packed lines per variable, at OLD + v JT RL
-  static constexpr int SL = 32 * E + (E > 1 ? 32 : 0);   // staging line (padded for the solves)
-  static constexpr int STAGE = NSLOT * SLOT;             // [2][JT][4][SL] after the ring
-  static constexpr int BAR = STAGE + 2 * JT * 4 * SL;    // NSLOT mbarriers after the staging
-  static constexpr size_t BYTES = sizeof(double) * (size_t)BAR + NSLOT * sizeof(unsigned long long);
+  static constexpr int RL = 32 * NW + 4;                      // values per row: >= nx + 4, multiple of 4
+  static constexpr int NFROW = 4 * (JT + 2);                  // ux, uy, uz, t: JT + 2 rows each
+  static constexpr size_t POFF = (size_t)NFROW * RL * sizeof(T);          // p: JT + 1 rows of double
+  static constexpr size_t OLDOFF = POFF + (size_t)(JT + 1) * RL * sizeof(double);
+  static constexpr size_t SLOT = OLDOFF + (size_t)4 * JT * RL * sizeof(T);  // JT lines per variable
+  static constexpr int SL = 32 * E + (E > 1 ? 32 : 0);        // staging line (padded for the solves)
+  static constexpr size_t STAGE = NSLOT * SLOT;               // [2][JT][4][SL] doubles after the ring
+  static constexpr size_t BAR = STAGE + sizeof(double) * 2 * JT * 4 * SL;   // NSLOT mbarriers
+  static constexpr size_t BYTES = BAR + NSLOT * sizeof(unsigned long long);
 };
 
 // Everything a group's march needs besides its coefficients.
+template <class T>
 struct MarchArgs {
   Geo g;
   Bc bc;
   Coefs cf;
   XFactors xf;
   double nu, kappa;
-  Fields in, out;
-  SrcSet ss;
+  FieldsT<T> in, out;
+  SrcSetT<T> ss;
   DeltaSet ds;
   int rkstep, mode, KC;
   unsigned * status;
@@ -424,10 +432,10 @@ struct MarchArgs {
 // The plane loop of one thread group: G = 0 computes ux and t, G = 1 uy and
 // uz, G = 2 all four (one group per line). With two groups both pass the same
 // barriers in the same order.
-template <int NW, int JT, int IMPL, int G>
-__device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, double * stage,
+template <int NW, int JT, int IMPL, int G, class T>
+__device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring, double * stage,
                                             unsigned long long * bar, int j0, int k0, int k1, double dt) {
-  using L = MarchLayout<NW, JT>;
+  using L = MarchLayout<NW, JT, T>;
   constexpr int E = L::E, RL = L::RL, SL = L::SL, NT = 32 * NW;
   constexpr bool GA = G != 1, GB = G != 0;   // group computes ux and t / uy and uz
   constexpr int NGRP = G == 2 ? 1 : 2;
@@ -437,8 +445,15 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
   const int lane = tx & 31, wid = tx >> 5;
   const int i = tx - (G == 1 ? NT : 0) + 1;
   const bool act = i <= nx;
-  const int of = (nx + 1) & 1, oc = (nx + 2) & 1;
+  // element offsets of odd rows in their widened copies: ux / centre fields
+  // (none in the FP32 layout, whose rows start on 16-byte boundaries) and p
+  constexpr bool D64 = sizeof(T) == 8;
+  const int of = D64 ? (nx + 1) & 1 : 0, oc = D64 ? (nx + 2) & 1 : 0, op = (nx + 2) & 1;
+  constexpr int FSH = D64 ? 1 : 0;   // ux face i at element i - FSH of its row
   const size_t sjc = (size_t)ny + 2;
+  auto frow = [&](char * slot, int f, int r) { return reinterpret_cast<T *>(slot) + (size_t)(f * (JT + 2) + r) * RL; };
+  auto prow = [&](char * slot, int r) { return reinterpret_cast<double *>(slot + L::POFF) + (size_t)r * RL; };
+  auto orow = [&](char * slot, int v) { return reinterpret_cast<T *>(slot + L::OLDOFF) + (size_t)v * JT * RL; };
 
   // Copies of plane kp into slot sl: the field rows and, for planes that are
   // computed in a substep with beta != 0, the source terms of the previous
@@ -446,36 +461,41 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
   // aligned as JT is even).
   const bool use_old = A.rkstep != 0;
   auto issue = [&](int kp, int sl) {
-    double * base = ring + (size_t)sl * L::SLOT;
-    const double * src[5] = {A.in.ux, A.in.uy, A.in.uz, A.in.t, A.in.p};
+    char * base = ring + (size_t)sl * L::SLOT;
     const bool olds = use_old && kp >= k0 && kp < k1;
-    unsigned total = 0;
-    for (int f = 0; f < 5; f++) {
-      const size_t n = (f == SF_UX) ? (size_t)nx + 1 : (size_t)nx + 2;
-      for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
-        const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
-        const size_t a = s0 & ~(size_t)1, b = (s0 + n + 1) & ~(size_t)1;
-        total += (unsigned)((b - a) * sizeof(double));
+    // every row of the five arrays (4 = p, in double), widened to 16-byte
+    // bounds: counts the bytes or issues the copies. With 8-byte storage the
+    // p rows continue the field rows' layout.
+    const char * src[5] = {reinterpret_cast<const char *>(A.in.ux), reinterpret_cast<const char *>(A.in.uy),
+                           reinterpret_cast<const char *>(A.in.uz), reinterpret_cast<const char *>(A.in.t),
+                           reinterpret_cast<const char *>(A.in.p)};
+    auto all = [&](bool go, unsigned & total) {
+      for (int f = 0; f < 5; f++) {
+        const size_t es = f == SF_P ? sizeof(double) : sizeof(T), al = 16 / es;
+        const size_t n = (f == SF_P || (D64 && f != SF_UX)) ? (size_t)nx + 2 : D64 ? (size_t)nx + 1 : (size_t)pitch32(nx);
+        for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
+          const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
+          const size_t a = s0 & ~(al - 1), b = (s0 + n + al - 1) & ~(al - 1);
+          const unsigned by = (unsigned)((b - a) * es);
+          const size_t off = (D64 || f != SF_P) ? (size_t)(f * (JT + 2) + r) * RL * sizeof(T)
+                                                : L::POFF + (size_t)r * RL * sizeof(double);
+          if (go) bulk_g2s(base + off, src[f] + a * es, by, &bar[sl]);
+          else total += by;
+        }
       }
-    }
-    if (olds) total += (unsigned)(JT * (4 * nx - 1) * sizeof(double));
+    };
+    unsigned total = 0;
+    all(false, total);
+    if (olds) total += (unsigned)(JT * (D64 ? 4 * nx - 1 : 4 * spitch32(nx)) * sizeof(T));
     mbar_expect_tx(&bar[sl], total);
     if (olds) {
       for (int v = 0; v < 4; v++) {
         const int ni = (v == VUX) ? nx - 1 : nx;
-        bulk_g2s(base + L::OLD + (size_t)v * JT * RL, A.ss.old_[v] + pidx(ni, ny, 0, j0, kp),
-                 (unsigned)(JT * ni * sizeof(double)), &bar[sl]);
+        const int li = D64 ? ni : spitch32(nx);   // packed line length (sline)
+        bulk_g2s(orow(base, v), A.ss.old_[v] + pidx(li, ny, 0, j0, kp), (unsigned)(JT * li * sizeof(T)), &bar[sl]);
       }
     }
-    for (int f = 0; f < 5; f++) {
-      const size_t n = (f == SF_UX) ? (size_t)nx + 1 : (size_t)nx + 2;
-      for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
-        const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
-        const size_t a = s0 & ~(size_t)1, b = (s0 + n + 1) & ~(size_t)1;
-        bulk_g2s(base + (size_t)(f * (JT + 2) + r) * RL, src[f] + a, (unsigned)((b - a) * sizeof(double)),
-                 &bar[sl]);
-      }
-    }
+    all(true, total);
   };
   if (tx == 0) {
     issue(k0 - 1, 0);
@@ -502,22 +522,23 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
   PrevA pa[JT];
   PrevB pb[JT];
   if (act) {
-    const double * cbs = ring + i, * fbs = ring + i - 1;
 #pragma unroll
     for (int jl = 0; jl < JT; jl++) {
       const int r1 = jl + 1, r2 = jl + 2;   // rows j and j + 1
       const int o1c = (r1 & 1) ? oc : 0, o1f = (r1 & 1) ? of : 0, o2c = (r2 & 1) ? oc : 0;
+      const int o1p = (r1 & 1) ? op : 0;
+      const T * ux1 = frow(ring, SF_UX, r1) + o1f + i - FSH;
       if constexpr (GA) {
-        pa[jl].ux0 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f];
-        pa[jl].t0 = cbs[(SF_T * (JT + 2) + r1) * RL + o1c];
+        pa[jl].ux0 = ux1[0];
+        pa[jl].t0 = frow(ring, SF_T, r1)[o1c + i];
       }
       if constexpr (GB) {
-        pb[jl].ux0 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f];
-        pb[jl].ux1 = fbs[(SF_UX * (JT + 2) + r1) * RL + o1f + 1];
-        pb[jl].uy0 = cbs[(SF_UY * (JT + 2) + r1) * RL + o1c];
-        pb[jl].uyjp = cbs[(SF_UY * (JT + 2) + r2) * RL + o2c];
-        pb[jl].uz0 = cbs[(SF_UZ * (JT + 2) + r1) * RL + o1c];
-        pb[jl].p0 = cbs[(SF_P * (JT + 2) + r1) * RL + o1c];
+        pb[jl].ux0 = ux1[0];
+        pb[jl].ux1 = ux1[1];
+        pb[jl].uy0 = frow(ring, SF_UY, r1)[o1c + i];
+        pb[jl].uyjp = frow(ring, SF_UY, r2)[o2c + i];
+        pb[jl].uz0 = frow(ring, SF_UZ, r1)[o1c + i];
+        pb[jl].p0 = prow(ring, r1)[o1p + i];
       }
     }
   }
@@ -541,31 +562,41 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
 #pragma unroll
       for (int v = 0; v < 4; v++) dl[jl][v] = u0[jl][v] = 0.;
     if (act) {
-      SlotView V;
-      V.cb = ring + (size_t)cur * L::SLOT + i;
+      char * cs = ring + (size_t)cur * L::SLOT;
+      char * ns = ring + (size_t)nxt * L::SLOT;
+      SlotView<T> V;
+      V.cb = reinterpret_cast<const T *>(cs) + i;
       V.cbo = V.cb + oc;
-      V.fb = V.cb - 1;
+      V.fb = V.cb - FSH;
       V.fbo = V.fb + of;
-      V.nb = ring + (size_t)nxt * L::SLOT + i;
+      V.nb = reinterpret_cast<const T *>(ns) + i;
       V.nbo = V.nb + oc;
-      V.nf = V.nb - 1;
+      V.nf = V.nb - FSH;
       V.nfo = V.nf + of;
-      const size_t qf = pidx(nx - 1, ny, i - 2, j0, k), qc = pidx(nx, ny, i - 1, j0, k);
-      const double * ob = ring + (size_t)cur * L::SLOT + L::OLD;   // old source terms of plane k
+      if constexpr (D64) {   // p rows follow the field rows: same base registers, constant offsets
+        V.pb = reinterpret_cast<const double *>(V.cb) + L::NFROW * RL;
+        V.pbo = reinterpret_cast<const double *>(V.cbo) + L::NFROW * RL;
+      } else {
+        V.pb = prow(cs, 0) + i;
+        V.pbo = V.pb + op;
+      }
+      const int lf = D64 ? nx - 1 : spitch32(nx), lc = D64 ? nx : spitch32(nx);   // source-term lines (sline)
+      const size_t qf = pidx(lf, ny, i - 2, j0, k), qc = pidx(lc, ny, i - 1, j0, k);
+      const T * ob = orow(cs, 0);   // old source terms of plane k
       auto cells = [&](auto jlc) {
         constexpr int JL = decltype(jlc)::value;
         double d2[2], w2[2];
         auto old = [&](int v, int e) {
-          return use_old ? ob[v * JT * RL + JL * (v == VUX ? nx - 1 : nx) + e] : 0.;
+          return use_old ? (double)ob[v * JT * RL + JL * (v == VUX ? lf : lc) + e] : 0.;
         };
         if constexpr (GA) {
-          cell_a<JT, RL, JL, IMPL>(qa, V, pa[JL], A.bc, A.cf, A.nu, A.kappa, i, qf + (size_t)JL * (nx - 1),
-                                   qc + (size_t)JL * nx, A.ss, ca, cb, cg, i >= 2 ? old(VUX, i - 2) : 0.,
+          cell_a<JT, RL, JL, IMPL>(qa, V, pa[JL], A.bc, A.cf, A.nu, A.kappa, i, qf + (size_t)JL * lf,
+                                   qc + (size_t)JL * lc, A.ss, ca, cb, cg, i >= 2 ? old(VUX, i - 2) : 0.,
                                    old(VT, i - 1), d2, w2);
           dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
         }
         if constexpr (GB) {
-          cell_b<JT, RL, JL, IMPL>(qb, V, pb[JL], A.bc, A.cf, A.nu, i, qc + (size_t)JL * nx, A.ss, ca, cb, cg,
+          cell_b<JT, RL, JL, IMPL>(qb, V, pb[JL], A.bc, A.cf, A.nu, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
                                    old(VUY, i - 1), old(VUZ, i - 1), d2, w2);
           dl[JL][VUY] = d2[0]; dl[JL][VUZ] = d2[1]; u0[JL][VUY] = w2[0]; u0[JL][VUZ] = w2[1];
         }
@@ -639,24 +670,24 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
       const double vz = u0[jl][VUZ] + dl[jl][VUZ];
       auto put = [&](int jj, int kk) {
         if constexpr (GA) {
-          A.out.ux[fidx(g, i, jj, kk)] = vx;
-          A.out.t[cidx(g, i, jj, kk)] = vt;
-          if (i == 1) A.out.t[cidx(g, 0, jj, kk)] = A.bc.t_xm;
+          A.out.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx;
+          A.out.t[sidx_c<T>(g, i, jj, kk)] = (T)vt;
+          if (i == 1) A.out.t[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.t_xm;
           if (i == nx) {
-            A.out.ux[fidx(g, nx + 1, jj, kk)] = 0.;
-            A.out.t[cidx(g, nx + 1, jj, kk)] = A.bc.t_xp;
+            A.out.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.;
+            A.out.t[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.t_xp;
           }
         }
         if constexpr (GB) {
-          A.out.uy[cidx(g, i, jj, kk)] = vy;
-          A.out.uz[cidx(g, i, jj, kk)] = vz;
+          A.out.uy[sidx_c<T>(g, i, jj, kk)] = (T)vy;
+          A.out.uz[sidx_c<T>(g, i, jj, kk)] = (T)vz;
           if (i == 1) {
-            A.out.uy[cidx(g, 0, jj, kk)] = A.bc.uy_xm;
-            A.out.uz[cidx(g, 0, jj, kk)] = 0.;
+            A.out.uy[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.uy_xm;
+            A.out.uz[sidx_c<T>(g, 0, jj, kk)] = (T)0.;
           }
           if (i == nx) {
-            A.out.uy[cidx(g, nx + 1, jj, kk)] = A.bc.uy_xp;
-            A.out.uz[cidx(g, nx + 1, jj, kk)] = 0.;
+            A.out.uy[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.uy_xp;
+            A.out.uz[sidx_c<T>(g, nx + 1, jj, kk)] = (T)0.;
           }
         }
       };
@@ -677,14 +708,14 @@ __device__ __forceinline__ void march_group(const MarchArgs & A, double * ring, 
 #endif
 // NG groups of 32 NW threads, one thread per radial index in each; CTA = JT
 // lines (j0 .. j0+JT-1) x KC planes.
-template <int NW, int JT, int IMPL>
+template <int NW, int JT, int IMPL, class T>
 __global__ void __launch_bounds__(32 * NW * TC_MARCH_GROUPS, 1)
-march_predict_kernel(MarchArgs A, const double * __restrict__ dtp) {
-  using L = MarchLayout<NW, JT>;
+march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
+  using L = MarchLayout<NW, JT, T>;
   extern __shared__ __align__(16) double sm[];
-  double * ring = sm;
-  double * stage = sm + L::STAGE;
-  unsigned long long * bar = reinterpret_cast<unsigned long long *>(sm + L::BAR);
+  char * ring = reinterpret_cast<char *>(sm);
+  double * stage = reinterpret_cast<double *>(ring + L::STAGE);
+  unsigned long long * bar = reinterpret_cast<unsigned long long *>(ring + L::BAR);
   const int tx = threadIdx.x;
   const int njg = A.g.ny / JT;
   const int j0 = (int)(blockIdx.x % njg) * JT + 1;   // odd
@@ -713,39 +744,38 @@ march_predict_kernel(MarchArgs A, const double * __restrict__ dtp) {
 #define TC_MARCH_KC 32
 #endif
 
-template <int NW>
-void launch_march_nw(const MarchArgs & A, const double * dtp, cudaStream_t st) {
+template <int NW, class T>
+void launch_march_nw(const MarchArgs<T> & A, const double * dtp, cudaStream_t st) {
   constexpr int JT = TC_MARCH_JT;   // ny is a power of two >= 4
   const long long nblk = (long long)(A.g.ny / JT) * (A.g.nz / A.KC);
   const int mask = (A.bc.implicit[0] ? 1 : 0) | (A.bc.implicit[1] ? 2 : 0) | (A.bc.implicit[2] ? 4 : 0);
   const unsigned grid = (unsigned)nblk, block = 32 * NW * TC_MARCH_GROUPS;
-  const size_t smem = MarchLayout<NW, JT>::BYTES;
+  const size_t smem = MarchLayout<NW, JT, T>::BYTES;
   switch (mask) {
-    case 1: march_predict_kernel<NW, JT, 1><<<grid, block, smem, st>>>(A, dtp); break;
-    case 7: march_predict_kernel<NW, JT, 7><<<grid, block, smem, st>>>(A, dtp); break;
-    case 0: march_predict_kernel<NW, JT, 0><<<grid, block, smem, st>>>(A, dtp); break;
-    default: march_predict_kernel<NW, JT, -1><<<grid, block, smem, st>>>(A, dtp); break;
+    case 1: march_predict_kernel<NW, JT, 1, T><<<grid, block, smem, st>>>(A, dtp); break;
+    case 7: march_predict_kernel<NW, JT, 7, T><<<grid, block, smem, st>>>(A, dtp); break;
+    case 0: march_predict_kernel<NW, JT, 0, T><<<grid, block, smem, st>>>(A, dtp); break;
+    default: march_predict_kernel<NW, JT, -1, T><<<grid, block, smem, st>>>(A, dtp); break;
   }
 }
 
-template <int NW>
+template <int NW, class T>
 void allow_march_smem() {
   constexpr int JT = TC_MARCH_JT;
-  const int bytes = (int)MarchLayout<NW, JT>::BYTES;
-  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 7>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const int bytes = (int)MarchLayout<NW, JT, T>::BYTES;
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 7, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
-}  // namespace
-
-void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
-                          double kappa, const Fields & in, const Fields & out, const SrcSet & ss,
-                          const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
-                          cudaStream_t st) {
-  MarchArgs A{g, bc, cf, xf, nu, kappa, in, out, ss, ds, rkstep, mode, g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC,
-              status};
+template <class T>
+void launch_march_t(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
+                    double kappa, const FieldBufs & in, const FieldBufs & out, const SrcBufs & ss,
+                    const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
+                    cudaStream_t st) {
+  MarchArgs<T> A{g, bc, cf, xf, nu, kappa, in.as<T>(), out.as<T>(), ss.as<T>(), ds, rkstep, mode,
+                 g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC, status};
   switch (predict_warps(g.nx)) {
     case 1: launch_march_nw<1>(A, dtp, st); break;
     case 2: launch_march_nw<2>(A, dtp, st); break;
@@ -754,11 +784,25 @@ void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const 
   }
 }
 
+}  // namespace
+
+void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const XFactors & xf, double nu,
+                          double kappa, const FieldBufs & in, const FieldBufs & out, const SrcBufs & ss,
+                          const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
+                          cudaStream_t st) {
+  if (in.bytes == 4) launch_march_t<float>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, status, st);
+  else launch_march_t<double>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, status, st);
+}
+
 void march_smem_limits() {
-  allow_march_smem<1>();
-  allow_march_smem<2>();
-  allow_march_smem<4>();
-  allow_march_smem<8>();
+  allow_march_smem<1, double>();
+  allow_march_smem<2, double>();
+  allow_march_smem<4, double>();
+  allow_march_smem<8, double>();
+  allow_march_smem<1, float>();
+  allow_march_smem<2, float>();
+  allow_march_smem<4, float>();
+  allow_march_smem<8, float>();
 }
 
 }  // namespace tcgpu

@@ -105,9 +105,9 @@ __device__ inline void warp_cfl(double ax, double ay, double az, double hx, doub
 #ifndef TC_CORRECT_MB_CFL
 #define TC_CORRECT_MB_CFL 4
 #endif
-template <int WHAT, int IMPL, bool CFL>
+template <int WHAT, int IMPL, bool CFL, class T>
 __global__ void __launch_bounds__(256, CFL ? TC_CORRECT_MB_CFL : TC_CORRECT_MB)
-correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp, int rkstep, double nu,
+correct_kernel(Geo g, Bc bc, Coefs cf, FieldsT<T> f, const double * __restrict__ dtp, int rkstep, double nu,
                unsigned long long * dtmin, unsigned * status) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -127,12 +127,13 @@ correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp
       // every input is loaded before the first store (the arrays are distinct,
       // which the compiler cannot know), so a thread's loads are in flight together
       const double * psi = f.psi;
-      const size_t qc = cidx(g, i, j, k), qf = fidx(g, i, j, k);
+      const size_t qp = cidx(g, i, j, k);                                 // p, psi
+      const size_t qc = sidx_c<T>(g, i, j, k), qf = sidx_f<T>(g, i, j, k);  // ux, uy, uz
       const size_t sj = (size_t)(nx + 2), sk = (size_t)(nx + 2) * (ny + 2);
-      const double psi0 = __ldg(psi + qc);
-      const double psi_im = __ldg(psi + qc - 1);
-      const double psi_jm = __ldg(psi + qc - sj);
-      const double psi_km = __ldg(psi + qc - sk);
+      const double psi0 = __ldg(psi + qp);
+      const double psi_im = __ldg(psi + qp - 1);
+      const double psi_jm = __ldg(psi + qp - sj);
+      const double psi_km = __ldg(psi + qp - sk);
       double psi_ip = 0., psi_jp = 0., psi_kp = 0.;
       double ux0 = 0., uy0 = 0., uz0 = 0., p0 = 0.;
       if (WHAT & CORRECT_VELOCITY) {
@@ -141,10 +142,10 @@ correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp
         uz0 = f.uz[qc];
       }
       if (WHAT & CORRECT_PRESSURE) {
-        p0 = f.p[qc];
-        if (ix) psi_ip = __ldg(psi + qc + 1);
-        if (iy) psi_jp = __ldg(psi + qc + sj);
-        if (iz) psi_kp = __ldg(psi + qc + sk);
+        p0 = f.p[qp];
+        if (ix) psi_ip = __ldg(psi + qp + 1);
+        if (iy) psi_jp = __ldg(psi + qp + sj);
+        if (iz) psi_kp = __ldg(psi + qp + sk);
       }
       const double dt = *dtp;
       const double pf = rk_gamma(rkstep) * dt;            // correct/main.c:21-22
@@ -152,21 +153,21 @@ correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp
       if (WHAT & CORRECT_VELOCITY) {
         // ux, i = 2..nx (correct/ux.c:25-52); walls stay zero
         const double vx = (i >= 2) ? ux0 - pf * __ldg(cf.c_invhxxf + i) * (-psi_im + psi0) : 0.;
-        f.ux[qf] = vx;
-        for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, i, jj, kk)] = vx; });
+        f.ux[qf] = (T)vx;
+        for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx; });
         if (i == nx) {
-          f.ux[qf + 1] = 0.;
-          for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[fidx(g, nx + 1, jj, kk)] = 0.; });
+          f.ux[qf + 1] = (T)0.;
+          for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.; });
         }
         // uy (correct/uy.c:25-52), uz (correct/uz.c:15-44) with their walls
         const double vy = uy0 - pf * __ldg(cf.c_invhyxc + i) * (-psi_jm + psi0);
         const double vz = uz0 - pf * cf.inv_hz * (-psi_km + psi0);
         auto put = [&](int jj, int kk) {
-          const size_t q = cidx(g, i, jj, kk);
-          f.uy[q] = vy;
-          f.uz[q] = vz;
-          if (i == 1) { f.uy[q - 1] = bc.uy_xm; f.uz[q - 1] = 0.; }
-          if (i == nx) { f.uy[q + 1] = bc.uy_xp; f.uz[q + 1] = 0.; }
+          const size_t q = sidx_c<T>(g, i, jj, kk);
+          f.uy[q] = (T)vy;
+          f.uz[q] = (T)vz;
+          if (i == 1) { f.uy[q - 1] = (T)bc.uy_xm; f.uz[q - 1] = (T)0.; }
+          if (i == nx) { f.uy[q + 1] = (T)bc.uy_xp; f.uz[q + 1] = (T)0.; }
         };
         put(j, k);
         for_images(j, k, ny, nz, put);
@@ -179,7 +180,7 @@ correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp
       }
       // p += psi, then the implicit-direction corrections (update_pressure.c:23-136)
       if (WHAT & CORRECT_PRESSURE) {
-        double val = p0 + psi0;
+        double val = p0 + psi0;   // p and psi are double in every storage mode
         const double ijd = __ldg(cf.c_invjdxc + i);
         if (ix) {
           const double l = __ldg(cf.c_pxl + i), u = __ldg(cf.c_pxu + i), c = -l - u;
@@ -210,45 +211,54 @@ correct_kernel(Geo g, Bc bc, Coefs cf, Fields f, const double * __restrict__ dtp
   }
 }
 
-template <int WHAT, int IMPL, bool CFL>
-static void launch_correct_t(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+template <int WHAT, int IMPL, bool CFL, class T>
+static void launch_correct_t(const Geo & g, const Bc & bc, const Coefs & cf, const FieldsT<T> & f, const double * dtp,
                              int rkstep, double nu, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz / (CFL ? TC_CFL_KZ : 1));   // nz: power of two >= 4
-  correct_kernel<WHAT, IMPL, CFL><<<grid, block, 0, st>>>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status);
+  correct_kernel<WHAT, IMPL, CFL, T><<<grid, block, 0, st>>>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status);
 }
 
-template <bool CFL>
-static void launch_correct_both(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f,
+template <bool CFL, class T>
+static void launch_correct_both(const Geo & g, const Bc & bc, const Coefs & cf, const FieldsT<T> & f,
                                 const double * dtp, int rkstep, double nu, unsigned long long * dtmin,
                                 unsigned * status, cudaStream_t st) {
   const int mask = (bc.implicit[0] ? 1 : 0) | (bc.implicit[1] ? 2 : 0) | (bc.implicit[2] ? 4 : 0);
   constexpr int B = CORRECT_VELOCITY | CORRECT_PRESSURE;
   switch (mask) {
-    case 1: launch_correct_t<B, 1, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
-    case 7: launch_correct_t<B, 7, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
-    case 0: launch_correct_t<B, 0, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
-    default: launch_correct_t<B, -1, CFL>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    case 1: launch_correct_t<B, 1, CFL, T>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    case 7: launch_correct_t<B, 7, CFL, T>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    case 0: launch_correct_t<B, 0, CFL, T>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
+    default: launch_correct_t<B, -1, CFL, T>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status, st); break;
   }
 }
 
-void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const Fields & f, const double * dtp,
+template <class T>
+static void launch_correct_s(const Geo & g, const Bc & bc, const Coefs & cf, const FieldsT<T> & f, const double * dtp,
+                             int rkstep, double nu, int what, unsigned long long * cfl_dtmin, unsigned * status,
+                             cudaStream_t st) {
+  if (what == CORRECT_VELOCITY)
+    launch_correct_t<CORRECT_VELOCITY, -1, false, T>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+  else if (what == CORRECT_PRESSURE)
+    launch_correct_t<CORRECT_PRESSURE, -1, false, T>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+  else if (cfl_dtmin)
+    launch_correct_both<true, T>(g, bc, cf, f, dtp, rkstep, nu, cfl_dtmin, status, st);
+  else
+    launch_correct_both<false, T>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+}
+
+void launch_correct(const Geo & g, const Bc & bc, const Coefs & cf, const FieldBufs & f, const double * dtp,
                     int rkstep, double nu, int what, unsigned long long * cfl_dtmin, unsigned * status,
                     cudaStream_t st) {
-  if (what == CORRECT_VELOCITY)
-    launch_correct_t<CORRECT_VELOCITY, -1, false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
-  else if (what == CORRECT_PRESSURE)
-    launch_correct_t<CORRECT_PRESSURE, -1, false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
-  else if (cfl_dtmin)
-    launch_correct_both<true>(g, bc, cf, f, dtp, rkstep, nu, cfl_dtmin, status, st);
-  else
-    launch_correct_both<false>(g, bc, cf, f, dtp, rkstep, nu, nullptr, status, st);
+  if (f.bytes == 4) launch_correct_s<float>(g, bc, cf, f.as<float>(), dtp, rkstep, nu, what, cfl_dtmin, status, st);
+  else launch_correct_s<double>(g, bc, cf, f.as<double>(), dtp, rkstep, nu, what, cfl_dtmin, status, st);
 }
 
 // --------------------------------------------------------------- decide_dt
+template <class T>
 __global__ void __launch_bounds__(256)
-dtmin_kernel(Geo g, const double * __restrict__ ux, const double * __restrict__ uy,
-             const double * __restrict__ uz, unsigned long long * dtmin, unsigned * status) {
+dtmin_kernel(Geo g, const T * __restrict__ ux, const T * __restrict__ uy,
+             const T * __restrict__ uz, unsigned long long * dtmin, unsigned * status) {
   const double small = 1.e-8;
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -260,12 +270,12 @@ dtmin_kernel(Geo g, const double * __restrict__ ux, const double * __restrict__ 
     hz = g.hz;
     for (int k = blockIdx.z + 1; k <= g.nz; k += gridDim.z) {
       if (i >= 2) {
-        const double v = __ldg(ux + fidx(g, i, j, k));
+        const double v = __ldg(ux + sidx_f<T>(g, i, j, k));
         bad |= !isfinite(v);
         ax = fmax(ax, fabs(v) + small);
       }
-      const double vy = __ldg(uy + cidx(g, i, j, k));
-      const double vz = __ldg(uz + cidx(g, i, j, k));
+      const double vy = __ldg(uy + sidx_c<T>(g, i, j, k));
+      const double vz = __ldg(uz + sidx_c<T>(g, i, j, k));
       bad |= !isfinite(vy) || !isfinite(vz);
       ay = fmax(ay, fabs(vy) + small);
       az = fmax(az, fabs(vz) + small);
@@ -302,10 +312,16 @@ dtfinal_kernel(double coef_adv, const double * caps, unsigned long long * dtmin,
   *dtp = dt;
 }
 
-void launch_dtmin(const Geo & g, const Fields & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
+void launch_dtmin(const Geo & g, const FieldBufs & f, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz < 16 ? g.nz : 16);
-  dtmin_kernel<<<grid, block, 0, st>>>(g, f.ux, f.uy, f.uz, dtmin, status);
+  if (f.bytes == 4) {
+    const FieldsT<float> a = f.as<float>();
+    dtmin_kernel<float><<<grid, block, 0, st>>>(g, a.ux, a.uy, a.uz, dtmin, status);
+  } else {
+    const FieldsT<double> a = f.as<double>();
+    dtmin_kernel<double><<<grid, block, 0, st>>>(g, a.ux, a.uy, a.uz, dtmin, status);
+  }
 }
 
 void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long * dtmin, double * dtp,
@@ -313,54 +329,61 @@ void launch_dtfinal(double coef_adv, const double * dt_caps, unsigned long long 
   dtfinal_kernel<<<1, DT_SLOTS, 0, st>>>(coef_adv, dt_caps, dtmin, dtp, status);
 }
 
-void launch_decide_dt(const Geo & g, const Fields & f, double coef_adv, const double * dt_caps,
+void launch_decide_dt(const Geo & g, const FieldBufs & f, double coef_adv, const double * dt_caps,
                       unsigned long long * dtmin, double * dtp, unsigned * status, cudaStream_t st) {
   launch_dtmin(g, f, dtmin, status, st);
   launch_dtfinal(coef_adv, dt_caps, dtmin, dtp, status, st);
 }
 
 // --------------------------------------------------------------- boundary conditions
-__global__ void bc_kernel(Geo g, Bc bc, int kind, double * __restrict__ a) {
+// T: storage type of the field (p and psi are always double; ux, uy, uz, t
+// follow the storage mode)
+template <class T>
+__global__ void bc_kernel(Geo g, Bc bc, int kind, T * __restrict__ a) {
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;   // position in the row
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   if (j > ny) return;
+  const bool state = kind != BC_P && kind != BC_PSI;     // p, psi: reference layout (double)
+  auto ic = [&](int ii, int jj, int kk) { return state ? sidx_c<T>(g, ii, jj, kk) : cidx(g, ii, jj, kk); };
   if (kind == BC_UX) {
     if (e > nx) return;                                  // i = e + 1
-    double * row = a + fidx(g, 1, j, k);
-    double val = (e == 0 || e == nx) ? 0. : row[e];
+    T * row = a + sidx_f<T>(g, 1, j, k);
+    const T val = (e == 0 || e == nx) ? (T)0. : row[e];
     row[e] = val;
-    for_images(j, k, ny, nz, [&](int jj, int kk) { a[fidx(g, 1, jj, kk) + e] = val; });
+    for_images(j, k, ny, nz, [&](int jj, int kk) { a[sidx_f<T>(g, 1, jj, kk) + e] = val; });
     return;
   }
   if (e > nx + 1) return;                                // i = e
-  double * row = a + cidx(g, 0, j, k);
-  double val;
+  T * row = a + ic(0, j, k);
+  T val;
   if (e == 0 || e == nx + 1) {
     const bool lo = (e == 0);
     switch (kind) {
-      case BC_UY: val = lo ? bc.uy_xm : bc.uy_xp; break;
-      case BC_UZ: val = 0.; break;
-      case BC_T: val = lo ? bc.t_xm : bc.t_xp; break;
+      case BC_UY: val = (T)(lo ? bc.uy_xm : bc.uy_xp); break;
+      case BC_UZ: val = (T)0.; break;
+      case BC_T: val = (T)(lo ? bc.t_xm : bc.t_xp); break;
       default: val = lo ? row[1] : row[nx]; break;       // p, psi: Neumann copy
     }
   } else {
     val = row[e];
   }
   row[e] = val;
-  for_images(j, k, ny, nz, [&](int jj, int kk) { a[cidx(g, 0, jj, kk) + e] = val; });
+  for_images(j, k, ny, nz, [&](int jj, int kk) { a[ic(0, jj, kk) + e] = val; });
 }
 
-void launch_bc(const Geo & g, const Bc & bc, BcKind kind, double * a, cudaStream_t st) {
+void launch_bc(const Geo & g, const Bc & bc, BcKind kind, void * a, int bytes, cudaStream_t st) {
   dim3 block(64, 4, 1);
   dim3 grid((g.nx + 2 + 63) / 64, (g.ny + 3) / 4, g.nz);
-  bc_kernel<<<grid, block, 0, st>>>(g, bc, (int)kind, a);
+  if (bytes == 4) bc_kernel<float><<<grid, block, 0, st>>>(g, bc, (int)kind, static_cast<float *>(a));
+  else bc_kernel<double><<<grid, block, 0, st>>>(g, bc, (int)kind, static_cast<double *>(a));
 }
 
 // --------------------------------------------------------------- tensors
 // Row lengths: face tensors (lxy lxz lyx0 lyx1 lzx) nx+1, centre tensors nx.
-__global__ void tensor_kernel(Geo g, Coefs cf, Fields f, Tensors tn) {
+template <class T>
+__global__ void tensor_kernel(Geo g, Coefs cf, FieldsT<T> f, Tensors tn) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;   // 1..nx+1
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
@@ -368,16 +391,16 @@ __global__ void tensor_kernel(Geo g, Coefs cf, Fields f, Tensors tn) {
   if (i > nx + 1 || j > ny) return;
   auto fi = [&](int ii, int jj, int kk) { return (size_t)(ii - 1) + (size_t)(nx + 1) * ((size_t)jj + (size_t)(ny + 2) * kk); };
   auto ci = [&](int ii, int jj, int kk) { return (size_t)(ii - 1) + (size_t)nx * ((size_t)jj + (size_t)(ny + 2) * kk); };
-  const double * ux = f.ux;
-  const double * uy = f.uy;
-  const double * uz = f.uz;
+  const T * ux = f.ux;
+  const T * uy = f.uy;
+  const T * uz = f.uz;
   {  // face tensors
     const double ih = __ldg(cf.c_invhxxf + i);
-    const double lxy = ih * (-uy[cidx(g, i - 1, j, k)] + uy[cidx(g, i, j, k)]);
-    const double lxz = ih * (-uz[cidx(g, i - 1, j, k)] + uz[cidx(g, i, j, k)]);
-    const double lyx0 = __ldg(cf.c_invhyxf + i) * (-ux[fidx(g, i, j - 1, k)] + ux[fidx(g, i, j, k)]);
-    const double lyx1 = __ldg(cf.c_lyx1f + i) * (__ldg(cf.c_wm + i) * uy[cidx(g, i - 1, j, k)] + __ldg(cf.c_wp + i) * uy[cidx(g, i, j, k)]);
-    const double lzx = cf.inv_hz * (-ux[fidx(g, i, j, k - 1)] + ux[fidx(g, i, j, k)]);
+    const double lxy = ih * (-(double)uy[sidx_c<T>(g, i - 1, j, k)] + (double)uy[sidx_c<T>(g, i, j, k)]);
+    const double lxz = ih * (-(double)uz[sidx_c<T>(g, i - 1, j, k)] + (double)uz[sidx_c<T>(g, i, j, k)]);
+    const double lyx0 = __ldg(cf.c_invhyxf + i) * (-(double)ux[sidx_f<T>(g, i, j - 1, k)] + (double)ux[sidx_f<T>(g, i, j, k)]);
+    const double lyx1 = __ldg(cf.c_lyx1f + i) * (__ldg(cf.c_wm + i) * (double)uy[sidx_c<T>(g, i - 1, j, k)] + __ldg(cf.c_wp + i) * (double)uy[sidx_c<T>(g, i, j, k)]);
+    const double lzx = cf.inv_hz * (-(double)ux[sidx_f<T>(g, i, j, k - 1)] + (double)ux[sidx_f<T>(g, i, j, k)]);
     const double vals[5] = {lxy, lxz, lyx0, lyx1, lzx};
     const int slot[5] = {1, 2, 3, 4, 8};
     for (int s = 0; s < 5; s++) {
@@ -387,13 +410,13 @@ __global__ void tensor_kernel(Geo g, Coefs cf, Fields f, Tensors tn) {
     }
   }
   if (i <= nx) {  // centre tensors
-    const double lxx = (1. / __ldg(g.hxxc + i)) * (-ux[fidx(g, i, j, k)] + ux[fidx(g, i + 1, j, k)]);
+    const double lxx = (1. / __ldg(g.hxxc + i)) * (-(double)ux[sidx_f<T>(g, i, j, k)] + (double)ux[sidx_f<T>(g, i + 1, j, k)]);
     const double ihy = __ldg(cf.c_invhyxc + i);
-    const double lyy0 = ihy * (-uy[cidx(g, i, j, k)] + uy[cidx(g, i, j + 1, k)]);
-    const double lyy1 = __ldg(cf.c_lyy1 + i) * (0.5 * ux[fidx(g, i, j, k)] + 0.5 * ux[fidx(g, i + 1, j, k)]);
-    const double lyz = ihy * (-uz[cidx(g, i, j - 1, k)] + uz[cidx(g, i, j, k)]);
-    const double lzy = cf.inv_hz * (-uy[cidx(g, i, j, k - 1)] + uy[cidx(g, i, j, k)]);
-    const double lzz = cf.inv_hz * (-uz[cidx(g, i, j, k)] + uz[cidx(g, i, j, k + 1)]);
+    const double lyy0 = ihy * (-(double)uy[sidx_c<T>(g, i, j, k)] + (double)uy[sidx_c<T>(g, i, j + 1, k)]);
+    const double lyy1 = __ldg(cf.c_lyy1 + i) * (0.5 * (double)ux[sidx_f<T>(g, i, j, k)] + 0.5 * (double)ux[sidx_f<T>(g, i + 1, j, k)]);
+    const double lyz = ihy * (-(double)uz[sidx_c<T>(g, i, j - 1, k)] + (double)uz[sidx_c<T>(g, i, j, k)]);
+    const double lzy = cf.inv_hz * (-(double)uy[sidx_c<T>(g, i, j, k - 1)] + (double)uy[sidx_c<T>(g, i, j, k)]);
+    const double lzz = cf.inv_hz * (-(double)uz[sidx_c<T>(g, i, j, k)] + (double)uz[sidx_c<T>(g, i, j, k + 1)]);
     const double vals[6] = {lxx, lyy0, lyy1, lyz, lzy, lzz};
     const int slot[6] = {0, 5, 6, 7, 9, 10};
     for (int s = 0; s < 6; s++) {
@@ -404,25 +427,27 @@ __global__ void tensor_kernel(Geo g, Coefs cf, Fields f, Tensors tn) {
   }
 }
 
-void launch_tensors(const Geo & g, const Coefs & cf, const Fields & f, const Tensors & tn, cudaStream_t st) {
+void launch_tensors(const Geo & g, const Coefs & cf, const FieldBufs & f, const Tensors & tn, cudaStream_t st) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 1 + 31) / 32, (g.ny + 7) / 8, g.nz);
-  tensor_kernel<<<grid, block, 0, st>>>(g, cf, f, tn);
+  if (f.bytes == 4) tensor_kernel<float><<<grid, block, 0, st>>>(g, cf, f.as<float>(), tn);
+  else tensor_kernel<double><<<grid, block, 0, st>>>(g, cf, f.as<double>(), tn);
 }
 
 // --------------------------------------------------------------- diagnostics
 // partial[b][0..8]: max|div|, inj_m, inj_s, dis_m, dis_s, e_ux, e_uy, e_uz, e_t
 constexpr int DIAG_BLOCKS = 296;
 
+template <class T>
 __global__ void __launch_bounds__(256)
-diag_kernel(Geo g, Coefs cf, Bc bc, Fields f, double * partial) {
+diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, double * partial) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long total = (long long)(nx + 1) * ny * nz;
   double acc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
-  const double * ux = f.ux;
-  const double * uy = f.uy;
-  const double * uz = f.uz;
-  const double * t = f.t;
+  const T * ux = f.ux;
+  const T * uy = f.uy;
+  const T * uz = f.uz;
+  const T * t = f.t;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
        c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % (nx + 1)) + 1;     // 1..nx+1
@@ -433,19 +458,19 @@ diag_kernel(Geo g, Coefs cf, Bc bc, Fields f, double * partial) {
     const double hxf = __ldg(g.hxxf + i);
     // face quantities at i
     const double ih = __ldg(cf.c_invhxxf + i);
-    const double uyim = uy[cidx(g, i - 1, j, k)], uyi = uy[cidx(g, i, j, k)];
+    const double uyim = (double)uy[sidx_c<T>(g, i - 1, j, k)], uyi = (double)uy[sidx_c<T>(g, i, j, k)];
     const double lxy = ih * (-uyim + uyi);
-    const double lxz = ih * (-uz[cidx(g, i - 1, j, k)] + uz[cidx(g, i, j, k)]);
-    const double lyx = __ldg(cf.c_invhyxf + i) * (-ux[fidx(g, i, j - 1, k)] + ux[fidx(g, i, j, k)])
+    const double lxz = ih * (-(double)uz[sidx_c<T>(g, i - 1, j, k)] + (double)uz[sidx_c<T>(g, i, j, k)]);
+    const double lyx = __ldg(cf.c_invhyxf + i) * (-(double)ux[sidx_f<T>(g, i, j - 1, k)] + (double)ux[sidx_f<T>(g, i, j, k)])
                      + __ldg(cf.c_lyx1f + i) * (__ldg(cf.c_wm + i) * uyim + __ldg(cf.c_wp + i) * uyi);
-    const double lzx = cf.inv_hz * (-ux[fidx(g, i, j, k - 1)] + ux[fidx(g, i, j, k)]);
+    const double lzx = cf.inv_hz * (-(double)ux[sidx_f<T>(g, i, j, k - 1)] + (double)ux[sidx_f<T>(g, i, j, k)]);
     // dissipation.c:40-151 (face contributions)
     acc[3] += jdf * lyx * (lyx + lxy);
     acc[3] += jdf * lzx * (lzx + lxz);
     acc[3] += jdf * lxy * (lxy + lyx);
     acc[3] += jdf * lxz * (lxz + lzx);
     {  // dissipation.c:240-265 (scalar, x)
-      const double d = -t[cidx(g, i - 1, j, k)] + t[cidx(g, i, j, k)];
+      const double d = -(double)t[sidx_c<T>(g, i - 1, j, k)] + (double)t[sidx_c<T>(g, i, j, k)];
       const double q = d / hxf;
       acc[4] += jdf * (q * q);
     }
@@ -454,20 +479,20 @@ diag_kernel(Geo g, Coefs cf, Bc bc, Fields f, double * partial) {
       const double sgn = (i == 1) ? -1. : 1.;
       const double uyw = (i == 1) ? uyim : uyi;
       acc[1] += sgn * jdf / hxf * uyw * (lyx + lxy);
-      const double tw = (i == 1) ? t[cidx(g, 0, j, k)] : t[cidx(g, nx + 1, j, k)];
-      const double dtw = (i == 1) ? (-t[cidx(g, 0, j, k)] + t[cidx(g, 1, j, k)])
-                                  : (-t[cidx(g, nx, j, k)] + t[cidx(g, nx + 1, j, k)]);
+      const double tw = (i == 1) ? (double)t[sidx_c<T>(g, 0, j, k)] : (double)t[sidx_c<T>(g, nx + 1, j, k)];
+      const double dtw = (i == 1) ? (-(double)t[sidx_c<T>(g, 0, j, k)] + (double)t[sidx_c<T>(g, 1, j, k)])
+                                  : (-(double)t[sidx_c<T>(g, nx, j, k)] + (double)t[sidx_c<T>(g, nx + 1, j, k)]);
       acc[2] += sgn * jdf / hxf * tw / hxf * dtw;
     }
     if (i >= 2 && i <= nx) {  // total_energy.c:45-51
-      const double v = ux[fidx(g, i, j, k)];
+      const double v = (double)ux[sidx_f<T>(g, i, j, k)];
       acc[5] += jdf * 0.5 * (v * v);
     }
     if (i <= nx) {
       const double jdc = __ldg(g.jdxc + i);
-      const double ux0 = ux[fidx(g, i, j, k)], ux1 = ux[fidx(g, i + 1, j, k)];
-      const double uy0 = uyi, uy1 = uy[cidx(g, i, j + 1, k)];
-      const double uz0 = uz[cidx(g, i, j, k)], uz1 = uz[cidx(g, i, j, k + 1)];
+      const double ux0 = (double)ux[sidx_f<T>(g, i, j, k)], ux1 = (double)ux[sidx_f<T>(g, i + 1, j, k)];
+      const double uy0 = uyi, uy1 = (double)uy[sidx_c<T>(g, i, j + 1, k)];
+      const double uz0 = (double)uz[sidx_c<T>(g, i, j, k)], uz1 = (double)uz[sidx_c<T>(g, i, j, k + 1)];
       // divergence.c:56-78
       const double div = __ldg(cf.c_invjdxc + i) * (
           -__ldg(cf.c_jf + i) * ux0 + __ldg(cf.c_jf + i + 1) * ux1
@@ -478,21 +503,21 @@ diag_kernel(Geo g, Coefs cf, Bc bc, Fields f, double * partial) {
       const double lxx = (1. / __ldg(g.hxxc + i)) * (-ux0 + ux1);
       const double ihy = __ldg(cf.c_invhyxc + i);
       const double lyy = ihy * (-uy0 + uy1) + __ldg(cf.c_lyy1 + i) * (0.5 * ux0 + 0.5 * ux1);
-      const double lyz = ihy * (-uz[cidx(g, i, j - 1, k)] + uz0);
-      const double lzy = cf.inv_hz * (-uy[cidx(g, i, j, k - 1)] + uy0);
+      const double lyz = ihy * (-(double)uz[sidx_c<T>(g, i, j - 1, k)] + uz0);
+      const double lzy = cf.inv_hz * (-(double)uy[sidx_c<T>(g, i, j, k - 1)] + uy0);
       const double lzz = cf.inv_hz * (-uz0 + uz1);
       acc[3] += jdc * lxx * (lxx + lxx);
       acc[3] += jdc * lyy * (lyy + lyy);
       acc[3] += jdc * lzy * (lzy + lyz);
       acc[3] += jdc * lyz * (lyz + lzy);
       acc[3] += jdc * lzz * (lzz + lzz);
-      const double t0 = t[cidx(g, i, j, k)];
+      const double t0 = (double)t[sidx_c<T>(g, i, j, k)];
       {
-        const double q = (-t[cidx(g, i, j - 1, k)] + t0) / __ldg(g.hyxc + i);
+        const double q = (-(double)t[sidx_c<T>(g, i, j - 1, k)] + t0) / __ldg(g.hyxc + i);
         acc[4] += jdc * (q * q);
       }
       {
-        const double q = (-t[cidx(g, i, j, k - 1)] + t0) / g.hz;
+        const double q = (-(double)t[sidx_c<T>(g, i, j, k - 1)] + t0) / g.hz;
         acc[4] += jdc * (q * q);
       }
       acc[6] += jdc * 0.5 * (uy0 * uy0);
@@ -529,10 +554,38 @@ __global__ void diag_final_kernel(const double * partial, int nblocks, double nu
   out[q] = v;
 }
 
-void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const Fields & f, double nu, double kappa,
+void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, double nu, double kappa,
                         double * out, double * partial, cudaStream_t st) {
-  diag_kernel<<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f, partial);
+  if (f.bytes == 4) diag_kernel<float><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<float>(), partial);
+  else diag_kernel<double><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<double>(), partial);
   diag_final_kernel<<<1, 32, 0, st>>>(partial, DIAG_BLOCKS, nu, kappa, out);
+}
+
+// --------------------------------------------------------------- FP32 storage
+// rows of nref doubles (the reference's layout) <-> rows of pitch floats with
+// element e of a row at e + shift (the FP32 layout: shift 1 for ux, whose face
+// i sits at element i - 1 of a reference row and at element i of an FP32 row)
+__global__ void pack32_kernel(const double * __restrict__ src, float * __restrict__ dst, size_t rows, int nref,
+                              int pitch, int shift) {
+  const size_t n = rows * (size_t)nref;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = q / nref, e = q % nref;
+    dst[r * pitch + e + shift] = (float)src[q];
+  }
+}
+__global__ void unpack32_kernel(const float * __restrict__ src, double * __restrict__ dst, size_t rows, int nref,
+                                int pitch, int shift) {
+  const size_t n = rows * (size_t)nref;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = q / nref, e = q % nref;
+    dst[q] = (double)src[r * pitch + e + shift];
+  }
+}
+void launch_pack32(const double * src, float * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st) {
+  pack32_kernel<<<2368, 256, 0, st>>>(src, dst, rows, nref, pitch, shift);
+}
+void launch_unpack32(const float * src, double * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st) {
+  unpack32_kernel<<<2368, 256, 0, st>>>(src, dst, rows, nref, pitch, shift);
 }
 
 }  // namespace tcgpu

@@ -61,6 +61,16 @@
 
 namespace tcgpu {
 
+// spectral values as stored: double2, or float2 in the FP32-storage mode
+// (arithmetic in double either way)
+__device__ __forceinline__ double2 zget(const double2 * p) { return *p; }
+__device__ __forceinline__ double2 zget(const float2 * p) {
+  const float2 v = *p;
+  return make_double2((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void zput(double2 * p, double2 v) { *p = v; }
+__device__ __forceinline__ void zput(float2 * p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+
 __device__ inline double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -305,11 +315,11 @@ __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg,
 // --------------------------------------------------------------- forward y
 // CTA: P complex lines (radial indices i0 .. i0+2P-1) x all j at one k;
 // TPL = ny / EPT threads per line.
-template <int EPT>
+template <int EPT, class T, class Z>
 __global__ void __launch_bounds__(TC_FFTY_THREADS, TC_DIVFFT_MIN_BLOCKS)
 div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
-                const double * __restrict__ ux, const double * __restrict__ uy,
-                const double * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
+                const T * __restrict__ ux, const T * __restrict__ uy,
+                const T * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz;
   const int TI = 2 * P;
@@ -329,12 +339,12 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
       const int i = i0 + ii;
       double val = 0.;
       if (i <= nx) {
-        const double ux_xm = __ldg(ux + fidx(g, i, j, k));
-        const double ux_xp = __ldg(ux + fidx(g, i + 1, j, k));
-        const double uy_ym = __ldg(uy + cidx(g, i, j, k));
-        const double uy_yp = __ldg(uy + cidx(g, i, j + 1, k));
-        const double uz_zm = __ldg(uz + cidx(g, i, j, k));
-        const double uz_zp = __ldg(uz + cidx(g, i, j, k + 1));
+        const double ux_xm = __ldg(ux + sidx_f<T>(g, i, j, k));
+        const double ux_xp = __ldg(ux + sidx_f<T>(g, i + 1, j, k));
+        const double uy_ym = __ldg(uy + sidx_c<T>(g, i, j, k));
+        const double uy_yp = __ldg(uy + sidx_c<T>(g, i, j + 1, k));
+        const double uz_zm = __ldg(uz + sidx_c<T>(g, i, j, k));
+        const double uz_zp = __ldg(uz + sidx_c<T>(g, i, j, k + 1));
         const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
         const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i);
         const double div = __ldg(cf.c_invjdxc + i) * (
@@ -356,11 +366,11 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
       const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
       const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i);
       const double ijd = __ldg(cf.c_invjdxc + i);
-      const double * __restrict__ pxm = ux + fidx(g, i, 0, k);
-      const double * __restrict__ pym = uy + cidx(g, i, 0, k);
-      const double * __restrict__ pzm = uz + cidx(g, i, 0, k);
-      const double * __restrict__ pzp = uz + cidx(g, i, 0, k + 1);
-      const int sf = nx + 1, sc = nx + 2;
+      const T * __restrict__ pxm = ux + sidx_f<T>(g, i, 0, k);
+      const T * __restrict__ pym = uy + sidx_c<T>(g, i, 0, k);
+      const T * __restrict__ pzm = uz + sidx_c<T>(g, i, 0, k);
+      const T * __restrict__ pzp = uz + sidx_c<T>(g, i, 0, k + 1);
+      const int sf = srow_f<T>(g), sc = srow_c<T>(g);
 #pragma unroll 8
       for (int r = 0; r < 2 * EPT; r++) {
         const int j = j0 + r * jstep;
@@ -397,7 +407,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
     double2 out;
     if ((ii & 1) == 0) out = make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y - zn.y));
     else out = make_double2(0.5 * (zm.y + zn.y), -0.5 * (zm.x - zn.x));
-    ps.spec[((size_t)(i - 1) * nz + (k - 1)) * nyh + m] = out;
+    zput(static_cast<Z *>(ps.spec) + ((size_t)(i - 1) * nz + (k - 1)) * nyh + m, out);
   };
   for (int idx = threadIdx.x; idx < TI * half; idx += blockDim.x) put(idx >> (lg - 1), idx & (half - 1));
   for (int ii = threadIdx.x; ii < TI; ii += blockDim.x) put(ii, half);
@@ -408,7 +418,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
 // (p, t) = (tid mod P, tid / P): lanes run along the contiguous wavenumbers, so
 // the first pass reads and the last pass writes rows of P values straight from
 // and to the spectral array.
-template <int EPT, int SIGN>
+template <int EPT, int SIGN, class Z>
 __global__ void __launch_bounds__(TC_FFTZ_THREADS, TC_FFTZ_MIN_BLOCKS)
 fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   extern __shared__ double2 smem[];
@@ -418,10 +428,10 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   const int i = blockIdx.x;          // 0..nx-1
   const int p = threadIdx.x % P, t = threadIdx.x / P;
   const int m = blockIdx.y * P + p;
-  double2 * col = ps.spec + (size_t)i * nz * nyh + m;
+  Z * col = static_cast<Z *>(ps.spec) + (size_t)i * nz * nyh + m;
   const bool gv = m < nyh;
-  auto ld = [&](int e) { return gv ? col[(size_t)e * nyh] : make_double2(0., 0.); };
-  auto st = [&](int e, double2 v) { if (gv) col[(size_t)e * nyh] = v; };
+  auto ld = [&](int e) { return gv ? zget(col + (size_t)e * nyh) : make_double2(0., 0.); };
+  auto st = [&](int e, double2 v) { if (gv) zput(col + (size_t)e * nyh, v); };
   fft_io<EPT, SIGN, true, true>(smem + (size_t)p * LS, ld, st, nz, lg, t, TPL, ps.tw_z);
 }
 
@@ -431,6 +441,7 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
 #ifndef TC_TDM_PREFETCH
 #define TC_TDM_PREFETCH 2
 #endif
+template <class Z>
 __global__ void __launch_bounds__(128, 8)
 tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * __restrict__ tab_z,
            const double * __restrict__ base) {
@@ -440,7 +451,7 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
   const int m = (int)(tid % nyh);
   const int kz = (int)(tid / nyh);
   const size_t st = (size_t)nz * nyh;
-  double2 * q = ps.spec + (size_t)kz * nyh + m;
+  Z * q = static_cast<Z *>(ps.spec) + (size_t)kz * nyh + m;
   double * v = ps.vscr + (size_t)kz * nyh + m;
   const double tz = __ldg(tab_z + kz);
   const bool pin = (m == 0 && kz == 0);
@@ -453,17 +464,17 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
   };
   if (n == 1) {
     const double c = cdiag(0);
-    double2 x = q[0];
-    q[0] = pin ? make_double2(0., 0.) : make_double2(x.x / c, x.y / c);
+    const double2 x = zget(q);
+    zput(q, pin ? make_double2(0., 0.) : make_double2(x.x / c, x.y / c));
     return;
   }
   // forward elimination (src/tdm.c:24-44)
   double c0 = cdiag(0);
   double vprev = __ldg(ps.tu) / c0;
   v[0] = vprev;
-  double2 qprev = q[0];
+  double2 qprev = zget(q);
   qprev = make_double2(qprev.x / c0, qprev.y / c0);
-  q[0] = qprev;
+  zput(q, qprev);
   // rows are fetched G at a time ahead of the recurrence, so G loads per
   // thread are in flight together
   constexpr int G = TC_TDM_PREFETCH;
@@ -474,7 +485,7 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
     for (int u = 0; u < G; u++) {
       const int i = ib + u;
       if (i < n - 1) {
-        r[u] = q[(size_t)i * st];
+        r[u] = zget(q + (size_t)i * st);
         cd[u] = cdiag(i);
       }
     }
@@ -487,7 +498,7 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
         vprev = val * __ldg(ps.tu + i);
         v[(size_t)i * st] = vprev;
         qprev = make_double2(val * (r[u].x - l * qprev.x), val * (r[u].y - l * qprev.y));
-        q[(size_t)i * st] = qprev;
+        zput(q + (size_t)i * st, qprev);
       }
     }
   }
@@ -495,14 +506,14 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
     const int i = n - 1;
     const double l = __ldg(ps.tl + i);
     const double val = cdiag(i) - l * vprev;
-    const double2 r = q[(size_t)i * st];
+    const double2 r = zget(q + (size_t)i * st);
     double2 x;
     if (pin) x = make_double2(0., 0.);
     else {
       const double iv = 1. / val;
       x = make_double2(iv * (r.x - l * qprev.x), iv * (r.y - l * qprev.y));
     }
-    q[(size_t)i * st] = x;
+    zput(q + (size_t)i * st, x);
     qprev = x;
   }
   // back substitution
@@ -514,7 +525,7 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
       const int i = ib - u;
       if (i >= 0) {
         vi[u] = v[(size_t)i * st];
-        r[u] = q[(size_t)i * st];
+        r[u] = zget(q + (size_t)i * st);
       }
     }
 #pragma unroll
@@ -522,14 +533,14 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
       const int i = ib - u;
       if (i >= 0) {
         qprev = make_double2(r[u].x - vi[u] * qprev.x, r[u].y - vi[u] * qprev.y);
-        q[(size_t)i * st] = qprev;
+        zput(q + (size_t)i * st, qprev);
       }
     }
   }
 }
 
 // --------------------------------------------------------------- inverse y
-template <int EPT>
+template <int EPT, class Z>
 __global__ void __launch_bounds__(TC_FFTY_THREADS, TC_IFFTY_MIN_BLOCKS)
 iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   extern __shared__ double2 smem[];
@@ -548,8 +559,9 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
     const int ia = i0 + 2 * pp, ib = ia + 1;
     const int mr = (m <= ny / 2) ? m : ny - m;
     double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
-    if (ia <= nx) xa = ps.spec[((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr];
-    if (ib <= nx) xb = ps.spec[((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr];
+    const Z * sp = static_cast<const Z *>(ps.spec);
+    if (ia <= nx) xa = zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr);
+    if (ib <= nx) xb = zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr);
     if (mr == 0 || 2 * mr == ny) { xa.y = 0.; xb.y = 0.; }
     double2 z;
     if (m <= ny / 2) z = make_double2(xa.x - xb.y, xa.y + xb.x);
@@ -602,8 +614,8 @@ static int lines_per_cta(int n, int cap, int ept_max = 16, int threads = 256) {
   return p < 1 ? 1 : p;
 }
 
-template <int EPTY, int EPTZ>
-static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+template <int EPTY, int EPTZ, class T, class Z>
+static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps, const FieldsT<T> & f,
                              const double * tab_y, const double * tab_z, const double * base,
                              const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
   auto mark = [&](int kk) { if (pm.mark) pm.mark(kk, 1); };
@@ -612,38 +624,51 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   const int tply = g.ny / EPTY;
   const size_t smy = sizeof(double2) * (size_t)Py * padded_len(g.ny);
   dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
-  div_ffty_kernel<EPTY><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
+  div_ffty_kernel<EPTY, T, Z><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
   mark(pm.k_div);
   const int Pz = lines_per_cta(g.nz, ps.nyh, EPTZ, TC_FFTZ_THREADS);
   const int tplz = g.nz / EPTZ;
   const size_t smz = sizeof(double2) * (size_t)Pz * padded_len(g.nz);
   dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
-  fftz_kernel<EPTZ, -1><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  fftz_kernel<EPTZ, -1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   mark(pm.k_fwd);
   const long long nl = (long long)ps.nyh * g.nz;
-  tdm_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+  tdm_kernel<Z><<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
   mark(pm.k_tdm);
-  fftz_kernel<EPTZ, +1><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  fftz_kernel<EPTZ, +1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   mark(pm.k_inv);
-  iffty_kernel<EPTY><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
+  iffty_kernel<EPTY, Z><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
   mark(pm.k_ify);
 }
 
-template <int EPTY>
-static void launch_poisson_z(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+template <int EPTY, class T, class Z>
+static void launch_poisson_z(const Geo & g, const Coefs & cf, const Poisson & ps, const FieldsT<T> & f,
                              const double * tab_y, const double * tab_z, const double * base,
                              const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
-  if (g.nz >= 16 && TC_FFTZ_EPT == 16) launch_poisson_t<EPTY, 16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else if (g.nz >= 8) launch_poisson_t<EPTY, 8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else launch_poisson_t<EPTY, 4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  if (g.nz >= 16 && TC_FFTZ_EPT == 16)
+    launch_poisson_t<EPTY, 16, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.nz >= 8) launch_poisson_t<EPTY, 8, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else launch_poisson_t<EPTY, 4, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
 }
 
-void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const Fields & f,
+template <class T, class Z>
+static void launch_poisson_s(const Geo & g, const Coefs & cf, const Poisson & ps, const FieldsT<T> & f,
+                             const double * tab_y, const double * tab_z, const double * base,
+                             const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
+  if (g.ny >= 16 && TC_FFTY_EPT == 16)
+    launch_poisson_z<16, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else if (g.ny >= 8) launch_poisson_z<8, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else launch_poisson_z<4, T, Z>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+}
+
+// storage: fields and spectra both double, or both float (FP32-storage mode)
+void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const FieldBufs & f,
                     const double * tab_y, const double * tab_z, const double * base,
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
-  if (g.ny >= 16 && TC_FFTY_EPT == 16) launch_poisson_z<16>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else if (g.ny >= 8) launch_poisson_z<8>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
-  else launch_poisson_z<4>(g, cf, ps, f, tab_y, tab_z, base, dtp, rkstep, st, pm);
+  if (f.bytes == 4)
+    launch_poisson_s<float, float2>(g, cf, ps, f.as<float>(), tab_y, tab_z, base, dtp, rkstep, st, pm);
+  else
+    launch_poisson_s<double, double2>(g, cf, ps, f.as<double>(), tab_y, tab_z, base, dtp, rkstep, st, pm);
 }
 
 template <typename K>
@@ -651,20 +676,26 @@ static void allow_dyn_smem(K kernel) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
 }
 
-void poisson_smem_limits() {
+template <class T, class Z>
+static void poisson_smem_limits_s() {
   // up to 256 threads x 16 elements of 16 bytes, padded: < 74 KB of dynamic shared memory
-  allow_dyn_smem(div_ffty_kernel<16>);
-  allow_dyn_smem(div_ffty_kernel<8>);
-  allow_dyn_smem(div_ffty_kernel<4>);
-  allow_dyn_smem(iffty_kernel<16>);
-  allow_dyn_smem(iffty_kernel<8>);
-  allow_dyn_smem(iffty_kernel<4>);
-  allow_dyn_smem(fftz_kernel<16, -1>);
-  allow_dyn_smem(fftz_kernel<16, +1>);
-  allow_dyn_smem(fftz_kernel<8, -1>);
-  allow_dyn_smem(fftz_kernel<8, +1>);
-  allow_dyn_smem(fftz_kernel<4, -1>);
-  allow_dyn_smem(fftz_kernel<4, +1>);
+  allow_dyn_smem(div_ffty_kernel<16, T, Z>);
+  allow_dyn_smem(div_ffty_kernel<8, T, Z>);
+  allow_dyn_smem(div_ffty_kernel<4, T, Z>);
+  allow_dyn_smem(iffty_kernel<16, Z>);
+  allow_dyn_smem(iffty_kernel<8, Z>);
+  allow_dyn_smem(iffty_kernel<4, Z>);
+  allow_dyn_smem(fftz_kernel<16, -1, Z>);
+  allow_dyn_smem(fftz_kernel<16, +1, Z>);
+  allow_dyn_smem(fftz_kernel<8, -1, Z>);
+  allow_dyn_smem(fftz_kernel<8, +1, Z>);
+  allow_dyn_smem(fftz_kernel<4, -1, Z>);
+  allow_dyn_smem(fftz_kernel<4, +1, Z>);
+}
+
+void poisson_smem_limits() {
+  poisson_smem_limits_s<double, double2>();
+  poisson_smem_limits_s<float, float2>();
 }
 
 }  // namespace tcgpu

@@ -57,33 +57,34 @@ __global__ void xfactor_kernel(XFactors xf, const double * __restrict__ dtp, dou
 }
 
 // out = in + delta for every cell, walls and images (after the y / z solves)
+template <class T>
 __global__ void __launch_bounds__(256)
-apply_kernel(Geo g, Bc bc, Fields in, Fields out, DeltaSet ds) {
+apply_kernel(Geo g, Bc bc, FieldsT<T> in, FieldsT<T> out, DeltaSet ds) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int k = blockIdx.z + 1;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   if (i > nx || j > ny) return;
   const size_t qc = pidx(nx, ny, i - 1, j, k);
-  const double vx = (i >= 2) ? in.ux[fidx(g, i, j, k)] + ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] : 0.;
-  const double vy = in.uy[cidx(g, i, j, k)] + ds.d[VUY][qc];
-  const double vz = in.uz[cidx(g, i, j, k)] + ds.d[VUZ][qc];
-  const double vt = in.t[cidx(g, i, j, k)] + ds.d[VT][qc];
+  const double vx = (i >= 2) ? (double)in.ux[sidx_f<T>(g, i, j, k)] + ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] : 0.;
+  const double vy = (double)in.uy[sidx_c<T>(g, i, j, k)] + ds.d[VUY][qc];
+  const double vz = (double)in.uz[sidx_c<T>(g, i, j, k)] + ds.d[VUZ][qc];
+  const double vt = (double)in.t[sidx_c<T>(g, i, j, k)] + ds.d[VT][qc];
   auto put = [&](int jj, int kk) {
-    out.ux[fidx(g, i, jj, kk)] = vx;
-    out.uy[cidx(g, i, jj, kk)] = vy;
-    out.uz[cidx(g, i, jj, kk)] = vz;
-    out.t[cidx(g, i, jj, kk)] = vt;
+    out.ux[sidx_f<T>(g, i, jj, kk)] = (T)(vx);
+    out.uy[sidx_c<T>(g, i, jj, kk)] = (T)(vy);
+    out.uz[sidx_c<T>(g, i, jj, kk)] = (T)(vz);
+    out.t[sidx_c<T>(g, i, jj, kk)] = (T)(vt);
     if (i == 1) {
-      out.uy[cidx(g, 0, jj, kk)] = bc.uy_xm;
-      out.uz[cidx(g, 0, jj, kk)] = 0.;
-      out.t[cidx(g, 0, jj, kk)] = bc.t_xm;
+      out.uy[sidx_c<T>(g, 0, jj, kk)] = (T)(bc.uy_xm);
+      out.uz[sidx_c<T>(g, 0, jj, kk)] = (T)(0.);
+      out.t[sidx_c<T>(g, 0, jj, kk)] = (T)(bc.t_xm);
     }
     if (i == nx) {
-      out.ux[fidx(g, nx + 1, jj, kk)] = 0.;
-      out.uy[cidx(g, nx + 1, jj, kk)] = bc.uy_xp;
-      out.uz[cidx(g, nx + 1, jj, kk)] = 0.;
-      out.t[cidx(g, nx + 1, jj, kk)] = bc.t_xp;
+      out.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)(0.);
+      out.uy[sidx_c<T>(g, nx + 1, jj, kk)] = (T)(bc.uy_xp);
+      out.uz[sidx_c<T>(g, nx + 1, jj, kk)] = (T)(0.);
+      out.t[sidx_c<T>(g, nx + 1, jj, kk)] = (T)(bc.t_xp);
     }
   };
   put(j, k);
@@ -241,11 +242,12 @@ void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double 
   xfactor_kernel<<<1, 32, 0, st>>>(xf, dtp, nu, kappa);
 }
 
-void launch_apply(const Geo & g, const Bc & bc, const Fields & in, const Fields & out, const DeltaSet & ds,
+void launch_apply(const Geo & g, const Bc & bc, const FieldBufs & in, const FieldBufs & out, const DeltaSet & ds,
                   cudaStream_t st) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
-  apply_kernel<<<grid, block, 0, st>>>(g, bc, in, out, ds);
+  if (in.bytes == 4) apply_kernel<float><<<grid, block, 0, st>>>(g, bc, in.as<float>(), out.as<float>(), ds);
+  else apply_kernel<double><<<grid, block, 0, st>>>(g, bc, in.as<double>(), out.as<double>(), ds);
 }
 
 void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st) {

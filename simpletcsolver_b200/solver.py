@@ -40,7 +40,9 @@ class Solver:
     # ---------------------------------------------------------------- set-up
     @classmethod
     def from_ic(cls, dirname: str, case: Case | None = None, Re: float | None = None, Pr: float | None = None,
-                params: abi.ParamsT | None = None, lib=None, coherence: int = 0) -> "Solver":
+                params: abi.ParamsT | None = None, lib=None, coherence: int = 0, storage: int = 8) -> "Solver":
+        """storage: bytes per stored value of ux, uy, uz, t, the source terms and
+        the spectra on the device (8, or 4 for the FP32-storage mode)."""
         lib = lib or abi.load()
         env = {}
         if case is not None:
@@ -60,9 +62,17 @@ class Solver:
         if lib.fluid_init(dirname.encode(), C.byref(domain), C.byref(fluid)) != 0:
             raise SolverError(f"fluid_init failed: {abi.last_error(lib)}")
         s = cls(lib, domain, fluid)
-        if coherence:
-            s.set_coherence(coherence)
+        previous = lib.tcgpu_get_storage(None)
+        s._check(lib.tcgpu_set_storage(storage), "set_storage")
+        try:
+            s.set_coherence(coherence)   # creates the device context with that storage
+        finally:
+            lib.tcgpu_set_storage(previous)
         return s
+
+    @property
+    def storage(self) -> int:
+        return self.lib.tcgpu_get_storage(C.byref(self.fluid))
 
     def _check(self, rc: int, what: str):
         if rc != 0:
