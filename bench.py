@@ -37,6 +37,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -59,6 +61,19 @@ BYTES_PER_CELL = {
     "CORRECT": 9 * 8,                          # psi, ux, uy, uz, p read; ux, uy, uz, p written
 }
 MODEL_BYTES_PER_CELL_STEP = 912
+# FP32-storage mode: ux, uy, uz, t, the source terms and the spectra in 4 bytes,
+# p and psi in 8
+BYTES_PER_CELL_FP32 = {
+    "DTMIN": 3 * 4,
+    # predict: ux, uy, uz, t (4 B) and p (8 B) read, 4 new sources + 4 fields
+    # written (56 B); substeps 2 and 3 also read the old sources (72 B)
+    "PREDICT": (56.0 + 72.0 + 72.0) / 3.0,
+    "DIV_FFTY": 3 * 4 + 4,
+    "FFTZ_FWD": 8, "TDM": 8, "FFTZ_INV": 8,
+    "IFFTY": 4 + 8,
+    "CORRECT": 8 + 12 + 8 + 12 + 8,            # psi, ux, uy, uz, p read; ux, uy, uz, p written
+}
+MODEL_BYTES_PER_CELL_STEP_FP32 = 500           # 200 (predict) + 3 x 100 (Poisson + correction)
 
 
 def parse_args(argv=None):
@@ -70,6 +85,9 @@ def parse_args(argv=None):
     ap.add_argument("--grid", type=str, default="256x1024x512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage arm")
+    ap.add_argument("--accuracy-steps", type=int, default=200,
+                    help="steps of the FP32-storage vs FP64 accuracy runs (0: skip)")
     return ap.parse_args(argv)
 
 
@@ -221,6 +239,46 @@ def parse_grid(s):
     return nx, ny, nz
 
 
+def run_timed(lib, s, nsteps, instrument):
+    """nsteps steps through tcgpu_run_timed in chunks of 64: device ms (CUDA
+    events on the library's stream) and, with instrument, per-kernel ms and
+    launch counts."""
+    import ctypes as C
+    from simpletcsolver_b200 import abi
+    el = C.c_float(0.)
+    kms = (C.c_double * 12)()
+    kl = (C.c_int * 12)()
+    dts = (C.c_double * max(nsteps, 1))()
+    done = 0
+    total_ms = 0.0
+    ktot = [0.0] * 12
+    ltot = [0] * 12
+    while done < nsteps:
+        n = min(64, nsteps - done)
+        rc = lib.tcgpu_run_timed(C.byref(s.domain), C.byref(s.fluid), n, instrument, dts, C.byref(el), kms, kl)
+        if rc != 0:
+            raise RuntimeError(abi.last_error(lib))
+        total_ms += el.value
+        ktot = [a + b for a, b in zip(ktot, kms)]
+        ltot = [a + b for a, b in zip(ltot, kl)]
+        done += n
+    return total_ms, ktot, ltot
+
+
+def kernel_table(kms_total, kdev, klaunch, ncell, bytes_map, peak):
+    per_kernel = {}
+    for i, name in enumerate(KERNELS):
+        if klaunch[i] == 0:
+            continue
+        avg = kdev[i] / klaunch[i]
+        entry = {"launches": klaunch[i], "ms_total": kdev[i], "share": kdev[i] / kms_total, "ms_per_launch": avg}
+        if name in bytes_map:
+            entry["gbs"] = bytes_map[name] * ncell / (avg / 1e3) / 1e9
+            entry["frac"] = entry["gbs"] / peak
+        per_kernel[name] = entry
+    return per_kernel
+
+
 def gpu_arm(args, rank, world, local):
     import ctypes as C
     from simpletcsolver_b200 import abi, build, ic
@@ -229,6 +287,8 @@ def gpu_arm(args, rank, world, local):
     lib = abi.load()
     if lib.tcgpu_set_device(local) != 0:
         raise RuntimeError(abi.last_error(lib))
+    lib.tcgpu_run_timed.argtypes = [C.POINTER(abi.DomainT), C.POINTER(abi.FluidT), C.c_int, C.c_int,
+                                    abi.c_double_p, C.POINTER(C.c_float), C.c_double * 12, C.c_int * 12]
     nx, ny, nz = parse_grid(args.grid)
     case = ic.taylor_couette(nx, ny, nz, 1.0e4)
     td = tempfile.mkdtemp(prefix="tcbench")
@@ -240,34 +300,12 @@ def gpu_arm(args, rank, world, local):
     s.run(W)                                     # warm-up, graph capture
     ncell = case.ncells
 
-    def timed(nsteps, instrument):
-        el = C.c_float(0.)
-        kms = (C.c_double * 12)()
-        kl = (C.c_int * 12)()
-        dts = (C.c_double * max(nsteps, 1))()
-        done = 0
-        total_ms = 0.0
-        ktot = [0.0] * 12
-        ltot = [0] * 12
-        while done < nsteps:
-            n = min(64, nsteps - done)
-            rc = lib.tcgpu_run_timed(C.byref(s.domain), C.byref(s.fluid), n, instrument, dts, C.byref(el), kms, kl)
-            if rc != 0:
-                raise RuntimeError(abi.last_error(lib))
-            total_ms += el.value
-            ktot = [a + b for a, b in zip(ktot, kms)]
-            ltot = [a + b for a, b in zip(ltot, kl)]
-            done += n
-        return total_ms, ktot, ltot
-
-    lib.tcgpu_run_timed.argtypes = [C.POINTER(abi.DomainT), C.POINTER(abi.FluidT), C.c_int, C.c_int,
-                                    abi.c_double_p, C.POINTER(C.c_float), C.c_double * 12, C.c_int * 12]
     import torch
     barrier(world)
     if torch.cuda.is_available():
         torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        ms, _, launches = timed(K, 0)
+        ms, _, launches = run_timed(lib, s, K, 0)
     barrier(world)
     if torch.cuda.is_available():
         torch.cuda.synchronize()
@@ -275,32 +313,19 @@ def gpu_arm(args, rank, world, local):
     value = units / elapsed / 1e6
 
     # per-kernel accounting: events around every launch of K instrumented steps
-    kms_total, kdev, klaunch = timed(K, 1)
-    per_kernel = {}
-    for i, name in enumerate(KERNELS):
-        if klaunch[i] == 0:
-            continue
-        avg = kdev[i] / klaunch[i]
-        entry = {"launches": klaunch[i], "ms_total": kdev[i], "share": kdev[i] / kms_total, "ms_per_launch": avg}
-        if name in BYTES_PER_CELL:
-            gbs = BYTES_PER_CELL[name] * ncell / (avg / 1e3) / 1e9
-            entry["gbs"] = gbs
-        per_kernel[name] = entry
-    dom = max((k for k in per_kernel if k in BYTES_PER_CELL), key=lambda k: per_kernel[k]["ms_total"])
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    kms_total, kdev, klaunch = run_timed(lib, s, K, 1)
+    per_kernel = kernel_table(kms_total, kdev, klaunch, ncell, BYTES_PER_CELL, peak)
+    dom = max((k for k in per_kernel if k in BYTES_PER_CELL), key=lambda k: per_kernel[k]["ms_total"])
     achieved = per_kernel[dom]["gbs"]
     traffic = measured_traffic(dom, ncell)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "algorithmic_bytes_per_launch": BYTES_PER_CELL[dom] * ncell,
-                "peak_source": "measured" if "hbm_gbs" in peaks and os.path.exists(
-                    os.path.join(ROOT, "MEASURED_PEAKS.json")) else "fallback"}
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
     step_model = MODEL_BYTES_PER_CELL_STEP * ncell / (ms / K / 1e3) / 1e9
-    for k in per_kernel:
-        if "gbs" in per_kernel[k]:
-            per_kernel[k]["frac"] = per_kernel[k]["gbs"] / peak
 
     e2e = None
     if not args.no_e2e:
@@ -315,6 +340,11 @@ def gpu_arm(args, rank, world, local):
                "d2h_bytes_per_step": (nf + 5 * nc) * 8, "timing": "host wall clock around synchronous integrate()"}
     s.release()
     gpu_launches = sum(launches)
+
+    fp32 = None
+    if not args.no_fp32:
+        fp32 = fp32_storage_arm(args, lib, d0, case, world, peak, value)
+        gpu_launches += fp32.pop("_launches")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -331,6 +361,7 @@ def gpu_arm(args, rank, world, local):
             "step_model": {"bytes_per_cell_step": MODEL_BYTES_PER_CELL_STEP, "achieved_gbs": step_model,
                            "frac": step_model / peak},
             "kernels": per_kernel,
+            "fp32_storage": fp32,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk.summary(),
@@ -338,6 +369,75 @@ def gpu_arm(args, rank, world, local):
         }
         print(json.dumps(out))
     return 0
+
+
+def fp32_storage_arm(args, lib, d0, case, world, peak, value64):
+    """The FP32-storage form on the same workload: throughput (same timing as
+    the FP64 arm) and, over --accuracy-steps steps from the same initial field,
+    its error against the FP64 path: relative L2 of every field, max
+    divergence, inner-wall torque (the momentum energy injection; the outer
+    wall is at rest) and Nusselt number (torque / its laminar value)."""
+    from simpletcsolver_b200 import abi
+    from simpletcsolver_b200.solver import Solver
+    K, W = args.steps, args.warmup
+    ncell = case.ncells
+    s = Solver.from_ic(d0, case=case, lib=lib, storage=4)
+    s.push()
+    s.run(W)
+    ms, _, launches = run_timed(lib, s, K, 0)
+    elapsed, units = aggregate(ms / 1e3, ncell * K, world)
+    value = units / elapsed / 1e6
+    kms_total, kdev, klaunch = run_timed(lib, s, K, 1)
+    per_kernel = kernel_table(kms_total, kdev, klaunch, ncell, BYTES_PER_CELL_FP32, peak)
+    s.release()
+    step_model = MODEL_BYTES_PER_CELL_STEP_FP32 * ncell / (ms / K / 1e3) / 1e9
+    out = {"value": value, "unit": UNIT, "ms_per_step": elapsed * 1e3 / K, "steps": K,
+           "dtype": "f32 storage (ux, uy, uz, t, sources, spectra); p, psi and arithmetic f64",
+           "speedup_vs_fp64": value / value64,
+           "step_model": {"bytes_per_cell_step": MODEL_BYTES_PER_CELL_STEP_FP32, "achieved_gbs": step_model,
+                          "frac": step_model / peak},
+           "kernels": per_kernel, "_launches": sum(launches)}
+    n = args.accuracy_steps
+    if n > 0:
+        runs = {}
+        for storage in (8, 4):
+            s = Solver.from_ic(d0, case=case, lib=lib, storage=storage)
+            try:
+                s.push()
+                dts = s.run(n)
+                s.pull(abi.FIELDS)
+                runs[storage] = {f: s.field(f)[1:-1, 1:-1].copy() for f in ("ux", "uy", "uz", "t", "p")}
+                runs[storage]["diag"] = s.diagnostics()
+                runs[storage]["time"] = float(np.sum(dts))
+            finally:
+                s.release()
+        a, b = runs[8], runs[4]
+        l2 = {}
+        for f in ("ux", "uy", "uz", "t", "p"):
+            x, y = b[f], a[f]
+            if f == "p":
+                x, y = x - x.mean(), y - y.mean()
+            l2[f] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+        tq64, tq32 = a["diag"]["injection_u"], b["diag"]["injection_u"]
+        lam = laminar_injection(case)
+        out["accuracy"] = {
+            "steps": n, "rel_l2": l2,
+            "divmax": {"fp64": a["diag"]["divmax"], "fp32_storage": b["diag"]["divmax"]},
+            "torque": {"fp64": tq64, "fp32_storage": tq32, "rel_err": abs(tq32 - tq64) / abs(tq64)},
+            "nusselt": {"fp64": tq64 / lam, "fp32_storage": tq32 / lam,
+                        "rel_err": abs(tq32 - tq64) / abs(tq64)},
+            "sim_time": {"fp64": a["time"], "fp32_storage": b["time"]},
+        }
+    return out
+
+
+def laminar_injection(case):
+    """Energy injection of circular Couette flow in the same box:
+    2/Re ri^2 ro^2 / (ro^2 - ri^2) (ui/ri)^2 ly lz, the normalisation of the
+    reference's Nusselt number (balance_main.py:14-21); ri = 1, ui = uy_xm."""
+    ri, ro = 1.0, 1.0 + case.lx
+    return (2.0 / case.Re * ri ** 2 * ro ** 2 / (ro ** 2 - ri ** 2) * (case.uy_xm / ri) ** 2
+            * case.ly * case.lz)
 
 
 def measured_traffic(kernel: str, ncell: int):

@@ -158,3 +158,17 @@ def test_domain_checks_single_rank_only(lib, tmp_path):
     dt = C.c_double()
     assert lib.decide_dt(C.byref(d), C.byref(fl), C.byref(dt)) != 0
     assert "single rank" in abi.last_error(lib)
+
+
+def test_storage_selection_is_validated(lib):
+    """tcgpu_set_storage takes 8 or 4 bytes per stored value and sets the
+    storage of contexts created afterwards (no device needed)."""
+    assert lib.tcgpu_get_storage(None) == 8
+    assert lib.tcgpu_set_storage(3) != 0
+    assert "8 or 4" in abi.last_error(lib)
+    try:
+        assert lib.tcgpu_set_storage(4) == 0
+        assert lib.tcgpu_get_storage(None) == 4
+    finally:
+        assert lib.tcgpu_set_storage(8) == 0
+    assert lib.tcgpu_get_storage(None) == 8
