@@ -278,6 +278,35 @@ int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, bool is_comple
 /* free the device state that belongs to this fluid_t */
 int tcgpu_release(fluid_t * fluid);
 
+/* ---- learned closure: network kernels --------------------------------------
+ * No counterpart in the reference. Device pointers, asynchronous on the given
+ * CUDA stream (NULL: the legacy default stream). Activations are channels-last
+ * BF16 over the interior cells of a grid (nx, ny, nz), act[((k ny + j) nx + i)
+ * C + c], C in {16, 32}; x is zero-padded, y and z periodic. All buffers
+ * 16-byte aligned; nx a multiple of 8, ny of 16.
+ *
+ * Weights: FP32 master copy w[t][co][ci] (t = 9 (dz+1) + 3 (dy+1) + (dx+1),
+ * real channel counts) packed into BF16 images for the forward convolution
+ * (fwd, 27 cinp coutp values) and, if bwd != NULL, for the input-gradient
+ * convolution (taps mirrored, channels swapped). */
+int tcgpu_nn_pack_weights(const float * w, int cin, int cout, int cinp, int coutp, void * fwd, void * bwd,
+                          void * stream);
+/* 3x3x3 convolution on the tensor cores (BF16 operands, FP32 accumulation).
+ * mode 0: out = GELU(conv(in) + bias) (BF16, cout channels), pre = conv(in) +
+ *         bias (BF16, optional, kept for the backward pass);
+ * mode 1: outf[cell][c] = conv(in) + bias for c < nout (FP32);
+ * mode 2: out = conv(in) * GELU'(zsave) (input gradient through the layer
+ *         below; in = the gradient of this layer's pre-activation, wpacked =
+ *         the bwd image, cin/cout = this layer's cout/cin). */
+int tcgpu_nn_conv3(int mode, int cin, int cout, int nx, int ny, int nz, const void * in, const void * wpacked,
+                   const float * bias, const void * zsave, void * out, void * pre, float * outf, int nout,
+                   void * stream);
+/* error bits raised by the network kernels since the last clear (4: a wait
+ * gave up); synchronises the device; -1 on a CUDA error */
+int tcgpu_nn_status(int clear);
+/* last error message of the network entry points of this thread */
+const char * tcgpu_nn_last_error(void);
+
 /* last error message of this thread ("" when none) */
 const char * tcgpu_last_error(void);
 

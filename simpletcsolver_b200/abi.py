@@ -95,6 +95,12 @@ _EXT_SIGS = {
     "tcgpu_set_storage": (C.c_int, [C.c_int]),
     "tcgpu_get_storage": (C.c_int, [C.POINTER(FluidT)]),
     "tcgpu_last_error": (C.c_char_p, []),
+    "tcgpu_nn_pack_weights": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "tcgpu_nn_conv3": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tcgpu_nn_status": (C.c_int, [C.c_int]),
+    "tcgpu_nn_last_error": (C.c_char_p, []),
 }
 
 
