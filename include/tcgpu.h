@@ -301,6 +301,24 @@ int tcgpu_nn_pack_weights(const float * w, int cin, int cout, int cinp, int cout
 int tcgpu_nn_conv3(int mode, int cin, int cout, int nx, int ny, int nz, const void * in, const void * wpacked,
                    const float * bias, const void * zsave, void * out, void * pre, float * outf, int nout,
                    void * stream);
+/* weight gradient of a convolution: dw[t][co][ci] (real counts cin x cout,
+ * FP32) = sum over cells of x[cell + tap t][ci] dy[cell][co], db[co] = sum of
+ * dy[cell][co]; beta 0 overwrites dw/db, 1 accumulates. x has cinp channels,
+ * dy coutp (padded counts, 16 or 32). workspace: device scratch of at least
+ * tcgpu_nn_wgrad_workspace() bytes. */
+size_t tcgpu_nn_wgrad_workspace(int nx, int ny, int nz, int coutp);
+int tcgpu_nn_conv3_wgrad(int cinp, int coutp, int cin, int cout, int nx, int ny, int nz, const void * x,
+                         const void * dy, float * dw, float * db, float beta, void * workspace, size_t ws_bytes,
+                         void * stream);
+/* mean squared error of f against t (FP32 [cell][nc], optional per-cell
+ * weight w): *loss += mean w (f - t)^2; grad (BF16 [cell][cp]) = its
+ * gradient with respect to f, zero in channels nc .. cp-1 */
+int tcgpu_nn_mse(const float * f, const float * t, const float * w, size_t ncell, int nc, int cp, void * grad,
+                 double * loss, void * stream);
+/* one Adam step on n FP32 parameters p with gradients g and moments m, v;
+ * step = 1, 2, ... (bias correction) */
+int tcgpu_nn_adam(float * p, const float * g, float * m, float * v, size_t n, float lr, float beta1, float beta2,
+                  float eps, int step, void * stream);
 /* error bits raised by the network kernels since the last clear (4: a wait
  * gave up); synchronises the device; -1 on a CUDA error */
 int tcgpu_nn_status(int clear);

@@ -99,6 +99,14 @@ _EXT_SIGS = {
                                         C.c_void_p]),
     "tcgpu_nn_conv3": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "tcgpu_nn_wgrad_workspace": (C.c_size_t, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "tcgpu_nn_conv3_wgrad": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_size_t,
+                                       C.c_void_p]),
+    "tcgpu_nn_mse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
+    "tcgpu_nn_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float, C.c_float,
+                                C.c_float, C.c_float, C.c_int, C.c_void_p]),
     "tcgpu_nn_status": (C.c_int, [C.c_int]),
     "tcgpu_nn_last_error": (C.c_char_p, []),
 }

@@ -308,6 +308,263 @@ __global__ void __launch_bounds__(NN_THREADS) conv3_kernel(ConvArgs A) {
   if (warp == 0) tmem_free(tmem, 32);
 }
 
+// ---- convolution: weight gradient -----------------------------------------
+// dW[t][co][ci] = sum over cells of X[cell + tap t][ci] dY[cell][co] as
+// D (M = 128, N = COUT) += A (M x K = 16 cells) B^T, both operands MN-major:
+// A is the input halo (a 16-byte unit = 8 channels of one cell; channel chunks
+// at CHB continue into the next halo row, so rows m = (y shift s, ci) cover
+// NSH = 128 / CIN shifts s = dy + 1 of one (dz, dx) pair); B is the gradient
+// tile of the plane, units [y][co chunk][x]. Nine accumulators (dz, dx) of
+// COUT columns each live in tensor memory for the whole life of the CTA,
+// which loops over (column tile, z chunk) work items; the CTA writes its raw
+// partial sums, reduced afterwards by wgrad_reduce_kernel.
+template <int CIN, int COUT>
+struct WgradLayout {
+  static constexpr int NSH = 128 / CIN;                  // y shifts per accumulator
+  static constexpr int HYW = TY + NSH - 1;               // halo rows y0 - 1 .. y0 + TY + NSH - 3
+  static constexpr int CHB = HX * 16;
+  static constexpr int ROWB = (CIN / 8) * CHB;
+  static constexpr int SLOTB = HYW * ROWB;
+  static constexpr int GB = TY * (COUT / 8) * TX * 16;   // gradient tile of one plane
+  static constexpr int GOFF = NSLOT_NN * SLOTB;          // two gradient slots after the halo ring
+  static constexpr int BAR = GOFF + 2 * GB;
+  static constexpr int USED = BAR + 16;
+  static constexpr int TCOLS = 9 * COUT > 256 ? 512 : 256;
+  // one CTA per SM, so that its tensor-memory allocation never waits on
+  // another CTA's: ask for more than half of the shared memory
+  static constexpr int BYTES = USED < 120 * 1024 ? 120 * 1024 : USED;
+};
+
+struct WgradArgs {
+  int nx, ny, nz, zc, nitems;
+  const __nv_bfloat16 * x;    // [cell][CIN] layer input
+  const __nv_bfloat16 * dy;   // [cell][COUT] gradient of the layer's pre-activation
+  float * part;               // [gridDim.x][9][128][COUT] raw sums, then [gridDim.x][COUT] bias sums
+  unsigned * status;
+};
+
+template <int CIN>
+__device__ __forceinline__ void load_halo_w(char * slot, const __nv_bfloat16 * in, int nx, int ny, int x0, int y0,
+                                            int kp, int hyw) {
+  constexpr int CC = CIN / 8;
+  for (int u = threadIdx.x; u < hyw * HX * CC; u += NN_THREADS) {
+    const int cc = u % CC, xh = (u / CC) % HX, yh = u / (CC * HX);
+    const int i = x0 - 1 + xh;
+    int j = (y0 - 1 + yh) % ny;
+    if (j < 0) j += ny;
+    const bool valid = i >= 0 && i < nx;
+    const __nv_bfloat16 * src = in + ((size_t)((size_t)kp * ny + j) * nx + (valid ? i : 0)) * CIN + cc * 8;
+    cp16(slot + ((yh * CC + cc) * HX + xh) * 16, src, valid);
+  }
+}
+template <int COUT>
+__device__ __forceinline__ void load_grad_tile(char * slot, const __nv_bfloat16 * dy, int nx, int ny, int x0, int y0,
+                                               int z) {
+  constexpr int CC = COUT / 8;
+  for (int u = threadIdx.x; u < TY * TX * CC; u += NN_THREADS) {
+    const int cc = u % CC, x = (u / CC) % TX, y = u / (CC * TX);
+    const __nv_bfloat16 * src = dy + ((size_t)((size_t)z * ny + y0 + y) * nx + x0 + x) * COUT + cc * 8;
+    cp16(slot + ((y * CC + cc) * TX + x) * 16, src, true);
+  }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(NN_THREADS, 1) conv3_wgrad_kernel(WgradArgs A) {
+  using L = WgradLayout<CIN, COUT>;
+  extern __shared__ __align__(128) char smw[];
+  char * halo = smw;
+  char * gsl = smw + L::GOFF;
+  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smw + L::BAR);
+  unsigned * tslot = reinterpret_cast<unsigned *>(smw + L::BAR + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nbx = A.nx / TX, ncol = nbx * (A.ny / TY);
+
+  if (warp == 0) tmem_alloc(tslot, L::TCOLS);
+  if (tid == 0) {
+    nn_mbar_init(bar, 1);
+    fence_barrier_init();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = *tslot;
+  constexpr uint32_t IDESC = instr_desc_bf16(128, COUT, 1, 1);
+  float bsum = 0.f;                 // bias gradient of channel tid (tid < COUT)
+  bool first = true;                // no accumulator written yet
+  unsigned phase = 0;
+  bool bad = false;
+
+  for (int item = blockIdx.x; item < A.nitems && !bad; item += gridDim.x) {
+    const int col = item % ncol, zch = item / ncol;
+    const int x0 = (col % nbx) * TX, y0 = (col / nbx) * TY;
+    const int z0 = zch * A.zc, z1 = min(z0 + A.zc, A.nz);
+    load_halo_w<CIN>(halo + 0 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, wrapi(z0 - 1, A.nz), L::HYW);
+    cp_commit();
+    load_halo_w<CIN>(halo + 1 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, z0, L::HYW);
+    load_grad_tile<COUT>(gsl + L::GB, A.dy, A.nx, A.ny, x0, y0, z0);   // plane z0 uses slot 1
+    cp_commit();
+    load_halo_w<CIN>(halo + 2 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, wrapi(z0 + 1, A.nz), L::HYW);
+    cp_commit();
+    for (int z = z0; z < z1; z++) {
+      const int r = z - z0 + 1;
+      if (z + 2 <= z1) load_halo_w<CIN>(halo + ((r + 2) % NSLOT_NN) * L::SLOTB, A.x, A.nx, A.ny, x0, y0,
+                                        wrapi(z + 2, A.nz), L::HYW);
+      if (z + 1 < z1) load_grad_tile<COUT>(gsl + ((r + 1) & 1) * L::GB, A.dy, A.nx, A.ny, x0, y0, z + 1);
+      cp_commit();
+      cp_wait<1>();
+      fence_proxy_async();
+      __syncthreads();
+      const char * g = gsl + (r & 1) * L::GB;
+      if (tid == 0) {
+        tc_fence_after();
+        const unsigned hb = su32(halo), gb = su32(g);
+#pragma unroll 1
+        for (int a = 0; a < 9; a++) {
+          const int dz = a / 3 - 1, dx = a % 3 - 1;
+          const unsigned a0 = hb + ((r + dz) % NSLOT_NN) * L::SLOTB + (1 + dx) * 16;
+#pragma unroll
+          for (int s = 0; s < TY / 2; s++) {
+            const uint64_t ad = smem_desc(a0 + 2 * s * L::ROWB, L::ROWB, L::CHB);
+            const uint64_t bd = smem_desc(gb + 2 * s * (COUT / 8) * TX * 16, (COUT / 8) * TX * 16, TX * 16);
+            mma_bf16(tmem + a * COUT, ad, bd, IDESC, !(first && s == 0));
+          }
+        }
+        mma_commit(bar);
+      }
+      if (tid < COUT) {   // bias gradient from the same tile
+        constexpr int CC = COUT / 8;
+        const __nv_bfloat16 * gv = reinterpret_cast<const __nv_bfloat16 *>(g);
+        float acc = 0.f;
+        for (int c = 0; c < TX * TY; c++) {
+          const int x = c % TX, y = c / TX;
+          acc += __bfloat162float(gv[((y * CC + tid / 8) * TX + x) * 8 + tid % 8]);
+        }
+        bsum += acc;
+      }
+      first = false;
+      const bool ok = nn_mbar_wait(bar, phase);
+      phase ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
+        bad = true;
+        break;
+      }
+      tc_fence_before();
+      __syncthreads();   // slots of plane z - 1 and of this gradient tile may be refilled
+    }
+    cp_wait<0>();
+    __syncthreads();
+  }
+  tc_fence_after();
+  // raw partial sums of this CTA: [a][m][co]
+  float * dst = A.part + (size_t)blockIdx.x * 9 * 128 * COUT;
+  const int m = warp * 32 + lane;
+  for (int a = 0; a < 9; a++) {
+#pragma unroll
+    for (int h = 0; h < COUT / 16; h++) {
+      float v[16];
+      tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + a * COUT + h * 16, v);
+#pragma unroll
+      for (int q = 0; q < 16; q++) dst[((size_t)a * 128 + m) * COUT + h * 16 + q] = first ? 0.f : v[q];
+    }
+  }
+  float * bdst = A.part + (size_t)gridDim.x * 9 * 128 * COUT + (size_t)blockIdx.x * COUT;
+  if (tid < COUT) bdst[tid] = bsum;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_free(tmem, L::TCOLS);
+}
+
+// Sum of the CTAs' raw partials into the master-layout gradients
+// dw[t][co][ci] (real channel counts) and db[co]; beta = 0 overwrites,
+// 1 accumulates.
+__global__ void wgrad_reduce_kernel(const float * __restrict__ part, int nblk, int cinp, int coutp, int cin, int cout,
+                                    float * __restrict__ dw, float * __restrict__ db, float beta) {
+  const int nw = 27 * cout * cin;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nw + cout; q += gridDim.x * blockDim.x) {
+    if (q < nw) {
+      const int ci = q % cin, co = (q / cin) % cout, t = q / (cin * cout);
+      const int dz = t / 9, dyi = (t / 3) % 3, dx = t % 3;   // dyi = dy + 1
+      const int a = dz * 3 + dx, m = (dyi * (cinp / 8) + ci / 8) * 8 + ci % 8;
+      float acc = 0.f;
+      for (int b = 0; b < nblk; b++) acc += part[(((size_t)b * 9 + a) * 128 + m) * coutp + co];
+      dw[q] = beta * dw[q] + acc;
+    } else {
+      const int co = q - nw;
+      float acc = 0.f;
+      const float * bp = part + (size_t)nblk * 9 * 128 * coutp;
+      for (int b = 0; b < nblk; b++) acc += bp[(size_t)b * coutp + co];
+      db[co] = beta * db[co] + acc;
+    }
+  }
+}
+
+template <int CIN, int COUT>
+int launch_wgrad(WgradArgs a, int nblk, cudaStream_t st) {
+  using L = WgradLayout<CIN, COUT>;
+  if (cudaFuncSetAttribute(conv3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES) !=
+      cudaSuccess)
+    return 1;
+  conv3_wgrad_kernel<CIN, COUT><<<nblk, NN_THREADS, L::BYTES, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// ---- loss, optimiser -------------------------------------------------------
+// Mean squared error of the predicted forcing against the target over n
+// cells x nc channels (FP32, [cell][nc]), optional per-cell weight (NULL: 1):
+// loss += sum w (f - t)^2 / (n nc) (double accumulator) and the gradient with
+// respect to f, 2 w (f - t) / (n nc), as BF16 [cell][cp] (channels >= nc zero).
+__global__ void mse_kernel(const float * __restrict__ f, const float * __restrict__ t, const float * __restrict__ w,
+                           size_t n, int nc, int cp, float scale, __nv_bfloat16 * __restrict__ g,
+                           double * __restrict__ loss) {
+  double acc = 0.;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const float wc = w ? w[q] : 1.f;
+    alignas(16) __nv_bfloat16 o[16];
+    for (int c = 0; c < 16; c++) o[c] = __float2bfloat16_rn(0.f);
+    for (int c = 0; c < nc; c++) {
+      const float d = f[q * nc + c] - t[q * nc + c];
+      acc += (double)(wc * d * d);
+      o[c] = __float2bfloat16_rn(2.f * wc * d * scale);
+    }
+    for (int c0 = 0; c0 < cp; c0 += 16) {
+      uint4 * dp = reinterpret_cast<uint4 *>(g + q * cp + c0);
+      if (c0 == 0) {
+        dp[0] = reinterpret_cast<const uint4 *>(o)[0];
+        dp[1] = reinterpret_cast<const uint4 *>(o)[1];
+      } else {
+        dp[0] = make_uint4(0, 0, 0, 0);
+        dp[1] = make_uint4(0, 0, 0, 0);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) s += red[i];
+    atomicAdd(loss, s * (double)scale);
+  }
+}
+
+// Adam (Kingma and Ba 2015) on FP32 master parameters; step >= 1 is the
+// update count, bias corrections 1 - beta^step.
+__global__ void adam_kernel(float * __restrict__ p, const float * __restrict__ g, float * __restrict__ m,
+                            float * __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const float gq = g[q];
+    const float mq = b1 * m[q] + (1.f - b1) * gq;
+    const float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+    m[q] = mq;
+    v[q] = vq;
+    p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+  }
+}
+
 // ---- weights ---------------------------------------------------------------
 // Master weights (FP32) w[t][co][ci], t = 9 (dz+1) + 3 (dy+1) + (dx+1), real
 // channel counts cin x cout, into the BF16 shared-memory images of the forward
@@ -344,6 +601,15 @@ int dispatch_conv3(int cin, int cout, const ConvArgs & a, cudaStream_t st) {
   if (cin == 32 && cout == 16) return launch_conv3<32, 16, EPI>(a, st);
   if (cin == 16 && cout == 16) return launch_conv3<16, 16, EPI>(a, st);
   return 1;
+}
+
+// weight gradient: (column tile, z chunk) work items and the CTAs over them
+void wgrad_split(int nx, int ny, int nz, int & zc, int & nitems, int & nblk) {
+  const int ncol = (nx / TX) * (ny / TY);
+  zc = nz;
+  while (zc > 4 && (long)ncol * ((nz + zc - 1) / zc) < 148L * 2) zc = (zc + 1) / 2;
+  nitems = ncol * ((nz + zc - 1) / zc);
+  nblk = nitems < 148 ? nitems : 148;
 }
 
 // z planes per CTA: about four CTAs' worth of work per SM pair
@@ -425,6 +691,62 @@ int tcgpu_nn_conv3(int mode, int cin, int cout, int nx, int ny, int nz, const vo
       return nn_fail("nn_conv3: mode 0 (forward, GELU), 1 (forward, linear) or 2 (input gradient)");
   }
   return rc ? nn_fail("nn_conv3: unsupported channel counts or launch failure") : 0;
+}
+
+size_t tcgpu_nn_wgrad_workspace(int nx, int ny, int nz, int coutp) {
+  if (nx % TX || ny % TY || nx <= 0 || ny <= 0 || nz <= 0) return 0;
+  int zc, nitems, nblk;
+  wgrad_split(nx, ny, nz, zc, nitems, nblk);
+  return (size_t)nblk * (9 * 128 + 1) * coutp * sizeof(float);
+}
+
+int tcgpu_nn_conv3_wgrad(int cinp, int coutp, int cin, int cout, int nx, int ny, int nz, const void * x,
+                         const void * dy, float * dw, float * db, float beta, void * workspace, size_t ws_bytes,
+                         void * stream) {
+  if (nx % TX || ny % TY || nx <= 0 || ny <= 0 || nz <= 0)
+    return nn_fail("nn_conv3_wgrad: nx must be a multiple of 8 and ny of 16");
+  if (cin > cinp || cout > coutp || !x || !dy || !dw || !db || !aligned16(x) || !aligned16(dy))
+    return nn_fail("nn_conv3_wgrad: bad arguments");
+  if (!workspace || ws_bytes < tcgpu_nn_wgrad_workspace(nx, ny, nz, coutp))
+    return nn_fail("nn_conv3_wgrad: workspace smaller than tcgpu_nn_wgrad_workspace()");
+  WgradArgs a{};
+  a.nx = nx; a.ny = ny; a.nz = nz;
+  int nblk;
+  wgrad_split(nx, ny, nz, a.zc, a.nitems, nblk);
+  a.x = static_cast<const __nv_bfloat16 *>(x);
+  a.dy = static_cast<const __nv_bfloat16 *>(dy);
+  a.part = static_cast<float *>(workspace);
+  a.status = nn_status_ptr();
+  if (!a.status) return nn_fail("nn_conv3_wgrad: status word unavailable");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = 1;
+  if (cinp == 16 && coutp == 32) rc = launch_wgrad<16, 32>(a, nblk, st);
+  else if (cinp == 32 && coutp == 32) rc = launch_wgrad<32, 32>(a, nblk, st);
+  else if (cinp == 32 && coutp == 16) rc = launch_wgrad<32, 16>(a, nblk, st);
+  else if (cinp == 16 && coutp == 16) rc = launch_wgrad<16, 16>(a, nblk, st);
+  if (rc) return nn_fail("nn_conv3_wgrad: unsupported channel counts or launch failure");
+  const int nred = 27 * cout * cin + cout;
+  wgrad_reduce_kernel<<<(nred + 255) / 256, 256, 0, st>>>(a.part, nblk, cinp, coutp, cin, cout, dw, db, beta);
+  return cudaGetLastError() == cudaSuccess ? 0 : nn_fail("nn_conv3_wgrad: reduction launch failed");
+}
+
+int tcgpu_nn_mse(const float * f, const float * t, const float * w, size_t ncell, int nc, int cp, void * grad,
+                 double * loss, void * stream) {
+  if (!f || !t || !grad || !loss || nc < 1 || nc > 16 || cp % 16 || cp < 16 || !aligned16(grad))
+    return nn_fail("nn_mse: bad arguments");
+  const float scale = 1.f / (float)((double)ncell * nc);
+  mse_kernel<<<1184, 256, 0, static_cast<cudaStream_t>(stream)>>>(f, t, w, ncell, nc, cp, scale,
+                                                                     static_cast<__nv_bfloat16 *>(grad), loss);
+  return cudaGetLastError() == cudaSuccess ? 0 : nn_fail("nn_mse: launch failed");
+}
+
+int tcgpu_nn_adam(float * p, const float * g, float * m, float * v, size_t n, float lr, float beta1, float beta2,
+                  float eps, int step, void * stream) {
+  if (!p || !g || !m || !v || step < 1) return nn_fail("nn_adam: bad arguments");
+  const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+  adam_kernel<<<(int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      p, g, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  return cudaGetLastError() == cudaSuccess ? 0 : nn_fail("nn_adam: launch failed");
 }
 
 // error bits raised by the network kernels since the last clear (synchronises the device)
