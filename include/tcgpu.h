@@ -278,6 +278,32 @@ int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, bool is_comple
 /* free the device state that belongs to this fluid_t */
 int tcgpu_release(fluid_t * fluid);
 
+/* ---- learned closure: grid side --------------------------------------------
+ * No counterpart in the reference. A coarse solver (its own fluid_t, a grid 4x
+ * coarser in every direction whose radial faces are every 4th fine face)
+ * takes a forcing, predicted by a 3x3x3 convolutional network from its own
+ * state, that is added to the explicit terms of ux, uy, uz in every predict.
+ * All coarse contexts need 8-byte storage. */
+/* the CUDA stream of this fluid's device context (network kernels launched on
+ * it stay ordered with the solver's own work) */
+void * tcgpu_stream(const domain_t * domain, fluid_t * fluid);
+/* restrict the fine device state to the coarse one: face fluxes summed (the
+ * restriction keeps a divergence-free field divergence-free), t and p volume
+ * means; walls and periodic images applied. Synchronous. */
+int tcgpu_coarsen(const domain_t * fine_domain, fluid_t * fine, const domain_t * coarse_domain, fluid_t * coarse);
+/* network input of this fluid's device state, asynchronous on its stream:
+ * BF16 [cell][cp] (cp a multiple of 16), channels ux at the centre / scale[0],
+ * uy / scale[1], uz / scale[2], radial index coordinate in [-1, 1], zeros */
+int tcgpu_closure_input(const domain_t * domain, fluid_t * fluid, const double scale[3], int cp, void * out);
+/* training target of one sample, synchronous: out[cell][3] =
+ * (reference - predicted) / tau for ux (channel 0 of cell i = face i + 1 of
+ * the reference's numbering), uy, uz; both fluids on the same coarse grid */
+int tcgpu_closure_target(const domain_t * domain, fluid_t * predicted, fluid_t * reference, double tau, float * out);
+/* f (FP32 [cell][nc], device) times scale becomes the forcing of every
+ * following predict of this fluid (asynchronous on its stream); f = NULL turns
+ * the forcing off */
+int tcgpu_set_forcing(const domain_t * domain, fluid_t * fluid, const float * f, int nc, const double scale[3]);
+
 /* ---- learned closure: network kernels --------------------------------------
  * No counterpart in the reference. Device pointers, asynchronous on the given
  * CUDA stream (NULL: the legacy default stream). Activations are channels-last

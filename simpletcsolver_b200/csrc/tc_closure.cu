@@ -622,6 +622,127 @@ int conv_zchunk(int nx, int ny, int nz) {
 }
 
 }  // namespace
+
+// ---- grid side: 4x restriction, network input, forcing --------------------
+// Restriction of a fine state to the grid coarser by R in every direction
+// (coarse cell = R^3 fine cells, coarse radial faces = every R-th fine face):
+// every coarse face flux is the sum of the fine fluxes through it, so a
+// discretely divergence-free fine field stays divergence-free. ux at coarse
+// face I: the mean of the R^2 fine faces (their flux weights J/hx do not vary
+// on a radial face); uy at coarse y-face J: weights J/hy = hx hz of the fine
+// faces' cells; uz at coarse z-face K: weights J/hz = hx hy; t and p: volume
+// (J) weighted cell means. Interior only; walls and images follow from the
+// boundary kernels.
+template <int R>
+__global__ void coarsen_kernel(Geo gf, FieldsT<double> f, Geo gc, FieldsT<double> c) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int J = blockIdx.y + 1, K = blockIdx.z + 1;
+  if (I > gc.nx) return;
+  const int i0 = R * (I - 1) + 1, j0 = R * (J - 1) + 1, k0 = R * (K - 1) + 1;
+  double sux = 0., suy = 0., wy = 0., suz = 0., wz = 0., st = 0., sp = 0., wv = 0.;
+  for (int a = 0; a < R; a++) {
+    const int i = i0 + a;
+    const double hxz = gf.jdxc[i] / gf.hyxc[i], hxy = gf.jdxc[i] / gf.hz, vol = gf.jdxc[i];
+    for (int b = 0; b < R; b++) {
+      if (a == 0) {   // x face i0: (j0 + b, k0 + e)
+        for (int e = 0; e < R; e++) sux += f.ux[fidx(gf, i0, j0 + b, k0 + e)];
+      }
+      suy += hxz * f.uy[cidx(gf, i, j0, k0 + b)];
+      suz += hxy * f.uz[cidx(gf, i, j0 + b, k0)];
+      for (int e = 0; e < R; e++) {
+        st += vol * f.t[cidx(gf, i, j0 + b, k0 + e)];
+        sp += vol * f.p[cidx(gf, i, j0 + b, k0 + e)];
+      }
+    }
+    wy += R * hxz;
+    wz += R * hxy;
+    wv += R * R * vol;
+  }
+  c.ux[fidx(gc, I, J, K)] = I == 1 ? 0. : sux / (R * R);
+  c.uy[cidx(gc, I, J, K)] = suy / wy;
+  c.uz[cidx(gc, I, J, K)] = suz / wz;
+  c.t[cidx(gc, I, J, K)] = st / wv;
+  c.p[cidx(gc, I, J, K)] = sp / wv;
+}
+
+void launch_coarsen(const Geo & gf, const FieldsT<double> & f, const Geo & gc, const FieldsT<double> & c,
+                    cudaStream_t st) {
+  const dim3 block(64), grid((gc.nx + 63) / 64, gc.ny, gc.nz);
+  coarsen_kernel<4><<<grid, block, 0, st>>>(gf, f, gc, c);
+}
+
+// Network input of the coarse state, BF16 [cell][cp] over interior cells
+// (i, j, k from 0): ux averaged to the centre, uy, uz, each divided by its
+// scale, and the radial index coordinate 2 (i + 1/2) / nx - 1; channels
+// 4 .. cp-1 zero.
+__global__ void closure_input_kernel(Geo g, const double * __restrict__ ux, const double * __restrict__ uy,
+                                     const double * __restrict__ uz, double s0, double s1, double s2, int cp,
+                                     __nv_bfloat16 * __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.nx) return;
+  const int I = i + 1, J = j + 1, K = k + 1;
+  alignas(16) __nv_bfloat16 o[16];
+  for (int q = 0; q < 16; q++) o[q] = __float2bfloat16_rn(0.f);
+  o[0] = __float2bfloat16_rn((float)(0.5 * (ux[fidx(g, I, J, K)] + ux[fidx(g, I + 1, J, K)]) / s0));
+  o[1] = __float2bfloat16_rn((float)(uy[cidx(g, I, J, K)] / s1));
+  o[2] = __float2bfloat16_rn((float)(uz[cidx(g, I, J, K)] / s2));
+  o[3] = __float2bfloat16_rn((float)(2.0 * (i + 0.5) / g.nx - 1.0));
+  uint4 * dp = reinterpret_cast<uint4 *>(out + (((size_t)k * g.ny + j) * g.nx + i) * cp);
+  dp[0] = reinterpret_cast<const uint4 *>(o)[0];
+  dp[1] = reinterpret_cast<const uint4 *>(o)[1];
+  for (int c0 = 16; c0 < cp; c0 += 8) dp[c0 / 8] = make_uint4(0, 0, 0, 0);
+}
+
+void launch_closure_input(const Geo & g, const double * ux, const double * uy, const double * uz, const double s[3],
+                          int cp, void * out, cudaStream_t st) {
+  const dim3 block(64), grid((g.nx + 63) / 64, g.ny, g.nz);
+  closure_input_kernel<<<grid, block, 0, st>>>(g, ux, uy, uz, s[0], s[1], s[2], cp,
+                                               static_cast<__nv_bfloat16 *>(out));
+}
+
+// Network output f (FP32 [cell][nc], nc >= 3) times the scales into the
+// packed forcing of ux (faces 2..nx: channel 0 of cell i = face i + 1 of the
+// reference's numbering), uy and uz (channels 1, 2).
+__global__ void closure_forcing_kernel(int nx, int ny, int nz, const float * __restrict__ f, int nc, double s0,
+                                       double s1, double s2, double * __restrict__ fux, double * __restrict__ fuy,
+                                       double * __restrict__ fuz) {
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % nx);
+    const size_t line = q / nx;
+    fuy[q] = s1 * (double)f[q * nc + 1];
+    fuz[q] = s2 * (double)f[q * nc + 2];
+    if (i >= 1) fux[(size_t)(i - 1) + (size_t)(nx - 1) * line] = s0 * (double)f[q * nc];
+  }
+}
+
+void launch_closure_forcing(int nx, int ny, int nz, const float * f, int nc, const double s[3], double * fux,
+                            double * fuy, double * fuz, cudaStream_t st) {
+  closure_forcing_kernel<<<1184, 256, 0, st>>>(nx, ny, nz, f, nc, s[0], s[1], s[2], fux, fuy, fuz);
+}
+
+// Closure target of one sample: (reference - predicted) / tau for ux (channel
+// 0 of cell i = face i + 1; zero at the wall face), uy, uz, FP32 [cell][3].
+__global__ void closure_target_kernel(Geo g, const double * __restrict__ pux, const double * __restrict__ puy,
+                                      const double * __restrict__ puz, const double * __restrict__ rux,
+                                      const double * __restrict__ ruy, const double * __restrict__ ruz,
+                                      double inv_tau, float * __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= g.nx) return;
+  const int I = i + 1, J = j + 1, K = k + 1;
+  const size_t q = ((size_t)k * g.ny + j) * g.nx + i;
+  const size_t f = fidx(g, I, J, K), c = cidx(g, I, J, K);
+  out[q * 3 + 0] = i == 0 ? 0.f : (float)((rux[f] - pux[f]) * inv_tau);
+  out[q * 3 + 1] = (float)((ruy[c] - puy[c]) * inv_tau);
+  out[q * 3 + 2] = (float)((ruz[c] - puz[c]) * inv_tau);
+}
+
+void launch_closure_target(const Geo & g, const FieldsT<double> & pred, const FieldsT<double> & ref, double tau,
+                           float * out, cudaStream_t st) {
+  const dim3 block(64), grid((g.nx + 63) / 64, g.ny, g.nz);
+  closure_target_kernel<<<grid, block, 0, st>>>(g, pred.ux, pred.uy, pred.uz, ref.ux, ref.uy, ref.uz, 1.0 / tau, out);
+}
+
 }  // namespace tcgpu
 
 using namespace tcgpu;

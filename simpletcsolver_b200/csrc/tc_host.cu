@@ -70,6 +70,8 @@ struct Ctx {
   int cur = 0;          // buffer holding the current state
   void * src[4][2]{};
   double * stage = nullptr;   // FP32 storage: reference-layout doubles between host and device
+  double * frc[4]{};          // closure forcing of ux, uy, uz (packed interior layout; frc[3] unused)
+  bool forcing = false;       // add frc to the explicit terms in every predict
   DeltaSet ds{};
   double * tab_y = nullptr;
   double * tab_z = nullptr;
@@ -642,6 +644,7 @@ static void enqueue_predict(Ctx & c, int rk) {
   for (int v = 0; v < 4; v++) {
     ss.new_[v] = s_new(c, v, rk);
     ss.old_[v] = s_old(c, v, rk);
+    ss.frc[v] = c.forcing ? c.frc[v] : nullptr;
   }
   const FieldBufs in = c.fb[c.cur];
   const FieldBufs out = c.fb[c.cur ^ 1];
@@ -1077,6 +1080,90 @@ int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
   CK(cudaMemcpyAsync(c->h_scalar, c->diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   if (finish(*c, "tcgpu_diagnostics")) return 1;
   memcpy(out, c->h_scalar, 9 * sizeof(double));
+  return 0;
+}
+
+void * tcgpu_stream(const domain_t * domain, fluid_t * fluid) {
+  Ctx * c = get_ctx(domain, fluid);
+  return c ? static_cast<void *>(c->st) : nullptr;
+}
+
+int tcgpu_coarsen(const domain_t * fine_domain, fluid_t * fine, const domain_t * coarse_domain, fluid_t * coarse) {
+  Ctx * f = get_ctx(fine_domain, fine);
+  Ctx * c = get_ctx(coarse_domain, coarse);
+  if (!f || !c) return 1;
+  if (f == c) return fail("tcgpu_coarsen: the fine and coarse fluids are the same");
+  if (f->sb != 8 || c->sb != 8) return fail("tcgpu_coarsen: both contexts need 8-byte storage");
+  if (f->nx != 4 * c->nx || f->ny != 4 * c->ny || f->nz != 4 * c->nz)
+    return fail("tcgpu_coarsen: the coarse grid must be 4x coarser in every direction");
+  // the coarse stream waits for the fine state
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, f->st));
+  CK(cudaStreamWaitEvent(c->st, ev, 0));
+  launch_coarsen(f->g, f->f().as<double>(), c->g, c->f().as<double>(), c->st);
+  apply_bcs(*c, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T);
+  invalidate_dt(*c);
+  const int rc = finish(*c, "tcgpu_coarsen");
+  cudaEventDestroy(ev);
+  return rc;
+}
+
+int tcgpu_closure_input(const domain_t * domain, fluid_t * fluid, const double scale[3], int cp, void * out) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (c->sb != 8) return fail("tcgpu_closure_input: needs 8-byte storage");
+  if (!scale || !out || cp < 16 || cp % 16 || (reinterpret_cast<uintptr_t>(out) & 15u))
+    return fail("tcgpu_closure_input: bad arguments");
+  const FieldsT<double> F = c->f().as<double>();
+  launch_closure_input(c->g, F.ux, F.uy, F.uz, scale, cp, out, c->st);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int tcgpu_closure_target(const domain_t * domain, fluid_t * predicted, fluid_t * reference, double tau, float * out) {
+  Ctx * a = get_ctx(domain, predicted);
+  Ctx * b = get_ctx(domain, reference);
+  if (!a || !b) return 1;
+  if (a->sb != 8 || b->sb != 8) return fail("tcgpu_closure_target: needs 8-byte storage");
+  if (a->nx != b->nx || a->ny != b->ny || a->nz != b->nz) return fail("tcgpu_closure_target: grids differ");
+  if (!(tau > 0.) || !out) return fail("tcgpu_closure_target: bad arguments");
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, b->st));
+  CK(cudaStreamWaitEvent(a->st, ev, 0));
+  launch_closure_target(a->g, a->f().as<double>(), b->f().as<double>(), tau, out, a->st);
+  const int rc = finish(*a, "tcgpu_closure_target");
+  cudaEventDestroy(ev);
+  return rc;
+}
+
+int tcgpu_set_forcing(const domain_t * domain, fluid_t * fluid, const float * f, int nc, const double scale[3]) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  const bool on = f != nullptr;
+  if (on) {
+    if (c->sb != 8) return fail("tcgpu_set_forcing: needs 8-byte storage");
+    if (nc < 3 || !scale) return fail("tcgpu_set_forcing: bad arguments");
+    if (!c->frc[0]) {
+      const size_t nin = (size_t)c->nx * c->ny * c->nz;
+      c->frc[0] = dalloc(*c, (size_t)(c->nx - 1) * c->ny * c->nz);
+      c->frc[1] = dalloc(*c, nin);
+      c->frc[2] = dalloc(*c, nin);
+      if (!c->frc[0] || !c->frc[1] || !c->frc[2]) return fail("tcgpu_set_forcing: cudaMalloc failed");
+    }
+    launch_closure_forcing(c->nx, c->ny, c->nz, f, nc, scale, c->frc[0], c->frc[1], c->frc[2], c->st);
+    CK(cudaGetLastError());
+  }
+  if (on != c->forcing) {   // the captured steps hold the other predict variant
+    for (int b = 0; b < 2; b++) {
+      if (c->step_graph[b]) {
+        cudaGraphExecDestroy(c->step_graph[b]);
+        c->step_graph[b] = nullptr;
+      }
+    }
+    c->forcing = on;
+  }
   return 0;
 }
 

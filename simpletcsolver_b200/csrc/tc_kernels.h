@@ -171,23 +171,28 @@ struct Poisson {
 };
 
 // RK source terms of one substep: old_ (srcA of the previous substep) and new_,
-// stored like the state fields
+// stored like the state fields; frc: optional forcing added to the new
+// explicit terms of ux, uy, uz (FP64, packed interior layout; the learned
+// closure of a coarse grid), null when off
 template <class T>
 struct SrcSetT {
   const T * old_[4];
   T * new_[4];
+  const double * frc[4];
 };
 using SrcSet = SrcSetT<double>;
 struct SrcBufs {
   const void * old_[4];
   void * new_[4];
   int bytes;
+  const double * frc[4];
   template <class T>
   SrcSetT<T> as() const {
     SrcSetT<T> s;
     for (int v = 0; v < 4; v++) {
       s.old_[v] = static_cast<const T *>(old_[v]);
       s.new_[v] = static_cast<T *>(new_[v]);
+      s.frc[v] = frc[v];
     }
     return s;
   }
@@ -260,5 +265,16 @@ void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const Fi
 // rows of pitch floats (element e at e + shift)
 void launch_pack32(const double * src, float * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st);
 void launch_unpack32(const float * src, double * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st);
+
+// learned closure (tc_closure.cu): 4x restriction of a fine state, network
+// input of a coarse state, network output into the predict forcing
+void launch_coarsen(const Geo & gf, const FieldsT<double> & f, const Geo & gc, const FieldsT<double> & c,
+                    cudaStream_t st);
+void launch_closure_input(const Geo & g, const double * ux, const double * uy, const double * uz, const double s[3],
+                          int cp, void * out, cudaStream_t st);
+void launch_closure_forcing(int nx, int ny, int nz, const float * f, int nc, const double s[3], double * fux,
+                            double * fuy, double * fuz, cudaStream_t st);
+void launch_closure_target(const Geo & g, const FieldsT<double> & pred, const FieldsT<double> & ref, double tau,
+                           float * out, cudaStream_t st);
 
 }  // namespace tcgpu

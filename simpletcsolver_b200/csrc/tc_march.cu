@@ -210,6 +210,7 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
     ROUTE(ix, 2. * nu * (q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p));
     ROUTE(iy, nu * (q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp));
     ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
+    if constexpr (IMPL == -2) e += ss.frc[VUX][qf];   // closure forcing
     ss.new_[VUX][qf] = (T)e;
     dl[0] = ca * e + cb * old_x + cg * gi;
   }
@@ -269,6 +270,7 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     ROUTE(ix, nu * (q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip));
     ROUTE(iy, 2. * nu * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
     ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
+    if constexpr (IMPL == -2) e += ss.frc[VUY][qc];
     ss.new_[VUY][qc] = (T)e;
     dl[0] = ca * e + cb * old_y + cg * gi;
   }
@@ -288,6 +290,7 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     ROUTE(ix, nu * (q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip));
     ROUTE(iy, nu * (q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp));
     ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
+    if constexpr (IMPL == -2) e += ss.frc[VUZ][qc];
     ss.new_[VUZ][qc] = (T)e;
     dl[1] = ca * e + cb * old_z + cg * gi;
   }
@@ -751,6 +754,12 @@ void launch_march_nw(const MarchArgs<T> & A, const double * dtp, cudaStream_t st
   const int mask = (A.bc.implicit[0] ? 1 : 0) | (A.bc.implicit[1] ? 2 : 0) | (A.bc.implicit[2] ? 4 : 0);
   const unsigned grid = (unsigned)nblk, block = 32 * NW * TC_MARCH_GROUPS;
   const size_t smem = MarchLayout<NW, JT, T>::BYTES;
+  if constexpr (sizeof(T) == 8) {   // IMPL -2: run-time implicit flags plus the closure forcing
+    if (A.ss.frc[0]) {
+      march_predict_kernel<NW, JT, -2, T><<<grid, block, smem, st>>>(A, dtp);
+      return;
+    }
+  }
   switch (mask) {
     case 1: march_predict_kernel<NW, JT, 1, T><<<grid, block, smem, st>>>(A, dtp); break;
     case 7: march_predict_kernel<NW, JT, 7, T><<<grid, block, smem, st>>>(A, dtp); break;
@@ -767,6 +776,8 @@ void allow_march_smem() {
   cudaFuncSetAttribute(march_predict_kernel<NW, JT, 7, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(march_predict_kernel<NW, JT, 0, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if constexpr (sizeof(T) == 8)
+    cudaFuncSetAttribute(march_predict_kernel<NW, JT, -2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <class T>
