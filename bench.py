@@ -26,6 +26,7 @@ summed; rank 0 only.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import csv
 import datetime
 import io
@@ -88,6 +89,13 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp32", action="store_true", help="skip the FP32-storage arm")
     ap.add_argument("--accuracy-steps", type=int, default=200,
                     help="steps of the FP32-storage vs FP64 accuracy runs (0: skip)")
+    ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure arm")
+    ap.add_argument("--closure-pairs", type=int, default=48, help="training pairs from the fine run")
+    ap.add_argument("--closure-epochs", type=int, default=30)
+    ap.add_argument("--closure-warm", type=int, default=200,
+                    help="fine steps before the first pair (lets the initial noise decay)")
+    ap.add_argument("--closure-window", type=int, default=240,
+                    help="fine steps of the torque comparison window")
     return ap.parse_args(argv)
 
 
@@ -344,7 +352,11 @@ def gpu_arm(args, rank, world, local):
     fp32 = None
     if not args.no_fp32:
         fp32 = fp32_storage_arm(args, lib, d0, case, world, peak, value)
-        gpu_launches += fp32.pop("_launches")
+        fp32["gpu_launches"] = fp32.pop("_launches")
+
+    clo = None
+    if not args.no_closure and nx % 32 == 0 and ny % 64 == 0 and nz % 4 == 0:
+        clo = closure_arm(args, lib, d0, case, peaks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -362,6 +374,7 @@ def gpu_arm(args, rank, world, local):
                            "frac": step_model / peak},
             "kernels": per_kernel,
             "fp32_storage": fp32,
+            "closure": clo,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk.summary(),
@@ -428,6 +441,116 @@ def fp32_storage_arm(args, lib, d0, case, world, peak, value64):
                         "rel_err": abs(tq32 - tq64) / abs(tq64)},
             "sim_time": {"fp64": a["time"], "fp32_storage": b["time"]},
         }
+    return out
+
+
+CLOSURE_FLOP_PER_CELL = 2 * 27 * (4 * 32 + 32 * 32 + 32 * 32 + 32 * 3)   # one forward, real channels
+
+
+def closure_arm(args, lib, d0, case, peaks):
+    """Learned closure on the 4x-coarsened grid: pairs from the fine FP64 run,
+    training on 3/4 of them (every 4th held out), the network's forward pass
+    timed against the tensor-core peak, and a torque comparison over a window
+    of --closure-window fine steps: the fine run, the coarse run with the
+    closure and without it, all started from the same (restricted) state."""
+    import torch
+    from simpletcsolver_b200 import abi, closure
+    from simpletcsolver_b200.solver import Solver
+    td = os.path.dirname(d0)
+    dc = closure.write_coarse_ic(case, os.path.join(td, "coarse"))
+    cc = closure.coarse_case(case)
+    fine = Solver.from_ic(d0, case=case, lib=lib)
+    ca = Solver.from_ic(dc, case=cc, lib=lib)
+    cb = Solver.from_ic(dc, case=cc, lib=lib)
+    cf = Solver.from_ic(dc, case=cc, lib=lib)     # the fine run restricted, for the coarse-grid diagnostics
+    out = {"grid_fine": [case.nx, case.ny, case.nz], "grid_coarse": [cc.nx, cc.ny, cc.nz]}
+    try:
+        for s in (fine, ca, cb, cf):
+            closure.resident(s)
+        fine.run(args.closure_warm)
+        in_scale = (0.05, 1.0, 0.05)
+        t0 = time.perf_counter()
+        data, t_scale = closure.generate(fine, ca, cb, args.closure_pairs, 8, in_scale=in_scale)
+        gen_s = time.perf_counter() - t0
+        n = data.n
+        train = [q for q in range(n) if q % 4]
+        held = [q for q in range(n) if q % 4 == 0]
+        net = closure.ClosureNet(lib, (cc.nx, cc.ny, cc.nz), seed=0)
+        before = closure.relative_error(net, data, held)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hist = closure.train(net, data, train, epochs=args.closure_epochs, batch=4, lr=2e-3)
+        train_s = time.perf_counter() - t0
+        err_train = closure.relative_error(net, data, train)
+        err_held = closure.relative_error(net, data, held)
+        # forward pass on the tensor cores: CUDA events on the stream it runs on
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        x = data.X[0]
+        for _ in range(3):
+            net.forward(x, keep=False)
+        e0.record()
+        for _ in range(20):
+            net.forward(x, keep=False)
+        e1.record()
+        torch.cuda.synchronize()
+        fwd_ms = e0.elapsed_time(e1) / 20
+        tflops = CLOSURE_FLOP_PER_CELL * net.ncell / (fwd_ms / 1e3) / 1e12
+        peak = float(peaks.get("bf16_tflops", 1590.0))
+        # torque window: fine, coarse with and without the closure from one state
+        for s in (ca, cb):
+            s._check(lib.tcgpu_coarsen(C.byref(fine.domain), C.byref(fine.fluid), C.byref(s.domain),
+                                       C.byref(s.fluid)), "coarsen")
+        def restricted_torque():
+            cf._check(lib.tcgpu_coarsen(C.byref(fine.domain), C.byref(fine.fluid), C.byref(cf.domain),
+                                        C.byref(cf.fluid)), "coarsen")
+            return cf.diagnostics()["injection_u"]
+
+        ft, fq, rq = [0.0], [fine.diagnostics()["injection_u"]], [restricted_torque()]
+        fine_s = 0.0
+        for _ in range(max(1, args.closure_window // 10)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ft.append(ft[-1] + float(np.sum(fine.run(10))))
+            fine_s += time.perf_counter() - t0
+            fq.append(fine.diagnostics()["injection_u"])
+            rq.append(restricted_torque())
+        t0 = time.perf_counter()
+        at, aq = closure.run_coarse(ca, ft[-1], net, in_scale, t_scale)
+        coarse_s = time.perf_counter() - t0
+        bt, bq = closure.run_coarse(cb, ft[-1])
+        tq_f = closure.time_average(ft, fq)
+        tq_r = closure.time_average(ft, rq)
+        tq_c = closure.time_average(at, aq)
+        tq_p = closure.time_average(bt, bq)
+        # mean azimuthal velocity profile at the end of the window (coarse grid)
+        prof = {}
+        for name, s in (("restricted_fine", cf), ("closure", ca), ("plain", cb)):
+            s.pull(abi.UY)
+            prof[name] = s.field("uy")[1:-1, 1:-1, 1:-1].mean(axis=(0, 1))
+        perr = lambda a: float(np.linalg.norm(a - prof["restricted_fine"]) / np.linalg.norm(prof["restricted_fine"]))
+        out.update({
+            "pairs": n, "pair_gap_fine_steps": 8, "generate_s": gen_s,
+            "training": {"epochs": args.closure_epochs, "samples": len(train), "batch": 8, "seconds": train_s,
+                         "loss_first": hist[0], "loss_last": hist[-1]},
+            "apriori_rel_error": {"no_closure": 1.0, "train": err_train, "held_out": err_held,
+                                  "held_out_untrained": before},
+            "forward": {"ms": fwd_ms, "tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
+                        "flop_per_cell": CLOSURE_FLOP_PER_CELL,
+                        "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
+            "torque_window": {
+                "sim_time": ft[-1], "fine_steps": 10 * (len(ft) - 1), "coarse_steps": len(at) - 1,
+                "fine": tq_f, "restricted_fine": tq_r, "coarse_closure": tq_c, "coarse_plain": tq_p,
+                "rel_err_closure": abs(tq_c - tq_f) / abs(tq_f), "rel_err_plain": abs(tq_p - tq_f) / abs(tq_f),
+                "rel_err_closure_vs_restricted": abs(tq_c - tq_r) / abs(tq_r),
+                "rel_err_plain_vs_restricted": abs(tq_p - tq_r) / abs(tq_r),
+                "mean_uy_profile_rel_err": {"closure": perr(prof["closure"]), "plain": perr(prof["plain"])},
+                "wall_s_fine": fine_s, "wall_s_coarse_closure": coarse_s,
+                "speedup_vs_fine": (fine_s / ft[-1]) / (coarse_s / max(at[-1], 1e-30)),
+            },
+        })
+    finally:
+        for s in (fine, ca, cb, cf):
+            s.release()
     return out
 
 

@@ -215,19 +215,20 @@ def generate(fine, coarse_a, coarse_b, nsamples: int, gap: int, in_scale, data: 
     into coarse_a (input), advance the fine solver by n steps (n fine time
     steps fit in one coarse time step, n <= max_sub), step coarse_a once with
     their total tau, restrict the new fine state into coarse_b and take the
-    target (b - a) / tau. All three solvers are device-resident. t_scale
-    (per channel) defaults to the rms of the first target."""
+    target (b - a) / tau. All three solvers are device-resident. The targets
+    are divided by t_scale (per channel; default: their rms over all pairs)."""
     lib = fine.lib
     torch = _torch()
     ncell = coarse_a.nx * coarse_a.ny * coarse_a.nz
     data = data or Dataset(ncell, nsamples)
     one = torch.zeros(ncell * NOUT, dtype=torch.float32, device="cuda")
+    raw = []
     for _ in range(nsamples):
         if gap > 0:
             fine.run(gap)
         coarse_a._check(lib.tcgpu_coarsen(C.byref(fine.domain), C.byref(fine.fluid), C.byref(coarse_a.domain),
                                           C.byref(coarse_a.fluid)), "coarsen")
-        x = data.X[data.n]
+        x = data.X[data.n + len(raw)]
         coarse_a._check(lib.tcgpu_closure_input(C.byref(coarse_a.domain), C.byref(coarse_a.fluid),
                                                 _d3(in_scale), NIN, _p(x)), "closure_input")
         dt_c = coarse_a.decide_dt()
@@ -239,11 +240,13 @@ def generate(fine, coarse_a, coarse_b, nsamples: int, gap: int, in_scale, data: 
                                           C.byref(coarse_b.fluid)), "coarsen")
         coarse_a._check(lib.tcgpu_closure_target(C.byref(coarse_a.domain), C.byref(coarse_a.fluid),
                                                  C.byref(coarse_b.fluid), tau, _p(one)), "closure_target")
-        t = one.cpu().numpy().reshape(-1, NOUT)
-        if t_scale is None:
-            t_scale = np.sqrt(np.mean(t.astype(np.float64) ** 2, axis=0)) + 1e-30
-        data.T[data.n].copy_(torch.from_numpy((t / np.asarray(t_scale, np.float32)[None, :]).ravel()))
+        raw.append(one.cpu().numpy().reshape(-1, NOUT).copy())
         data.tau.append(tau)
+    if t_scale is None:
+        ss = sum(np.sum(r.astype(np.float64) ** 2, axis=0) for r in raw)
+        t_scale = np.sqrt(ss / (len(raw) * ncell)) + 1e-30
+    for r in raw:
+        data.T[data.n].copy_(torch.from_numpy((r / np.asarray(t_scale, np.float32)[None, :]).ravel()))
         data.n += 1
     return data, np.asarray(t_scale, dtype=np.float64)
 
@@ -292,16 +295,18 @@ def relative_error(net: ClosureNet, data: Dataset, idx) -> float:
     return num / den
 
 
-def run_coarse(s, nsteps: int, net: ClosureNet | None = None, in_scale=None, t_scale=None, every: int = 1):
-    """nsteps adaptive steps of the device-resident coarse solver s, with the
-    network's forcing (computed from the state at the start of each step, held
-    over the step) when net is given. Returns times and the energy injection
-    (inner-wall torque) after each `every` steps."""
+def run_coarse(s, t_end: float, net: ClosureNet | None = None, in_scale=None, t_scale=None, max_steps: int = 100000):
+    """Adaptive steps of the device-resident coarse solver s until its time
+    reaches t_end, with the network's forcing (computed from the state at the
+    start of each step, held over the step) when net is given. Returns the
+    times and the energy injection (inner-wall torque) after every step."""
     lib = s.lib
     st = stream_of(s)
-    times, torque = [], []
+    times, torque = [0.0], [s.diagnostics()["injection_u"]]
     t = 0.0
-    for k in range(nsteps):
+    for _ in range(max_steps):
+        if t >= t_end:
+            break
         if net is not None:
             s._check(lib.tcgpu_closure_input(C.byref(s.domain), C.byref(s.fluid), _d3(in_scale), NIN,
                                              _p(net.a[0])), "closure_input")
@@ -309,10 +314,16 @@ def run_coarse(s, nsteps: int, net: ClosureNet | None = None, in_scale=None, t_s
             s._check(lib.tcgpu_set_forcing(C.byref(s.domain), C.byref(s.fluid), _p(net.out), NOUT, _d3(t_scale)),
                      "set_forcing")
         t += float(s.run(1)[0])
-        if (k + 1) % every == 0:
-            times.append(t)
-            torque.append(s.diagnostics()["injection_u"])
+        times.append(t)
+        torque.append(s.diagnostics()["injection_u"])
     if net is not None:
         s._check(lib.tcgpu_set_forcing(C.byref(s.domain), C.byref(s.fluid), None, NOUT, _d3((1, 1, 1))),
                  "set_forcing")
     return np.asarray(times), np.asarray(torque)
+
+
+def time_average(times, values) -> float:
+    """trapezoidal mean of values(times) over [times[0], times[-1]]"""
+    t = np.asarray(times, dtype=np.float64)
+    v = np.asarray(values, dtype=np.float64)
+    return float(np.sum(0.5 * (v[1:] + v[:-1]) * np.diff(t)) / (t[-1] - t[0]))
