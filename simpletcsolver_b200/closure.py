@@ -327,3 +327,44 @@ def time_average(times, values) -> float:
     t = np.asarray(times, dtype=np.float64)
     v = np.asarray(values, dtype=np.float64)
     return float(np.sum(0.5 * (v[1:] + v[:-1]) * np.diff(t)) / (t[-1] - t[0]))
+
+
+def _main(argv=None) -> int:
+    """python -m simpletcsolver_b200.closure [--grid NXxNYxNZ] [--iters N]:
+    time the network's forward and backward passes on a synthetic input of a
+    coarse grid (CUDA events on the stream the kernels run on)."""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", default="64x256x128")
+    ap.add_argument("--iters", type=int, default=10)
+    args = ap.parse_args(argv)
+    torch = _torch()
+    grid = tuple(int(v) for v in args.grid.lower().split("x"))
+    lib = abi.load()
+    net = ClosureNet(lib, grid, seed=0)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(net.ncell * NIN, device="cuda", generator=gen).to(torch.bfloat16)
+    tgt = torch.randn(net.ncell * NOUT, device="cuda", generator=gen)
+    net.forward(x)
+    net.backward(tgt, x=x)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(args.iters):
+        net.forward(x)
+    e[1].record()
+    for _ in range(args.iters):
+        net.backward(tgt, x=x)
+    e[2].record()
+    torch.cuda.synchronize()
+    f_ms, b_ms = e[0].elapsed_time(e[1]) / args.iters, e[1].elapsed_time(e[2]) / args.iters
+    flop = 2 * 27 * (4 * 32 + 32 * 32 + 32 * 32 + 32 * 3) * net.ncell
+    print(f"grid {grid}: forward {f_ms:.3f} ms ({flop / f_ms / 1e9:.1f} TFLOP/s), backward {b_ms:.3f} ms")
+    if lib.tcgpu_nn_status(1) != 0:
+        print("a network kernel reported a wait that gave up")
+        return 1
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())
