@@ -417,6 +417,13 @@ static int build_tables(Ctx & c, const domain_t * d) {
       yf.lapy_c[v] = dP + (size_t)v * 6 * L + 4 * L;
       yf.lapy_u[v] = dP + (size_t)v * 6 * L + 5 * L;
     }
+    yf.uniform_y = 1;
+    for (int v = 0; v < 4; v++) {
+      const double * b = P.data() + (size_t)v * 6 * L;
+      for (int e = 1; e < yf.n_i[v]; e++)
+        for (int r = 3; r < 6; r++)
+          if (b[r * L + e] != b[r * L]) yf.uniform_y = 0;
+    }
     yf.lapz_l = cf.lz_l;
     yf.lapz_c = cf.lz_c;
     yf.lapz_u = cf.lz_u;
@@ -578,6 +585,7 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   if (build_tables(*c, d)) { destroy_ctx(c); return nullptr; }
   poisson_smem_limits();
   march_smem_limits();
+  allow_periodic_lines_smem();
   c->nu = 0.;
   if (set_physics(*c, fl, d)) { destroy_ctx(c); return nullptr; }
   return c;

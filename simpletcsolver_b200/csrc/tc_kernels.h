@@ -134,6 +134,7 @@ struct XFactors {
 struct YZFactors {
   int n_i[4];
   int max_i;
+  int uniform_y;            // the y operators do not depend on i (planar grids): factors of i = 0 serve all
   size_t stride_y;          // max_i * ny
   size_t stride_z;          // nz
   const double * lapy_l[4];
@@ -216,6 +217,7 @@ void launch_apply(const Geo & g, const Bc & bc, const FieldBufs & in, const Fiel
 void launch_yzfactors(const Geo & g, const YZFactors & yf, const double * dtp, double nu, double kappa, cudaStream_t st);
 void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st);
 void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st);
+void allow_periodic_lines_smem();
 
 // optional per-launch callback of the host's kernel accounting
 struct PoissonMarks {

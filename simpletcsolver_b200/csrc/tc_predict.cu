@@ -107,12 +107,13 @@ __global__ void ysolve_kernel(Geo g, YZFactors yf, int rkstep, int var,
   const int n = g.ny;
   const size_t so = (size_t)(rkstep * 4 + var) * yf.stride_y;
   // per-ii factors of the reduced (n-1) system and the correction vector
-  const double * v = yf.v + so + (size_t)ii * n;
-  const double * w = yf.w + so + (size_t)ii * n;
-  const double * q1 = yf.q1 + so + (size_t)ii * n;
-  const double l = yf.l[(rkstep * 4 + var) * yf.max_i + ii];
-  const double c = yf.c[(rkstep * 4 + var) * yf.max_i + ii];
-  const double u = yf.u[(rkstep * 4 + var) * yf.max_i + ii];
+  const int fi = yf.uniform_y ? 0 : ii;
+  const double * v = yf.v + so + (size_t)fi * n;
+  const double * w = yf.w + so + (size_t)fi * n;
+  const double * q1 = yf.q1 + so + (size_t)fi * n;
+  const double l = yf.l[(rkstep * 4 + var) * yf.max_i + fi];
+  const double c = yf.c[(rkstep * 4 + var) * yf.max_i + fi];
+  const double u = yf.u[(rkstep * 4 + var) * yf.max_i + fi];
   double * q = delta + (size_t)ii + (size_t)n_i * (size_t)n * (size_t)(k - 1);
   const size_t st = (size_t)n_i;
   // gtsv on q[0..n-2]
@@ -169,6 +170,179 @@ __global__ void zsolve_kernel(Geo g, YZFactors yf, int rkstep, int var,
   for (int e = 0; e < n - 1; e++) q[e * st] = q[e * st] + last * q1[e];
 }
 
+// ------------------------------------------------------------ periodic solves, one warp per line
+// The same solves for lines of N = 32 E points: a CTA takes a tile of PT
+// consecutive radial indices of one plane (y lines) or one row (z lines) into
+// shared memory with coalesced loads, and each warp solves whole lines with
+// the forward and backward Thomas recurrences written as affine maps
+// (y_j = a_j y_{j-1} + b_j) combined by a 5-level shuffle scan, E points per
+// lane; then the Sherman-Morrison correction (src/tdm.c:88-99) and a coalesced
+// store. Element (j, t) of the tile sits at j PT + (t ^ (j / E mod PT)), so the
+// 32 lanes reading element j = lane E + e of one line hit distinct banks.
+#ifndef TC_PLINES_PT
+#define TC_PLINES_PT 16
+#endif
+#ifndef TC_PLINES_THREADS
+#define TC_PLINES_THREADS 256
+#endif
+constexpr int PT = TC_PLINES_PT;
+
+struct PAff { double a, b; };
+
+template <int E>
+__global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
+    int n_i, long long outer_stride, long long elem_stride, const double * __restrict__ fl,
+    const double * __restrict__ fc, const double * __restrict__ fu, int lcu_stride, const double * __restrict__ fw,
+    const double * __restrict__ fv, const double * __restrict__ fq1, int fac_stride, double * __restrict__ delta) {
+  constexpr int N = 32 * E;
+  extern __shared__ double sq[];
+  const int ntile = (n_i + PT - 1) / PT;
+  const int tile = (int)(blockIdx.x % ntile);
+  const long long outer = blockIdx.x / ntile;
+  const int ii0 = tile * PT;
+  const int nt = min(PT, n_i - ii0);
+  double * base = delta + ii0 + outer_stride * outer;
+  // all of a thread's loads in flight at once (PER independent loads)
+  constexpr int NT = TC_PLINES_THREADS, PER = N * PT / NT;
+  static_assert((N * PT) % NT == 0, "tile size must be a multiple of the thread count");
+  {
+    double buf[PER];
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+      const int q = threadIdx.x + r * NT, t = q % PT, j = q / PT;
+      buf[r] = t < nt ? base[(long long)j * elem_stride + t] : 0.;
+    }
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+      const int q = threadIdx.x + r * NT, t = q % PT, j = q / PT;
+      sq[j * PT + (t ^ ((j / E) & (PT - 1)))] = buf[r];
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int t = wid; t < nt; t += nw) {
+    const int ii = ii0 + t;
+    const double l = fl[ii * lcu_stride], c = fc[ii * lcu_stride], u = fu[ii * lcu_stride];
+    const double * w = fw + (size_t)ii * fac_stride;
+    const double * v = fv + (size_t)ii * fac_stride;
+    const double * q1 = fq1 + (size_t)ii * fac_stride;
+    const int sw = t ^ (lane & (PT - 1));
+    double q[E], ww[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      q[e] = sq[(lane * E + e) * PT + sw];
+      ww[e] = w[lane * E + e];
+    }
+    const double qlast = __shfl_sync(0xffffffffu, q[E - 1], 31);   // right-hand side of row N - 1
+    // forward sweep of the reduced system (rows 0 .. N-2): y_0 = q_0 / c,
+    // y_j = w_j (q_j - l y_{j-1}); row N - 1 is left as it is
+    PAff acc{1., 0.};
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int j = lane * E + e;
+      double fa, fb;
+      if (j == 0) { fa = 0.; fb = q[e] / c; }
+      else if (j == N - 1) { fa = 1.; fb = 0.; }
+      else { fa = -ww[e] * l; fb = ww[e] * q[e]; }
+      acc.b = fa * acc.b + fb;
+      acc.a = fa * acc.a;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double oa = __shfl_up_sync(0xffffffffu, acc.a, off);
+      const double ob = __shfl_up_sync(0xffffffffu, acc.b, off);
+      if (lane >= off) { acc.b = acc.a * ob + acc.b; acc.a = acc.a * oa; }
+    }
+    double yin = __shfl_up_sync(0xffffffffu, acc.b, 1);
+    if (lane == 0) yin = 0.;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int j = lane * E + e;
+      if (j == N - 1) continue;
+      const double r = (j == 0) ? q[e] / c : ww[e] * (q[e] - l * yin);
+      q[e] = r;
+      yin = r;
+    }
+    // backward sweep: x_{N-2} = y_{N-2}, x_j = y_j - v_j x_{j+1} (v_{N-2} = 0)
+    double vv[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) vv[e] = v[lane * E + e];
+    PAff bac{1., 0.};
+#pragma unroll
+    for (int e = E - 1; e >= 0; e--) {
+      const int j = lane * E + e;
+      const double fa = (j == N - 1) ? 0. : -vv[e], fb = (j == N - 1) ? 0. : q[e];
+      bac.b = fa * bac.b + fb;
+      bac.a = fa * bac.a;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double oa = __shfl_down_sync(0xffffffffu, bac.a, off);
+      const double ob = __shfl_down_sync(0xffffffffu, bac.b, off);
+      if (lane + off < 32) { bac.b = bac.a * ob + bac.b; bac.a = bac.a * oa; }
+    }
+    double xin = __shfl_down_sync(0xffffffffu, bac.b, 1);
+    if (lane == 31) xin = 0.;
+#pragma unroll
+    for (int e = E - 1; e >= 0; e--) {
+      const int j = lane * E + e;
+      if (j == N - 1) { xin = 0.; continue; }
+      const double x = q[e] - vv[e] * xin;
+      q[e] = x;
+      xin = x;
+    }
+    // Sherman-Morrison: the last unknown, then the correction of rows 0 .. N-2
+    const double x0 = __shfl_sync(0xffffffffu, q[0], 0);
+    const double xn2 = __shfl_sync(0xffffffffu, q[E - 2], 31);
+    const double num = qlast - u * x0 - l * xn2;
+    const double den = c + u * q1[0] + l * q1[N - 2];
+    const double last = fabs(den) < 2.220446049250313e-16 ? 0. : num / den;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int j = lane * E + e;
+      const double x = (j == N - 1) ? last : q[e] + last * q1[j];
+      sq[j * PT + sw] = x;
+    }
+  }
+  __syncthreads();
+#pragma unroll 8
+  for (int r = 0; r < PER; r++) {
+    const int q = threadIdx.x + r * NT, t = q % PT, j = q / PT;
+    if (t < nt) base[(long long)j * elem_stride + t] = sq[j * PT + (t ^ ((j / E) & (PT - 1)))];
+  }
+}
+
+// lines of n points through the warp kernel when n = 32 E, E in {2, 4, 8, 16};
+// false: not handled
+static bool launch_periodic_lines(int n, int n_i, long long nouter, long long outer_stride, long long elem_stride,
+                                  const double * fl, const double * fc, const double * fu, int lcu_stride,
+                                  const double * fw, const double * fv, const double * fq1, int fac_stride,
+                                  double * delta, cudaStream_t st) {
+  const long long nblk = (long long)((n_i + PT - 1) / PT) * nouter;
+  const size_t smem = (size_t)n * PT * sizeof(double);
+#define PLK(EE)                                                                                              \
+  case 32 * EE:                                                                                              \
+    periodic_lines_kernel<EE><<<(unsigned)nblk, TC_PLINES_THREADS, smem, st>>>(n_i, outer_stride, elem_stride, fl, fc, fu,   \
+                                                                 lcu_stride, fw, fv, fq1, fac_stride, delta); \
+    return true;
+  switch (n) {
+    PLK(2)
+    PLK(4)
+    PLK(8)
+    PLK(16)
+    default:
+      return false;
+  }
+#undef PLK
+}
+
+void allow_periodic_lines_smem() {
+  cudaFuncSetAttribute(periodic_lines_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * PT * 8);
+}
+
 // ------------------------------------------------------------ periodic factors
 // Factors of the reduced (n-1) systems of the periodic solves (src/tdm.c:78-87):
 // one thread per (substep, variable, radial index) for y, per (substep,
@@ -197,7 +371,7 @@ __global__ void yzfactor_kernel(Geo g, YZFactors yf, const double * __restrict__
   if (tid < total_y) {
     const int rv = tid / yf.max_i, ii = tid % yf.max_i;
     const int rk = rv / 4, var = rv % 4;
-    if (ii >= yf.n_i[var]) return;
+    if (ii >= yf.n_i[var] || (yf.uniform_y && ii > 0)) return;
     const double diff = var == VT ? kappa : nu;
     double pf = 0.5 * rk_gamma(rk) * dt * diff;
     if (var == VUY || var == VT) pf = 2. * pf;
@@ -252,14 +426,26 @@ void launch_apply(const Geo & g, const Bc & bc, const FieldBufs & in, const Fiel
 
 void launch_ysolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st) {
   for (int v = 0; v < 4; v++) {
-    const long long n = (long long)yf.n_i[v] * g.nz;
+    const int n_i = yf.n_i[v], rv = rkstep * 4 + v;
+    const size_t so = (size_t)rv * yf.stride_y;
+    const int us = yf.uniform_y ? 0 : 1;   // uniform: every line uses the factors of i = 0
+    if (launch_periodic_lines(g.ny, n_i, g.nz, (long long)n_i * g.ny, n_i, yf.l + rv * yf.max_i,
+                              yf.c + rv * yf.max_i, yf.u + rv * yf.max_i, us, yf.w + so, yf.v + so, yf.q1 + so,
+                              us * g.ny, ds.d[v], st))
+      continue;
+    const long long n = (long long)n_i * g.nz;
     ysolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, ds.d[v]);
   }
 }
 
 void launch_zsolve(const Geo & g, const YZFactors & yf, int rkstep, const DeltaSet & ds, cudaStream_t st) {
   for (int v = 0; v < 4; v++) {
-    const long long n = (long long)yf.n_i[v] * g.ny;
+    const int n_i = yf.n_i[v], rv = rkstep * 4 + v;
+    const size_t so = (size_t)rv * yf.stride_z;
+    if (launch_periodic_lines(g.nz, n_i, g.ny, n_i, (long long)n_i * g.ny, yf.lz + rv, yf.cz + rv, yf.uz + rv, 0,
+                              yf.wz + so, yf.vz + so, yf.q1z + so, 0, ds.d[v], st))
+      continue;
+    const long long n = (long long)n_i * g.ny;
     zsolve_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(g, yf, rkstep, v, ds.d[v]);
   }
 }

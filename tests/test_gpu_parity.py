@@ -27,6 +27,8 @@ CASES = {
     "tc": ic.taylor_couette(16, 32, 16, 3400.0),
     "tcexp": ic.taylor_couette(20, 16, 8, 3400.0, implicit=(False, False, False)),
     "planar": ic.plane_couette(12, 16, 8, 2000.0),
+    # y and z lines of 64 and 128 points: the warp-per-line periodic solves
+    "planar_lines": ic.plane_couette(12, 64, 128, 2000.0),
 }
 
 
