@@ -189,7 +189,11 @@ constexpr int PT = TC_PLINES_PT;
 
 struct PAff { double a, b; };
 
-template <int E>
+// element j of a staged factor row: row j / 16, column (j mod 16) ^ (j / 16 mod
+// 16), so the lanes reading j = lane E + e (E = 4 .. 16) hit distinct banks
+__device__ __forceinline__ int fsw(int j) { return (j & ~15) | ((j & 15) ^ ((j >> 4) & 15)); }
+
+template <int E, bool UNI>
 __global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
     int n_i, long long outer_stride, long long elem_stride, const double * __restrict__ fl,
     const double * __restrict__ fc, const double * __restrict__ fu, int lcu_stride, const double * __restrict__ fw,
@@ -218,6 +222,15 @@ __global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
       sq[j * PT + (t ^ ((j / E) & (PT - 1)))] = buf[r];
     }
   }
+  // one set of factors for every line: staged once (w, v, q1 after the tile)
+  double * sfw = sq + N * PT, * sfv = sfw + N, * sfq = sfv + N;
+  if constexpr (UNI) {
+    for (int j = threadIdx.x; j < N; j += NT) {
+      sfw[fsw(j)] = fw[j];
+      sfv[fsw(j)] = fv[j];
+      sfq[fsw(j)] = fq1[j];
+    }
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int t = wid; t < nt; t += nw) {
@@ -231,22 +244,30 @@ __global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
 #pragma unroll
     for (int e = 0; e < E; e++) {
       q[e] = sq[(lane * E + e) * PT + sw];
-      ww[e] = w[lane * E + e];
+      ww[e] = UNI ? sfw[fsw(lane * E + e)] : w[lane * E + e];
     }
     const double qlast = __shfl_sync(0xffffffffu, q[E - 1], 31);   // right-hand side of row N - 1
     // forward sweep of the reduced system (rows 0 .. N-2): y_0 = q_0 / c,
     // y_j = w_j (q_j - l y_{j-1}); row N - 1 is left as it is
-    PAff acc{1., 0.};
+    // the lane's maps y_j = fa_j y_{j-1} + fb_j, combined by an in-register
+    // prefix (log2 E levels of independent compositions, not an E-long chain)
+    double fa[E], fb[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int j = lane * E + e;
-      double fa, fb;
-      if (j == 0) { fa = 0.; fb = q[e] / c; }
-      else if (j == N - 1) { fa = 1.; fb = 0.; }
-      else { fa = -ww[e] * l; fb = ww[e] * q[e]; }
-      acc.b = fa * acc.b + fb;
-      acc.a = fa * acc.a;
+      if (j == 0) { fa[e] = 0.; fb[e] = q[e] / c; }
+      else if (j == N - 1) { fa[e] = 1.; fb[e] = 0.; }
+      else { fa[e] = -ww[e] * l; fb[e] = ww[e] * q[e]; }
     }
+#pragma unroll
+    for (int d = 1; d < E; d <<= 1) {
+#pragma unroll
+      for (int e = E - 1; e >= d; e--) {
+        fb[e] = fa[e] * fb[e - d] + fb[e];
+        fa[e] = fa[e] * fa[e - d];
+      }
+    }
+    PAff acc{fa[E - 1], fb[E - 1]};
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const double oa = __shfl_up_sync(0xffffffffu, acc.a, off);
@@ -256,25 +277,27 @@ __global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
     double yin = __shfl_up_sync(0xffffffffu, acc.b, 1);
     if (lane == 0) yin = 0.;
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const int j = lane * E + e;
-      if (j == N - 1) continue;
-      const double r = (j == 0) ? q[e] / c : ww[e] * (q[e] - l * yin);
-      q[e] = r;
-      yin = r;
-    }
-    // backward sweep: x_{N-2} = y_{N-2}, x_j = y_j - v_j x_{j+1} (v_{N-2} = 0)
+    for (int e = 0; e < E; e++) q[e] = fa[e] * yin + fb[e];   // row N - 1 is not used below
+    // backward sweep: x_{N-2} = y_{N-2}, x_j = y_j - v_j x_{j+1} (v_{N-2} = 0),
+    // suffix maps combined the same way
     double vv[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) vv[e] = v[lane * E + e];
-    PAff bac{1., 0.};
+    for (int e = 0; e < E; e++) vv[e] = UNI ? sfv[fsw(lane * E + e)] : v[lane * E + e];
 #pragma unroll
-    for (int e = E - 1; e >= 0; e--) {
+    for (int e = 0; e < E; e++) {
       const int j = lane * E + e;
-      const double fa = (j == N - 1) ? 0. : -vv[e], fb = (j == N - 1) ? 0. : q[e];
-      bac.b = fa * bac.b + fb;
-      bac.a = fa * bac.a;
+      fa[e] = (j == N - 1) ? 0. : -vv[e];
+      fb[e] = (j == N - 1) ? 0. : q[e];
     }
+#pragma unroll
+    for (int d = 1; d < E; d <<= 1) {
+#pragma unroll
+      for (int e = 0; e + d < E; e++) {
+        fb[e] = fa[e] * fb[e + d] + fb[e];
+        fa[e] = fa[e] * fa[e + d];
+      }
+    }
+    PAff bac{fa[0], fb[0]};
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
       const double oa = __shfl_down_sync(0xffffffffu, bac.a, off);
@@ -284,23 +307,17 @@ __global__ void __launch_bounds__(TC_PLINES_THREADS) periodic_lines_kernel(
     double xin = __shfl_down_sync(0xffffffffu, bac.b, 1);
     if (lane == 31) xin = 0.;
 #pragma unroll
-    for (int e = E - 1; e >= 0; e--) {
-      const int j = lane * E + e;
-      if (j == N - 1) { xin = 0.; continue; }
-      const double x = q[e] - vv[e] * xin;
-      q[e] = x;
-      xin = x;
-    }
+    for (int e = 0; e < E; e++) q[e] = fa[e] * xin + fb[e];
     // Sherman-Morrison: the last unknown, then the correction of rows 0 .. N-2
     const double x0 = __shfl_sync(0xffffffffu, q[0], 0);
     const double xn2 = __shfl_sync(0xffffffffu, q[E - 2], 31);
     const double num = qlast - u * x0 - l * xn2;
-    const double den = c + u * q1[0] + l * q1[N - 2];
+    const double den = c + u * (UNI ? sfq[fsw(0)] : q1[0]) + l * (UNI ? sfq[fsw(N - 2)] : q1[N - 2]);
     const double last = fabs(den) < 2.220446049250313e-16 ? 0. : num / den;
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int j = lane * E + e;
-      const double x = (j == N - 1) ? last : q[e] + last * q1[j];
+      const double x = (j == N - 1) ? last : q[e] + last * (UNI ? sfq[fsw(j)] : q1[j]);
       sq[j * PT + sw] = x;
     }
   }
@@ -319,11 +336,16 @@ static bool launch_periodic_lines(int n, int n_i, long long nouter, long long ou
                                   const double * fw, const double * fv, const double * fq1, int fac_stride,
                                   double * delta, cudaStream_t st) {
   const long long nblk = (long long)((n_i + PT - 1) / PT) * nouter;
-  const size_t smem = (size_t)n * PT * sizeof(double);
+  const bool uni = fac_stride == 0;
+  const size_t smem = (size_t)n * (PT + (uni ? 3 : 0)) * sizeof(double);
 #define PLK(EE)                                                                                              \
   case 32 * EE:                                                                                              \
-    periodic_lines_kernel<EE><<<(unsigned)nblk, TC_PLINES_THREADS, smem, st>>>(n_i, outer_stride, elem_stride, fl, fc, fu,   \
-                                                                 lcu_stride, fw, fv, fq1, fac_stride, delta); \
+    if (uni)                                                                                                 \
+      periodic_lines_kernel<EE, true><<<(unsigned)nblk, TC_PLINES_THREADS, smem, st>>>(                      \
+          n_i, outer_stride, elem_stride, fl, fc, fu, lcu_stride, fw, fv, fq1, fac_stride, delta);           \
+    else                                                                                                     \
+      periodic_lines_kernel<EE, false><<<(unsigned)nblk, TC_PLINES_THREADS, smem, st>>>(                     \
+          n_i, outer_stride, elem_stride, fl, fc, fu, lcu_stride, fw, fv, fq1, fac_stride, delta);           \
     return true;
   switch (n) {
     PLK(2)
@@ -337,10 +359,14 @@ static bool launch_periodic_lines(int n, int n_i, long long nouter, long long ou
 }
 
 void allow_periodic_lines_smem() {
-  cudaFuncSetAttribute(periodic_lines_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * PT * 8);
-  cudaFuncSetAttribute(periodic_lines_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * PT * 8);
-  cudaFuncSetAttribute(periodic_lines_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * PT * 8);
-  cudaFuncSetAttribute(periodic_lines_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 512 * (PT + 3) * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 256 * (PT + 3) * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * (PT + 3) * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * PT * 8);
+  cudaFuncSetAttribute(periodic_lines_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * (PT + 3) * 8);
 }
 
 // ------------------------------------------------------------ periodic factors
