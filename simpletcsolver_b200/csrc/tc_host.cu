@@ -397,6 +397,7 @@ static int build_tables(Ctx & c, const domain_t * d) {
   // elements per lane) and start on 16-byte boundaries for paired loads
   const size_t LX = ((std::max(L, (size_t)32 * predict_warps(nx)) + 1) / 2) * 2;
   c.xf.stride = LX;
+  c.xf.ne = predict_warps(nx);   // the march kernel solves with E = its warp count elements per lane
   for (int v = 0; v < 4; v++) {
     c.xf.n[v] = (v == VUX) ? nx - 1 : nx;
     c.xf.lap_l[v] = dP + (size_t)v * 6 * L;

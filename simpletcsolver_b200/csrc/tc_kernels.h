@@ -125,9 +125,10 @@ struct XFactors {
   const double * lap_l[4];  // per-variable Laplacian coefficients, packed e = i - i0
   const double * lap_c[4];
   const double * lap_u[4];
-  double * lo;              // [12][stride]
-  double * w;
-  double * v;
+  double * lo;              // [12][stride], element e of a row at (e % ne) 32 + e / ne: the
+  double * w;               // ne elements a lane of the solving warp owns (e = lane ne + m)
+  double * v;               // are read with one coalesced load per m
+  int ne;                   // elements per lane of the radial solves (warps of the predict kernel)
 };
 
 // Periodic y / z factors (planar configuration with implicit y and z).

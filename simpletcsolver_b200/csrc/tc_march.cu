@@ -321,21 +321,14 @@ __device__ __forceinline__ int spad(int e) { return E > 1 ? e + e / E : e; }
 
 struct Aff { double a, b; };
 
-// Lane's chunk of a factor row: E consecutive values, as 16-byte pairs when
-// E > 1 (rows start 16-byte aligned and hold at least 32 E values).
+// Lane's chunk of a factor row: the E values of elements lane E .. lane E + E-1
+// (rows hold at least 32 E values).
 template <int E>
 __device__ __forceinline__ void load_chunk(double (&r)[E], const double * __restrict__ row, int lane) {
-  if constexpr (E == 1) {
-    r[0] = LD(row + lane);
-  } else {
-    const double2 * p2 = reinterpret_cast<const double2 *>(row + lane * E);
+  // rows are stored interleaved (element lane E + m at m 32 + lane): one
+  // coalesced 256-byte load per m
 #pragma unroll
-    for (int m = 0; m < E / 2; m++) {
-      const double2 t = __ldg(p2 + m);
-      r[2 * m] = t.x;
-      r[2 * m + 1] = t.y;
-    }
-  }
+  for (int m = 0; m < E; m++) r[m] = LD(row + m * 32 + lane);
 }
 
 // Radial Thomas solve of one line by one warp (src/tdm.c:24-48): lane t owns

@@ -18,7 +18,8 @@ namespace tcgpu {
 // (ux-x ux.c:502, uy-y uy.c:541, uz-z uz.c:451, t-y t.c:348).
 // Output per line family: lo[n] = l (lo[0] = 0), w[n] (w[0] = 1/c[0],
 // w[i] = 1/(c - l v)), v[n] (v[n-1] = 0), so every row of the forward sweep
-// reads q = w (r - l q_prev). Entries from n on stay zero.
+// reads q = w (r - l q_prev). Entries from n on stay zero. Rows are stored
+// interleaved for the warp that solves them (XFactors::ne).
 __global__ void xfactor_kernel(XFactors xf, const double * __restrict__ dtp, double nu, double kappa) {
   const int tid = threadIdx.x;
   if (tid >= 12) return;
@@ -34,24 +35,26 @@ __global__ void xfactor_kernel(XFactors xf, const double * __restrict__ dtp, dou
   double * lo = xf.lo + (size_t)(rk * 4 + var) * xf.stride;
   double * w = xf.w + (size_t)(rk * 4 + var) * xf.stride;
   double * v = xf.v + (size_t)(rk * 4 + var) * xf.stride;
+  const int ne = xf.ne;
   double vprev = 0.;
   for (int e = 0; e < n; e++) {
+    const int pe = (e % ne) * 32 + e / ne;   // interleaved position of element e
     const double l = -pf * ll[e];
     const double c = 1. - pf * lc[e];
     const double u = -pf * lu[e];
-    lo[e] = (e == 0) ? 0. : l;
+    lo[pe] = (e == 0) ? 0. : l;
     if (e == 0) {
-      w[0] = 1. / c;
+      w[pe] = 1. / c;
       vprev = u / c;
-      v[0] = (n > 1) ? vprev : 0.;
+      v[pe] = (n > 1) ? vprev : 0.;
     } else if (e < n - 1) {
       const double val = 1. / (c - l * vprev);
-      w[e] = val;
+      w[pe] = val;
       vprev = val * u;
-      v[e] = vprev;
+      v[pe] = vprev;
     } else {
-      w[e] = 1. / (c - l * vprev);
-      v[e] = 0.;
+      w[pe] = 1. / (c - l * vprev);
+      v[pe] = 0.;
     }
   }
 }
