@@ -91,7 +91,7 @@ def parse_args(argv=None):
                     help="steps of the FP32-storage vs FP64 accuracy runs (0: skip)")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure arm")
     ap.add_argument("--closure-pairs", type=int, default=48, help="training pairs from the fine run")
-    ap.add_argument("--closure-epochs", type=int, default=30)
+    ap.add_argument("--closure-epochs", type=int, default=60)
     ap.add_argument("--closure-warm", type=int, default=200,
                     help="fine steps before the first pair (lets the initial noise decay)")
     ap.add_argument("--closure-window", type=int, default=240,
