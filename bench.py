@@ -90,6 +90,7 @@ def parse_args(argv=None):
     ap.add_argument("--accuracy-steps", type=int, default=200,
                     help="steps of the FP32-storage vs FP64 accuracy runs (0: skip)")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure arm")
+    ap.add_argument("--no-planar", action="store_true", help="skip the planar-channel workload")
     ap.add_argument("--closure-pairs", type=int, default=48, help="training pairs from the fine run")
     ap.add_argument("--closure-epochs", type=int, default=60)
     ap.add_argument("--closure-warm", type=int, default=200,
@@ -354,6 +355,10 @@ def gpu_arm(args, rank, world, local):
         fp32 = fp32_storage_arm(args, lib, d0, case, world, peak, value)
         fp32["gpu_launches"] = fp32.pop("_launches")
 
+    planar = None
+    if not args.no_planar:
+        planar = planar_arm(args, lib, world, peak)
+
     clo = None
     if not args.no_closure and nx % 32 == 0 and ny % 64 == 0 and nz % 4 == 0:
         clo = closure_arm(args, lib, d0, case, peaks)
@@ -375,6 +380,7 @@ def gpu_arm(args, rank, world, local):
             "kernels": per_kernel,
             "fp32_storage": fp32,
             "closure": clo,
+            "planar": planar,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clk.summary(),
@@ -441,6 +447,38 @@ def fp32_storage_arm(args, lib, d0, case, world, peak, value64):
                         "rel_err": abs(tq32 - tq64) / abs(tq64)},
             "sim_time": {"fp64": a["time"], "fp32_storage": b["time"]},
         }
+    return out
+
+
+MODEL_BYTES_PER_CELL_STEP_PLANAR = 1512   # + y and z implicit solves and the increment round trip per substep
+
+
+def planar_arm(args, lib, world, peak):
+    """The planar channel workload (192x512x256, Re = 2000, Pr = 1, walls at
+    -0.5 / +0.5, scalar 1 / 0, implicit diffusion in x, y and z): device time
+    of K steps in FP64 and in the FP32-storage form, timed like the main arm."""
+    from simpletcsolver_b200 import abi, ic
+    from simpletcsolver_b200.solver import Solver
+    case = ic.PLANAR
+    d0 = ic.write_ic(case, os.path.join(tempfile.mkdtemp(prefix="tcplanar"), "ic"))
+    K, W = args.steps, args.warmup
+    out = {"workload": f"planar channel {case.nx}x{case.ny}x{case.nz} Re=2000 Pr=1 implicit xyz",
+           "steps": K, "bytes_per_cell_step_model": MODEL_BYTES_PER_CELL_STEP_PLANAR}
+    for storage, key in ((8, "fp64"), (4, "fp32_storage")):
+        s = Solver.from_ic(d0, case=case, lib=lib, storage=storage)
+        try:
+            s.set_coherence(abi.NO_COHERENCE)
+            s.push()
+            s.run(W)
+            ms, _, _ = run_timed(lib, s, K, 0)
+            elapsed, units = aggregate(ms / 1e3, case.ncells * K, world)
+            out[key] = {"value": units / elapsed / 1e6, "unit": UNIT, "ms_per_step": elapsed * 1e3 / K,
+                        "divmax": s.diagnostics()["divmax"]}
+            if storage == 8:
+                out[key]["step_model_frac"] = (MODEL_BYTES_PER_CELL_STEP_PLANAR * case.ncells / (ms / K / 1e3)
+                                               / 1e9 / peak)
+        finally:
+            s.release()
     return out
 
 

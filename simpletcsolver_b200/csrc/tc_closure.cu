@@ -163,8 +163,8 @@ struct ConvLayout {
   static constexpr int SLOTB = HY * ROWB;                // one halo plane
   static constexpr int WB = 27 * CIN * COUT * 2;         // packed BF16 weights
   static constexpr int HALO = WB;                        // halo slots after the weights
-  static constexpr int BAR = HALO + NSLOT_NN * SLOTB;    // mbarrier, then the TMEM address
-  static constexpr int BYTES = BAR + 16;
+  static constexpr int BAR = HALO + NSLOT_NN * SLOTB;    // two mbarriers, then the TMEM address
+  static constexpr int BYTES = BAR + 32;
 };
 
 struct ConvArgs {
@@ -197,22 +197,85 @@ __device__ __forceinline__ void load_halo(char * slot, const __nv_bfloat16 * in,
   }
 }
 
+// Two-stage pipeline over the planes of the chunk: the MMAs of plane z (into
+// accumulator z & 1) run while the warps drain the accumulator of plane z - 1
+// and the halo of plane z + 2 streams in (into the slot of plane z - 2, free
+// once the MMAs of z - 1 completed).
+#ifndef TC_CONV_NPART
+#define TC_CONV_NPART 1
+#endif
+// partial accumulators per plane: the taps alternate between them, so
+// consecutive MMAs do not accumulate into the same tensor-memory columns
+constexpr int NPART = TC_CONV_NPART;
+
+template <int CIN, int COUT, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tacc, int warp, size_t cell) {
+#pragma unroll
+  for (int h = 0; h < COUT / 16; h++) {
+    float v[16];
+    tmem_ld16(tacc + ((unsigned)(warp * 32) << 16) + h * 16, v);
+#pragma unroll
+    for (int pp = 1; pp < NPART; pp++) {
+      float w2[16];
+      tmem_ld16(tacc + ((unsigned)(warp * 32) << 16) + pp * 32 + h * 16, w2);
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] += w2[q];
+    }
+    if constexpr (EPI == EPI_LINEAR) {
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (h * 16 + q < A.nout) A.outf[cell * A.nout + h * 16 + q] = v[q] + A.bias[h * 16 + q];
+    } else {
+      alignas(16) __nv_bfloat16 o[16];
+      if constexpr (EPI == EPI_GELU) {
+        alignas(16) __nv_bfloat16 zp[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+          const float zv = v[q] + A.bias[h * 16 + q];
+          zp[q] = __float2bfloat16_rn(zv);
+          o[q] = __float2bfloat16_rn(gelu(zv));
+        }
+        if (A.pre) {
+          uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + h * 16);
+          dp[0] = reinterpret_cast<const uint4 *>(zp)[0];
+          dp[1] = reinterpret_cast<const uint4 *>(zp)[1];
+        }
+      } else {
+        alignas(16) __nv_bfloat16 zs[16];
+        const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + h * 16);
+        reinterpret_cast<uint4 *>(zs)[0] = sp[0];
+        reinterpret_cast<uint4 *>(zs)[1] = sp[1];
+#pragma unroll
+        for (int q = 0; q < 16; q++) o[q] = __float2bfloat16_rn(v[q] * gelu_grad(__bfloat162float(zs[q])));
+      }
+      uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + h * 16);
+      op[0] = reinterpret_cast<const uint4 *>(o)[0];
+      op[1] = reinterpret_cast<const uint4 *>(o)[1];
+    }
+  }
+}
+
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(NN_THREADS) conv3_kernel(ConvArgs A) {
   using L = ConvLayout<CIN, COUT>;
   extern __shared__ __align__(128) char smc[];
   char * wsm = smc;
   char * halo = smc + L::HALO;
-  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smc + L::BAR);
-  unsigned * tslot = reinterpret_cast<unsigned *>(smc + L::BAR + 8);
+  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smc + L::BAR);   // two
+  unsigned * tslot = reinterpret_cast<unsigned *>(smc + L::BAR + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nbx = A.nx / TX;
   const int x0 = (blockIdx.x % nbx) * TX, y0 = (blockIdx.x / nbx) * TY;
   const int z0 = blockIdx.y * A.zc, z1 = min(z0 + A.zc, A.nz);
 
-  if (warp == 0) tmem_alloc(tslot, 32);
+  // two planes x NPART accumulators of 32 columns, rounded up to the power of
+  // two an allocation takes
+  constexpr unsigned TCOLS = 64 * NPART <= 64 ? 64 : 64 * NPART <= 128 ? 128 : 256;
+  static_assert(NPART >= 1 && NPART <= 4, "1 to 4 partial accumulators");
+  if (warp == 0) tmem_alloc(tslot, TCOLS);
   if (tid == 0) {
-    nn_mbar_init(bar, 1);
+    nn_mbar_init(&bar[0], 1);
+    nn_mbar_init(&bar[1], 1);
     fence_barrier_init();
   }
   // weights (exact shared-memory image) and the first three halo planes
@@ -230,82 +293,66 @@ __global__ void __launch_bounds__(NN_THREADS) conv3_kernel(ConvArgs A) {
   constexpr uint32_t IDESC = instr_desc_bf16(128, COUT, 0, 0);
   const int m = warp * 32 + lane;                // accumulator row = TMEM lane of this thread
   const int xi = x0 + (m & 7), yj = y0 + (m >> 3);
+  unsigned phase[2] = {0u, 0u};
+  bool bad = false;
 
-  for (int z = z0, it = 0; z < z1; z++, it++) {
+  for (int z = z0, it = 0; z <= z1 && !bad; z++, it++) {
     const int r = z - z0 + 1;                    // plane z in slot r % 4
-    if (z + 2 <= z1) load_halo<CIN>(halo + ((r + 2) % NSLOT_NN) * L::SLOTB, A.in, A.nx, A.ny, x0, y0,
-                                       wrapi(z + 2, A.nz));
-    cp_commit();
-    cp_wait<1>();                                // planes up to z + 1 have landed
-    fence_proxy_async();                         // make them visible to the tensor cores
-    __syncthreads();
-    if (tid == 0) {
+    if (z < z1) {
+      // planes up to z + 1 have landed (plane z + 1 was the last group issued)
+      cp_wait<0>();
+      fence_proxy_async();                       // make them visible to the tensor cores
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const unsigned hb = su32(halo), wb = su32(wsm);
+        const unsigned dacc = tmem + (it & 1) * 32 * NPART;
+        // slot base of each of the three planes, then every tap's descriptors
+        // from compile-time offsets
+        const unsigned sb[3] = {hb + ((r - 1) % NSLOT_NN) * L::SLOTB, hb + (r % NSLOT_NN) * L::SLOTB,
+                                hb + ((r + 1) % NSLOT_NN) * L::SLOTB};
+#pragma unroll
+        for (int t = 0; t < 27; t++) {
+          const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+          const unsigned a0 = sb[dz + 1] + (1 + dy) * L::ROWB + (1 + dx) * 16;
+          const int pp = t % NPART;
+#pragma unroll
+          for (int kk = 0; kk < CIN / 16; kk++) {
+            const uint64_t ad = smem_desc(a0 + kk * 2 * L::CHB, L::CHB, L::ROWB);
+            const uint64_t bd = smem_desc(wb + (t * (CIN / 8) + 2 * kk) * COUT * 16, COUT * 16, 128);
+            mma_bf16(dacc + pp * 32, ad, bd, IDESC, t >= NPART || kk > 0);
+          }
+        }
+        mma_commit(&bar[it & 1]);
+      }
+    }
+    if (it > 0) {
+      // plane z - 1: its MMAs done, so the slot of plane z - 2 is free for z + 2
+      const int pb = (it - 1) & 1;
+      const bool ok = nn_mbar_wait(&bar[pb], phase[pb]);
+      phase[pb] ^= 1u;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
+        bad = true;
+        break;
+      }
       tc_fence_after();
-      const unsigned hb = su32(halo), wb = su32(wsm);
-#pragma unroll 1
-      for (int t = 0; t < 27; t++) {
-        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-        const unsigned a0 = hb + ((r + dz) % NSLOT_NN) * L::SLOTB + (1 + dy) * L::ROWB + (1 + dx) * 16;
-#pragma unroll
-        for (int kk = 0; kk < CIN / 16; kk++) {
-          const uint64_t ad = smem_desc(a0 + kk * 2 * L::CHB, L::CHB, L::ROWB);
-          const uint64_t bd = smem_desc(wb + (t * (CIN / 8) + 2 * kk) * COUT * 16, COUT * 16, 128);
-          mma_bf16(tmem, ad, bd, IDESC, t > 0 || kk > 0);
-        }
-      }
-      mma_commit(bar);
     }
-    const bool ok = nn_mbar_wait(bar, it & 1);
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
-      break;
-    }
-    tc_fence_after();
-    const size_t cell = ((size_t)z * A.ny + yj) * A.nx + xi;
-#pragma unroll
-    for (int h = 0; h < COUT / 16; h++) {
-      float v[16];
-      tmem_ld16(tmem + ((unsigned)(warp * 32) << 16) + h * 16, v);
-      if constexpr (EPI == EPI_LINEAR) {
-#pragma unroll
-        for (int q = 0; q < 16; q++)
-          if (h * 16 + q < A.nout) A.outf[cell * A.nout + h * 16 + q] = v[q] + A.bias[h * 16 + q];
-      } else {
-        alignas(16) __nv_bfloat16 o[16];
-        if constexpr (EPI == EPI_GELU) {
-          alignas(16) __nv_bfloat16 zp[16];
-#pragma unroll
-          for (int q = 0; q < 16; q++) {
-            const float zv = v[q] + A.bias[h * 16 + q];
-            zp[q] = __float2bfloat16_rn(zv);
-            o[q] = __float2bfloat16_rn(gelu(zv));
-          }
-          if (A.pre) {
-            uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + h * 16);
-            dp[0] = reinterpret_cast<const uint4 *>(zp)[0];
-            dp[1] = reinterpret_cast<const uint4 *>(zp)[1];
-          }
-        } else {
-          alignas(16) __nv_bfloat16 zs[16];
-          const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + h * 16);
-          reinterpret_cast<uint4 *>(zs)[0] = sp[0];
-          reinterpret_cast<uint4 *>(zs)[1] = sp[1];
-#pragma unroll
-          for (int q = 0; q < 16; q++) o[q] = __float2bfloat16_rn(v[q] * gelu_grad(__bfloat162float(zs[q])));
-        }
-        uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + h * 16);
-        op[0] = reinterpret_cast<const uint4 *>(o)[0];
-        op[1] = reinterpret_cast<const uint4 *>(o)[1];
-      }
+    if (z < z1 && z + 2 <= z1)
+      load_halo<CIN>(halo + ((r + 2) % NSLOT_NN) * L::SLOTB, A.in, A.nx, A.ny, x0, y0, wrapi(z + 2, A.nz));
+    cp_commit();
+    if (it > 0) {
+      const size_t cell = ((size_t)(z - 1) * A.ny + yj) * A.nx + xi;
+      conv_epilogue<CIN, COUT, EPI>(A, tmem + ((it - 1) & 1) * 32 * NPART, warp, cell);
     }
     tc_fence_before();
-    __syncthreads();                             // TMEM and the oldest slot free for the next plane
+    __syncthreads();                             // the drained accumulator may be written again
   }
   cp_wait<0>();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_free(tmem, 32);
+  if (warp == 0) tmem_free(tmem, TCOLS);
 }
 
 // ---- convolution: weight gradient -----------------------------------------
@@ -326,9 +373,10 @@ struct WgradLayout {
   static constexpr int ROWB = (CIN / 8) * CHB;
   static constexpr int SLOTB = HYW * ROWB;
   static constexpr int GB = TY * (COUT / 8) * TX * 16;   // gradient tile of one plane
-  static constexpr int GOFF = NSLOT_NN * SLOTB;          // two gradient slots after the halo ring
-  static constexpr int BAR = GOFF + 2 * GB;
-  static constexpr int USED = BAR + 16;
+  static constexpr int NSW = 5, NGS = 3;                 // halo and gradient slots: MMAs of two planes in flight
+  static constexpr int GOFF = NSW * SLOTB;               // gradient slots after the halo ring
+  static constexpr int BAR = GOFF + NGS * GB;            // two mbarriers, then the TMEM address
+  static constexpr int USED = BAR + 32;
   static constexpr int TCOLS = 9 * COUT > 256 ? 512 : 256;
   // one CTA per SM, so that its tensor-memory allocation never waits on
   // another CTA's: ask for more than half of the shared memory
@@ -374,14 +422,15 @@ __global__ void __launch_bounds__(NN_THREADS, 1) conv3_wgrad_kernel(WgradArgs A)
   extern __shared__ __align__(128) char smw[];
   char * halo = smw;
   char * gsl = smw + L::GOFF;
-  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smw + L::BAR);
-  unsigned * tslot = reinterpret_cast<unsigned *>(smw + L::BAR + 8);
+  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smw + L::BAR);   // two
+  unsigned * tslot = reinterpret_cast<unsigned *>(smw + L::BAR + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nbx = A.nx / TX, ncol = nbx * (A.ny / TY);
 
   if (warp == 0) tmem_alloc(tslot, L::TCOLS);
   if (tid == 0) {
-    nn_mbar_init(bar, 1);
+    nn_mbar_init(&bar[0], 1);
+    nn_mbar_init(&bar[1], 1);
     fence_barrier_init();
   }
   tc_fence_before();
@@ -391,37 +440,59 @@ __global__ void __launch_bounds__(NN_THREADS, 1) conv3_wgrad_kernel(WgradArgs A)
   constexpr uint32_t IDESC = instr_desc_bf16(128, COUT, 1, 1);
   float bsum = 0.f;                 // bias gradient of channel tid (tid < COUT)
   bool first = true;                // no accumulator written yet
-  unsigned phase = 0;
+  unsigned phase[2] = {0u, 0u};
+  int pending[2] = {0, 0};          // commits on each barrier not yet waited for
   bool bad = false;
+  // wait for the MMAs committed on barrier b (bounded)
+  auto drain = [&](int b) {
+    if (!pending[b]) return;
+    const bool ok = nn_mbar_wait(&bar[b], phase[b]);
+    phase[b] ^= 1u;
+    pending[b] = 0;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
+      bad = true;
+    }
+  };
 
+  // Per plane z: (a) the MMAs of plane z - 2 have finished (their barrier is
+  // the one plane z commits on), so the halo slot of z + 2 and the gradient
+  // slot of z + 1 are free; (b) issue those copies; (c) wait for the planes up
+  // to z + 1 and the tile of z; (d) issue the plane's 72 MMAs; the MMAs of
+  // z - 1 and z overlap the copies of the next planes.
   for (int item = blockIdx.x; item < A.nitems && !bad; item += gridDim.x) {
     const int col = item % ncol, zch = item / ncol;
     const int x0 = (col % nbx) * TX, y0 = (col / nbx) * TY;
     const int z0 = zch * A.zc, z1 = min(z0 + A.zc, A.nz);
+    drain(0);
+    drain(1);
+    if (bad) break;
     load_halo_w<CIN>(halo + 0 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, wrapi(z0 - 1, A.nz), L::HYW);
-    cp_commit();
     load_halo_w<CIN>(halo + 1 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, z0, L::HYW);
-    load_grad_tile<COUT>(gsl + L::GB, A.dy, A.nx, A.ny, x0, y0, z0);   // plane z0 uses slot 1
-    cp_commit();
     load_halo_w<CIN>(halo + 2 * L::SLOTB, A.x, A.nx, A.ny, x0, y0, wrapi(z0 + 1, A.nz), L::HYW);
+    load_grad_tile<COUT>(gsl + 1 * L::GB, A.dy, A.nx, A.ny, x0, y0, z0);   // tile of plane z in slot r % 3
     cp_commit();
-    for (int z = z0; z < z1; z++) {
+    for (int z = z0, it = 0; z < z1; z++, it++) {
       const int r = z - z0 + 1;
-      if (z + 2 <= z1) load_halo_w<CIN>(halo + ((r + 2) % NSLOT_NN) * L::SLOTB, A.x, A.nx, A.ny, x0, y0,
+      drain(it & 1);
+      if (bad) break;
+      if (z + 2 <= z1) load_halo_w<CIN>(halo + ((r + 2) % L::NSW) * L::SLOTB, A.x, A.nx, A.ny, x0, y0,
                                         wrapi(z + 2, A.nz), L::HYW);
-      if (z + 1 < z1) load_grad_tile<COUT>(gsl + ((r + 1) & 1) * L::GB, A.dy, A.nx, A.ny, x0, y0, z + 1);
+      if (z + 1 < z1) load_grad_tile<COUT>(gsl + ((r + 1) % L::NGS) * L::GB, A.dy, A.nx, A.ny, x0, y0, z + 1);
       cp_commit();
       cp_wait<1>();
       fence_proxy_async();
       __syncthreads();
-      const char * g = gsl + (r & 1) * L::GB;
+      const char * g = gsl + (r % L::NGS) * L::GB;
       if (tid == 0) {
         tc_fence_after();
         const unsigned hb = su32(halo), gb = su32(g);
-#pragma unroll 1
+        const unsigned sb[3] = {hb + ((r - 1) % L::NSW) * L::SLOTB, hb + (r % L::NSW) * L::SLOTB,
+                                hb + ((r + 1) % L::NSW) * L::SLOTB};
+#pragma unroll
         for (int a = 0; a < 9; a++) {
           const int dz = a / 3 - 1, dx = a % 3 - 1;
-          const unsigned a0 = hb + ((r + dz) % NSLOT_NN) * L::SLOTB + (1 + dx) * 16;
+          const unsigned a0 = sb[dz + 1] + (1 + dx) * 16;
 #pragma unroll
           for (int s = 0; s < TY / 2; s++) {
             const uint64_t ad = smem_desc(a0 + 2 * s * L::ROWB, L::ROWB, L::CHB);
@@ -429,8 +500,9 @@ __global__ void __launch_bounds__(NN_THREADS, 1) conv3_wgrad_kernel(WgradArgs A)
             mma_bf16(tmem + a * COUT, ad, bd, IDESC, !(first && s == 0));
           }
         }
-        mma_commit(bar);
+        mma_commit(&bar[it & 1]);
       }
+      pending[it & 1] = 1;
       if (tid < COUT) {   // bias gradient from the same tile
         constexpr int CC = COUT / 8;
         const __nv_bfloat16 * gv = reinterpret_cast<const __nv_bfloat16 *>(g);
@@ -442,19 +514,14 @@ __global__ void __launch_bounds__(NN_THREADS, 1) conv3_wgrad_kernel(WgradArgs A)
         bsum += acc;
       }
       first = false;
-      const bool ok = nn_mbar_wait(bar, phase);
-      phase ^= 1u;
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
-        bad = true;
-        break;
-      }
       tc_fence_before();
-      __syncthreads();   // slots of plane z - 1 and of this gradient tile may be refilled
+      __syncthreads();
     }
     cp_wait<0>();
     __syncthreads();
   }
+  drain(0);
+  drain(1);
   tc_fence_after();
   // raw partial sums of this CTA: [a][m][co]
   float * dst = A.part + (size_t)blockIdx.x * 9 * 128 * COUT;
