@@ -581,6 +581,11 @@ def closure_arm(args, lib, d0, case, peaks):
                 "rel_err_closure": abs(tq_c - tq_f) / abs(tq_f), "rel_err_plain": abs(tq_p - tq_f) / abs(tq_f),
                 "rel_err_closure_vs_restricted": abs(tq_c - tq_r) / abs(tq_r),
                 "rel_err_plain_vs_restricted": abs(tq_p - tq_r) / abs(tq_r),
+                # the coarse grid's wall-gradient estimator calibrated once, at the
+                # window start, by the ratio fine / restricted-fine torque
+                "estimator_calibration": fq[0] / rq[0],
+                "rel_err_closure_calibrated": abs(tq_c * fq[0] / rq[0] - tq_f) / abs(tq_f),
+                "rel_err_plain_calibrated": abs(tq_p * fq[0] / rq[0] - tq_f) / abs(tq_f),
                 "mean_uy_profile_rel_err": {"closure": perr(prof["closure"]), "plain": perr(prof["plain"])},
                 "wall_s_fine": fine_s, "wall_s_coarse_closure": coarse_s,
                 "speedup_vs_fine": (fine_s / ft[-1]) / (coarse_s / max(at[-1], 1e-30)),
