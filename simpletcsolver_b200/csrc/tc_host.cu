@@ -496,6 +496,15 @@ static int build_tables(Ctx & c, const domain_t * d) {
   c.ps.spec = valloc(c, nspec * c.ps.spec_bytes);
   c.ps.vscr = dalloc(c, nspec);
   if (!c.ps.tw_y || !c.ps.tw_z || !c.ps.spec || !c.ps.vscr) return fail("cudaMalloc of Poisson buffers failed");
+  // radial solves by warps when nx = 32 E: per-line factors computed once
+  c.ps.fe = (nx == 64 || nx == 128 || nx == 256) ? nx / 32 : 0;
+  if (c.ps.fe) {
+    c.ps.fw = dalloc(c, nspec);
+    c.ps.fv = c.ps.vscr;   // not otherwise used on this path
+    if (!c.ps.fw) return fail("cudaMalloc of Poisson buffers failed");
+    launch_tdm_factors(c.g, c.ps, c.tab_y, c.tab_z, c.base, c.st);
+    CK(cudaGetLastError());
+  }
   return 0;
 }
 

@@ -162,6 +162,14 @@ struct Poisson {
   void * spec;              // [nx][nz][nyh] complex spectra: double2, or float2 (spec_bytes 8)
   int spec_bytes;           // 16 or 8 per complex value
   double * vscr;            // [nx][nz][nyh] elimination factors
+  // Radial solves by warps over tiles of lines (nx = 32 fe, fe in {2, 4, 8}):
+  // the factors of every line (kz, m) computed once per context, since the
+  // Poisson matrix does not change; [line][nx] with element i at
+  // (i % fe) 32 + i / fe (the fe elements a lane owns arrive coalesced).
+  // fe = 0: the per-column kernel with factors from each call.
+  int fe;
+  double * fw;              // multipliers of the forward sweep
+  double * fv;              // back-substitution factors
   const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny
   const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz
   const double * tl;        // radial l_i (compute_potential.c:197-200), length nx
@@ -230,6 +238,9 @@ void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const F
                     const double * tab_y, const double * tab_z, const double * base,
                     const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm = PoissonMarks());
 void poisson_smem_limits();
+// per-line factors of the warp radial solves (Poisson::fe > 0), once per context
+void launch_tdm_factors(const Geo & g, const Poisson & ps, const double * tab_y, const double * tab_z,
+                        const double * base, cudaStream_t st);
 enum { CORRECT_VELOCITY = 1, CORRECT_PRESSURE = 2 };
 // cfl_dtmin: when non-null (velocity and pressure together), the advective
 // time-step limit of the corrected velocities is folded into it

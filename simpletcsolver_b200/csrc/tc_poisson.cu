@@ -539,6 +539,171 @@ tdm_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y, const double * 
   }
 }
 
+// ---------------------------------------------------- radial solves by warps
+// Factors of line l = kz nyh + m (the forward elimination of src/tdm.c:24-44
+// with the Neumann ends folded into the diagonal, as in tdm_kernel): the
+// forward sweep y_i = w_i (q_i - l_i y_{i-1}), y_{-1} = 0, and the back
+// substitution x_i = y_i - v_i x_{i+1}, x_n = 0 (v_{n-1} = 0). The pinned mode
+// (line 0) has w_{n-1} = 0, which sets its last unknown to zero.
+__global__ void tdm_factor_kernel(Geo g, Poisson ps, const double * __restrict__ tab_y,
+                                  const double * __restrict__ tab_z, const double * __restrict__ base) {
+  const int nyh = ps.nyh, nz = g.nz, n = g.nx, fe = ps.fe;
+  const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= (long long)nyh * nz) return;
+  const int m = (int)(l % nyh), kz = (int)(l / nyh);
+  const double tz = tab_z[kz];
+  auto cdiag = [&](int i) {
+    double c = base[i] + tab_y[(size_t)i * nyh + m] + tz;
+    if (i == 0) c += ps.tl[0];
+    if (i == n - 1) c += ps.tu[n - 1];
+    return c;
+  };
+  double * w = ps.fw + (size_t)l * n;
+  double * v = ps.fv + (size_t)l * n;
+  auto at = [&](int i) { return (i % fe) * 32 + i / fe; };
+  const double c0 = cdiag(0);
+  double vprev = ps.tu[0] / c0;
+  w[at(0)] = 1. / c0;
+  v[at(0)] = vprev;
+  for (int i = 1; i < n - 1; i++) {
+    const double val = 1. / (cdiag(i) - ps.tl[i] * vprev);
+    vprev = val * ps.tu[i];
+    w[at(i)] = val;
+    v[at(i)] = vprev;
+  }
+  const double last = cdiag(n - 1) - ps.tl[n - 1] * vprev;
+  w[at(n - 1)] = (l == 0) ? 0. : 1. / last;
+  v[at(n - 1)] = 0.;
+}
+
+void launch_tdm_factors(const Geo & g, const Poisson & ps, const double * tab_y, const double * tab_z,
+                        const double * base, cudaStream_t st) {
+  const long long nl = (long long)ps.nyh * g.nz;
+  tdm_factor_kernel<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+}
+
+// The radial systems of 16 consecutive lines (kz, m) as one tile: for every i
+// their 16 complex values are contiguous (256 bytes), loaded and stored once;
+// each warp solves whole lines from shared memory with the affine-map scans
+// (E = n / 32 points per lane, in-register prefix + 5-level shuffle scan).
+constexpr int TDM_PT = 16;
+
+template <int E, class Z>
+__global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
+  constexpr int N = 32 * E, NT = 256, PER = N * TDM_PT / NT;
+  extern __shared__ double2 tq[];
+  const int nyh = ps.nyh;
+  const long long nlines = (long long)nyh * g.nz;
+  const long long l0 = (long long)blockIdx.x * TDM_PT;
+  const int nt = (int)min((long long)TDM_PT, nlines - l0);
+  const size_t st = (size_t)nlines;               // complex values between radial indices
+  Z * spec = static_cast<Z *>(ps.spec);
+  {
+    double2 buf[PER];
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+      const int q = threadIdx.x + r * NT, t = q % TDM_PT, i = q / TDM_PT;
+      buf[r] = t < nt ? zget(spec + (size_t)i * st + l0 + t) : make_double2(0., 0.);
+    }
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+      const int q = threadIdx.x + r * NT, t = q % TDM_PT, i = q / TDM_PT;
+      tq[i * TDM_PT + (t ^ ((i / E) & (TDM_PT - 1)))] = buf[r];
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double ll[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) ll[e] = ps.tl[lane * E + e];
+  for (int t = wid; t < nt; t += NT / 32) {
+    const long long l = l0 + t;
+    const double * w = ps.fw + (size_t)l * N;
+    const double * v = ps.fv + (size_t)l * N;
+    const int sw = t ^ (lane & (TDM_PT - 1));
+    double fa[E], bre[E], bim[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double2 qv = tq[(lane * E + e) * TDM_PT + sw];
+      const double we = w[e * 32 + lane];
+      fa[e] = -we * ll[e];
+      bre[e] = we * qv.x;
+      bim[e] = we * qv.y;
+    }
+    // forward: prefix of the lane's maps, then across lanes
+#pragma unroll
+    for (int d = 1; d < E; d <<= 1) {
+#pragma unroll
+      for (int e = E - 1; e >= d; e--) {
+        bre[e] = fa[e] * bre[e - d] + bre[e];
+        bim[e] = fa[e] * bim[e - d] + bim[e];
+        fa[e] = fa[e] * fa[e - d];
+      }
+    }
+    double A = fa[E - 1], Bre = bre[E - 1], Bim = bim[E - 1];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double oa = __shfl_up_sync(0xffffffffu, A, off);
+      const double ore = __shfl_up_sync(0xffffffffu, Bre, off);
+      const double oim = __shfl_up_sync(0xffffffffu, Bim, off);
+      if (lane >= off) { Bre = A * ore + Bre; Bim = A * oim + Bim; A = A * oa; }
+    }
+    double yre = __shfl_up_sync(0xffffffffu, Bre, 1), yim = __shfl_up_sync(0xffffffffu, Bim, 1);
+    if (lane == 0) { yre = 0.; yim = 0.; }
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      bre[e] = fa[e] * yre + bre[e];
+      bim[e] = fa[e] * yim + bim[e];
+    }
+    // backward: x_i = y_i - v_i x_{i+1}, suffix maps
+#pragma unroll
+    for (int e = 0; e < E; e++) fa[e] = -v[e * 32 + lane];
+#pragma unroll
+    for (int d = 1; d < E; d <<= 1) {
+#pragma unroll
+      for (int e = 0; e + d < E; e++) {
+        bre[e] = fa[e] * bre[e + d] + bre[e];
+        bim[e] = fa[e] * bim[e + d] + bim[e];
+        fa[e] = fa[e] * fa[e + d];
+      }
+    }
+    A = fa[0];
+    Bre = bre[0];
+    Bim = bim[0];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double oa = __shfl_down_sync(0xffffffffu, A, off);
+      const double ore = __shfl_down_sync(0xffffffffu, Bre, off);
+      const double oim = __shfl_down_sync(0xffffffffu, Bim, off);
+      if (lane + off < 32) { Bre = A * ore + Bre; Bim = A * oim + Bim; A = A * oa; }
+    }
+    double xre = __shfl_down_sync(0xffffffffu, Bre, 1), xim = __shfl_down_sync(0xffffffffu, Bim, 1);
+    if (lane == 31) { xre = 0.; xim = 0.; }
+#pragma unroll
+    for (int e = 0; e < E; e++)
+      tq[(lane * E + e) * TDM_PT + sw] = make_double2(fa[e] * xre + bre[e], fa[e] * xim + bim[e]);
+  }
+  __syncthreads();
+#pragma unroll 8
+  for (int r = 0; r < PER; r++) {
+    const int q = threadIdx.x + r * NT, t = q % TDM_PT, i = q / TDM_PT;
+    if (t < nt) zput(spec + (size_t)i * st + l0 + t, tq[i * TDM_PT + (t ^ ((i / E) & (TDM_PT - 1)))]);
+  }
+}
+
+template <class Z>
+static bool launch_tdm_lines(const Geo & g, const Poisson & ps, cudaStream_t st) {
+  const long long nl = (long long)ps.nyh * g.nz;
+  const unsigned nblk = (unsigned)((nl + TDM_PT - 1) / TDM_PT);
+  const size_t smem = sizeof(double2) * (size_t)g.nx * TDM_PT;
+  switch (ps.fe) {
+    case 2: tdm_lines_kernel<2, Z><<<nblk, 256, smem, st>>>(g, ps); return true;
+    case 4: tdm_lines_kernel<4, Z><<<nblk, 256, smem, st>>>(g, ps); return true;
+    case 8: tdm_lines_kernel<8, Z><<<nblk, 256, smem, st>>>(g, ps); return true;
+    default: return false;
+  }
+}
+
 // --------------------------------------------------------------- inverse y
 template <int EPT, class Z>
 __global__ void __launch_bounds__(TC_FFTY_THREADS, TC_IFFTY_MIN_BLOCKS)
@@ -632,8 +797,10 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
   fftz_kernel<EPTZ, -1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   mark(pm.k_fwd);
-  const long long nl = (long long)ps.nyh * g.nz;
-  tdm_kernel<Z><<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+  if (!launch_tdm_lines<Z>(g, ps, st)) {
+    const long long nl = (long long)ps.nyh * g.nz;
+    tdm_kernel<Z><<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
+  }
   mark(pm.k_tdm);
   fftz_kernel<EPTZ, +1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   mark(pm.k_inv);
@@ -696,6 +863,10 @@ static void poisson_smem_limits_s() {
 void poisson_smem_limits() {
   poisson_smem_limits_s<double, double2>();
   poisson_smem_limits_s<float, float2>();
+  allow_dyn_smem(tdm_lines_kernel<8, double2>);
+  allow_dyn_smem(tdm_lines_kernel<8, float2>);
+  allow_dyn_smem(tdm_lines_kernel<4, double2>);
+  allow_dyn_smem(tdm_lines_kernel<4, float2>);
 }
 
 }  // namespace tcgpu

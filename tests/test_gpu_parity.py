@@ -29,6 +29,8 @@ CASES = {
     "planar": ic.plane_couette(12, 16, 8, 2000.0),
     # y and z lines of 64 and 128 points: the warp-per-line periodic solves
     "planar_lines": ic.plane_couette(12, 64, 128, 2000.0),
+    # 64 radial points: the Poisson radial solves by warps over tiles of lines
+    "tc_radial64": ic.taylor_couette(64, 16, 8, 3400.0),
 }
 
 
