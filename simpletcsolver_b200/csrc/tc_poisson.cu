@@ -33,6 +33,9 @@
 // y transforms (divergence + forward, inverse): elements per thread and
 // threads per CTA. Measured at 256 x 1024 x 512 (ms, divergence + forward /
 // inverse): 16 / 256 1.32 / 0.96; 8 / 512 1.59-1.68 / 1.02; 8 / 256 1.68 / 0.97.
+#ifndef TC_FFT_SMEM_MAX
+#define TC_FFT_SMEM_MAX (80 * 1024)   // dynamic shared memory the FFT kernels may ask for
+#endif
 #ifndef TC_FFTY_EPT
 #define TC_FFTY_EPT 16
 #endif
@@ -840,7 +843,7 @@ void launch_poisson(const Geo & g, const Coefs & cf, const Poisson & ps, const F
 
 template <typename K>
 static void allow_dyn_smem(K kernel) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_FFT_SMEM_MAX);
 }
 
 template <class T, class Z>
