@@ -203,12 +203,12 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
     e += q.h1 * sm * sm + q.h2 * sp * sp;
     // cross diffusion (:266-375): diffusion_y1 and the uy part of diffusion_a
     // as differences of uy across j, the ux part of diffusion_a, diffusion_z1
-    e += nu * (q.cy1 * (uy_m1 - uy_m0) + q.cy2 * (uy_01 - uy_00) + q.ca1 * (ux_m + ux_0) +
-               q.ca2 * (ux_0 + ux_p) + q.cz1 * ((uz_01 - uz_m1) - (uz_00 - uz_m0)));
+    e += q.cy1 * (uy_m1 - uy_m0) + q.cy2 * (uy_01 - uy_00) + q.ca1 * (ux_m + ux_0) +
+         q.ca2 * (ux_0 + ux_p) + q.cz1 * ((uz_01 - uz_m1) - (uz_00 - uz_m0));   // coefficients carry nu
     // pressure gradient (:377-394)
     gi = -q.px * (PP(0, 0) - PP(-1, 0));
-    ROUTE(ix, 2. * nu * (q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p));
-    ROUTE(iy, nu * (q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp));
+    ROUTE(ix, q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p);          // carries 2 nu
+    ROUTE(iy, q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp);          // carries nu
     ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUX][qf];   // closure forcing
     ss.new_[VUX][qf] = (T)e;
@@ -223,8 +223,8 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
     e = q.tx0 * ux_0 * (tim - t_0) - q.tx1 * ux_p * (tip - t_0);
     e += q.ty * uy_00 * (tjm - t_0) - q.ty * uy_01 * (tjp - t_0);
     e += q.tz * uz_00 * (tkm - t_0) - q.tz * uz_01 * (tkp - t_0);
-    ROUTE(ix, kappa * (q.clxl * tim + q.clxc * t_0 + q.clxu * tip));
-    ROUTE(iy, kappa * (q.clyl * tjm + q.clyc * t_0 + q.clyu * tjp));
+    ROUTE(ix, q.clxl * tim + q.clxc * t_0 + q.clxu * tip);            // carry kappa
+    ROUTE(iy, q.clyl * tjm + q.clyc * t_0 + q.clyu * tjp);
     ROUTE(iz, kappa * (cf.lz_l * tkm + cf.lz_c * t_0 + cf.lz_u * tkp));
     ss.new_[VT][qc] = (T)e;
     dl[1] = ca * e + cb * old_t + cg * gi;
@@ -264,11 +264,11 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     e -= q.h * ((uy_jm + uy_0) * (ux_0m + ux_1m) + (uy_0 + uy_jp) * (ux_0 + ux_1));
     // diffusion_x1 + diffusion_a (lyx at faces i, i+1 and lxy), diffusion_y1
     // (lyy1 at j-1, j), diffusion_z1 (lyz at k, k+1)
-    e += nu * (q.p1 * (ux_0 - ux_0m) + q.p2 * (ux_1 - ux_1m) + q.qm * uy_im + q.q0 * uy_0 + q.qp * uy_ip +
-               q.yk * ((ux_0 + ux_1) - (ux_0m + ux_1m)) + q.yz * ((uz_kp - uz_jmkp) - (uz_0 - uz_jm)));
+    e += q.p1 * (ux_0 - ux_0m) + q.p2 * (ux_1 - ux_1m) + q.qm * uy_im + q.q0 * uy_0 + q.qp * uy_ip +
+         q.yk * ((ux_0 + ux_1) - (ux_0m + ux_1m)) + q.yz * ((uz_kp - uz_jmkp) - (uz_0 - uz_jm));   // carry nu
     gi = -q.py * (p_0 - PP(0, -1));
-    ROUTE(ix, nu * (q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip));
-    ROUTE(iy, 2. * nu * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
+    ROUTE(ix, q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip);          // carry nu
+    ROUTE(iy, 2. * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
     ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUY][qc];
     ss.new_[VUY][qc] = (T)e;
@@ -285,10 +285,10 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     e += q.b * (uy_km + uy_0) * (uz_jm - uz_0) - q.b * (uy_jpkm + uy_jp) * (uz_jp - uz_0);
     e += q.c * (uz_km + uz_0) * (uz_km - uz_0) - q.c * (uz_0 + uz_kp) * (uz_kp - uz_0);
     // diffusion_x1 (lzx at faces i, i+1), diffusion_y1 (lzy at j, j+1)
-    e += nu * (q.zx1 * (ux_1 - ux_1k) - q.zx0 * (ux_0 - ux_0k) + q.zy * ((uy_jp - uy_jpkm) - (uy_0 - uy_km)));
+    e += q.zx1 * (ux_1 - ux_1k) - q.zx0 * (ux_0 - ux_0k) + q.zy * ((uy_jp - uy_jpkm) - (uy_0 - uy_km));   // carry nu
     gi = -cf.inv_hz * (p_0 - pv.p0);
-    ROUTE(ix, nu * (q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip));
-    ROUTE(iy, nu * (q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp));
+    ROUTE(ix, q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip);
+    ROUTE(iy, q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp);
     ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUZ][qc];
     ss.new_[VUZ][qc] = (T)e;
@@ -509,6 +509,22 @@ __device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring,
   CoefB qb;
   if constexpr (GA) load_coefs(qa, A.cf, act ? i : 1);
   if constexpr (GB) load_coefs(qb, A.cf, act ? i : 1);
+  // the diffusivities folded into the per-thread coefficients once, so the
+  // cell updates multiply by them no more (the z Laplacian, a shared scalar
+  // set, keeps its factor)
+  if constexpr (GA) {
+    const double nu = A.nu, n2 = 2. * A.nu, ka = A.kappa;
+    qa.lxl *= n2; qa.lxc *= n2; qa.lxu *= n2;
+    qa.lyl *= nu; qa.lyc *= nu; qa.lyu *= nu;
+    qa.cy1 *= nu; qa.cy2 *= nu; qa.ca1 *= nu; qa.ca2 *= nu; qa.cz1 *= nu;
+    qa.clxl *= ka; qa.clxc *= ka; qa.clxu *= ka; qa.clyl *= ka; qa.clyc *= ka; qa.clyu *= ka;
+  }
+  if constexpr (GB) {
+    const double nu = A.nu;
+    qb.lxl *= nu; qb.lxc *= nu; qb.lxu *= nu; qb.lyl *= nu; qb.lyc *= nu; qb.lyu *= nu;
+    qb.p1 *= nu; qb.p2 *= nu; qb.qm *= nu; qb.q0 *= nu; qb.qp *= nu; qb.yk *= nu; qb.yz *= nu;
+    qb.zx0 *= nu; qb.zx1 *= nu; qb.zy *= nu;
+  }
   const int rk = A.rkstep;
   const double ca = rk_alpha(rk) * dt, cb = rk_beta(rk) * dt, cg = rk_gamma(rk) * dt;
 
