@@ -517,7 +517,8 @@ def closure_arm(args, lib, d0, case, peaks):
         before = closure.relative_error(net, data, held)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hist = closure.train(net, data, train, epochs=args.closure_epochs, batch=4, lr=2e-3)
+        batch = 4
+        hist = closure.train(net, data, train, epochs=args.closure_epochs, batch=batch, lr=2e-3)
         train_s = time.perf_counter() - t0
         err_train = closure.relative_error(net, data, train)
         err_held = closure.relative_error(net, data, held)
@@ -568,7 +569,7 @@ def closure_arm(args, lib, d0, case, peaks):
         perr = lambda a: float(np.linalg.norm(a - prof["restricted_fine"]) / np.linalg.norm(prof["restricted_fine"]))
         out.update({
             "pairs": n, "pair_gap_fine_steps": 8, "generate_s": gen_s,
-            "training": {"epochs": args.closure_epochs, "samples": len(train), "batch": 8, "seconds": train_s,
+            "training": {"epochs": args.closure_epochs, "samples": len(train), "batch": batch, "seconds": train_s,
                          "loss_first": hist[0], "loss_last": hist[-1]},
             "apriori_rel_error": {"no_closure": 1.0, "train": err_train, "held_out": err_held,
                                   "held_out_untrained": before},
