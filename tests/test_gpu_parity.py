@@ -31,6 +31,9 @@ CASES = {
     "planar_lines": ic.plane_couette(12, 64, 128, 2000.0),
     # 64 radial points: the Poisson radial solves by warps over tiles of lines
     "tc_radial64": ic.taylor_couette(64, 16, 8, 3400.0),
+    # 128 and 256 radial points: predict kernels of 4 and 8 warps per line, Poisson solves with 4 and 8 points per lane
+    "tc_radial128": ic.taylor_couette(128, 16, 8, 1.0e4),
+    "tc_radial256": ic.taylor_couette(256, 16, 8, 1.0e4),
 }
 
 
