@@ -275,6 +275,13 @@ int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]);
 int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, bool is_complex, const double * l,
                             const double * c, const double * u, double * data);
 
+/* Self-test of the bounded waits inside the kernels. No counterpart in the
+ * reference. Runs one block whose mbarrier wait can never complete (it expects
+ * bytes no copy delivers): the wait must give up after its limit (about two
+ * seconds of SM clock), the kernel report it and return, and the device stay
+ * usable. Returns 0 when that happened; *seconds (if not NULL) = elapsed time. */
+int tcgpu_selftest_wait(double * seconds);
+
 /* free the device state that belongs to this fluid_t */
 int tcgpu_release(fluid_t * fluid);
 

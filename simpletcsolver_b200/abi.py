@@ -95,6 +95,7 @@ _EXT_SIGS = {
     "tcgpu_set_storage": (C.c_int, [C.c_int]),
     "tcgpu_get_storage": (C.c_int, [C.POINTER(FluidT)]),
     "tcgpu_last_error": (C.c_char_p, []),
+    "tcgpu_selftest_wait": (C.c_int, [c_double_p]),
     "tcgpu_stream": (C.c_void_p, [C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_coarsen": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_closure_input": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 3, C.c_int, C.c_void_p]),

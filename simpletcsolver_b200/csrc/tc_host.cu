@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <string>
@@ -1098,6 +1099,29 @@ int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
   CK(cudaMemcpyAsync(c->h_scalar, c->diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
   if (finish(*c, "tcgpu_diagnostics")) return 1;
   memcpy(out, c->h_scalar, 9 * sizeof(double));
+  return 0;
+}
+
+int tcgpu_selftest_wait(double * seconds) {
+  unsigned * d = nullptr;
+  unsigned h = 0;
+  cudaStream_t st = nullptr;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  if (cudaMalloc(&d, sizeof(unsigned)) != cudaSuccess) {
+    cudaStreamDestroy(st);
+    return fail("tcgpu_selftest_wait: cudaMalloc failed");
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaMemsetAsync(d, 0, sizeof(unsigned), st);
+  launch_wait_selftest(d, st);
+  cudaMemcpyAsync(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  const auto t1 = std::chrono::steady_clock::now();
+  cudaFree(d);
+  cudaStreamDestroy(st);
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  if (e != cudaSuccess) return fail("tcgpu_selftest_wait: %s", cudaGetErrorString(e));
+  if (!(h & ST_TIMEOUT)) return fail("tcgpu_selftest_wait: the wait did not report giving up");
   return 0;
 }
 

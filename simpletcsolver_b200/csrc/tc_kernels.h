@@ -220,6 +220,8 @@ void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const 
                           const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
                           cudaStream_t st);
 void march_smem_limits();
+// one CTA whose mbarrier wait can never complete: sets ST_TIMEOUT in *status
+void launch_wait_selftest(unsigned * status, cudaStream_t st);
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);
 void launch_apply(const Geo & g, const Bc & bc, const FieldBufs & in, const FieldBufs & out, const DeltaSet & ds,
                   cudaStream_t st);

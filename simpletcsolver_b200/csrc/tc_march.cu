@@ -814,6 +814,24 @@ void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const 
   else launch_march_t<double>(g, bc, cf, xf, nu, kappa, in, out, ss, ds, dtp, rkstep, mode, status, st);
 }
 
+// Self-test of the bounded waits: an mbarrier expects 16 bytes that no copy
+// will ever deliver; every thread's wait must give up after kWaitCycles and the
+// kernel report ST_TIMEOUT and return (the same wait the predict kernel uses).
+__global__ void wait_selftest_kernel(unsigned * status) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);   // the only arrival; its bytes never come
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(status, ST_TIMEOUT);
+}
+
+void launch_wait_selftest(unsigned * status, cudaStream_t st) { wait_selftest_kernel<<<1, 64, 0, st>>>(status); }
+
 void march_smem_limits() {
   allow_march_smem<1, double>();
   allow_march_smem<2, double>();
