@@ -33,6 +33,12 @@
 // y transforms (divergence + forward, inverse): elements per thread and
 // threads per CTA. Measured at 256 x 1024 x 512 (ms, divergence + forward /
 // inverse): 16 / 256 1.32 / 0.96; 8 / 512 1.59-1.68 / 1.02; 8 / 256 1.68 / 0.97.
+#ifndef TC_DIV_UNROLL
+#define TC_DIV_UNROLL 4     // rows of the divergence loads in flight per thread
+#endif
+#ifndef TC_IFFTY_UNROLL
+#define TC_IFFTY_UNROLL 4   // spectrum loads in flight per thread, inverse y transform
+#endif
 #ifndef TC_FFT_SMEM_MAX
 #define TC_FFT_SMEM_MAX (80 * 1024)   // dynamic shared memory the FFT kernels may ask for
 #endif
@@ -63,6 +69,8 @@
 #endif
 
 namespace tcgpu {
+
+constexpr int kDivUnroll = TC_DIV_UNROLL, kIfftyUnroll = TC_IFFTY_UNROLL;
 
 // spectral values as stored: double2, or float2 in the FP32-storage mode
 // (arithmetic in double either way)
@@ -374,7 +382,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
       const T * __restrict__ pzm = uz + sidx_c<T>(g, i, 0, k);
       const T * __restrict__ pzp = uz + sidx_c<T>(g, i, 0, k + 1);
       const int sf = srow_f<T>(g), sc = srow_c<T>(g);
-#pragma unroll 8
+#pragma unroll kDivUnroll
       for (int r = 0; r < 2 * EPT; r++) {
         const int j = j0 + r * jstep;
         const double ux_xm = __ldg(pxm + (size_t)j * sf);
@@ -719,7 +727,7 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
   // Hermitian extension of the two packed real lines
-#pragma unroll 8
+#pragma unroll kIfftyUnroll
   for (int r = 0; r < EPT; r++) {
     const int idx = threadIdx.x + r * blockDim.x;
     const int m = idx & (ny - 1);
