@@ -89,21 +89,33 @@ __device__ inline void warp_cfl(double ax, double ay, double az, double hx, doub
 #endif
 
 // WHAT: CORRECT_VELOCITY and/or CORRECT_PRESSURE; IMPL: implicit directions
-// as a compile-time mask (bit 0 x, 1 y, 2 z) or -1 to read them from bc. One
-// thread per cell, TC_CFL_KZ cells along z with CFL. With CFL the advective
+// as a compile-time mask (bit 0 x, 1 y, 2 z) or -1 to read them from bc. A
+// thread takes TC_CORRECT_KZ cells along z, TC_CFL_KZ with CFL. With CFL the advective
 // limit of decide_dt_adv
 // (src/decide_dt.c:32-80) is taken on the corrected velocities as they are
 // written, for the next step's dt (the reference computes it at the start of
 // that step from the same values).
-// Resident blocks requested from the register allocator; measured at
-// 256 x 1024 x 512 (ms per launch, averaged over a step's three): 6/5 (plain /
-// with CFL) 2.23, 5/4 2.15, 4/4 2.09. With all loads issued up front the
-// registers holding them buy more than the extra warps.
+// Resident blocks requested from the register allocator (plain / with CFL),
+// cells per thread along z without CFL (TC_CORRECT_KZ), and the cells whose
+// inputs are loaded together before any of them is stored (TC_CORRECT_G with
+// CFL, all KZ cells without). Within a group psi at k-1 and k+1 of an inner
+// cell is its neighbour's psi at k, loaded once. Measured at 256 x 1024 x 512
+// (ms per launch, averaged over a step's three): blocks 6/5, 1 cell 2.23; 5/4
+// 2.15; 4/4 2.04 (the CFL kernel spills at 64 registers); 4/3 1.95 (no
+// spills); 3/3 with 2 cells 1.88; 4/4 with 2 cells 2.03; 4/2 with CFL groups
+// of 2 1.94. With all loads issued up front the registers holding them buy
+// more than the extra warps.
 #ifndef TC_CORRECT_MB
-#define TC_CORRECT_MB 4
+#define TC_CORRECT_MB 3
 #endif
 #ifndef TC_CORRECT_MB_CFL
-#define TC_CORRECT_MB_CFL 4
+#define TC_CORRECT_MB_CFL 3
+#endif
+#ifndef TC_CORRECT_KZ
+#define TC_CORRECT_KZ 2
+#endif
+#ifndef TC_CORRECT_G
+#define TC_CORRECT_G 1
 #endif
 template <int WHAT, int IMPL, bool CFL, class T>
 __global__ void __launch_bounds__(256, CFL ? TC_CORRECT_MB_CFL : TC_CORRECT_MB)
@@ -112,7 +124,9 @@ correct_kernel(Geo g, Bc bc, Coefs cf, FieldsT<T> f, const double * __restrict__
   const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
-  constexpr int KZ = CFL ? TC_CFL_KZ : 1;
+  constexpr int KZ = CFL ? TC_CFL_KZ : TC_CORRECT_KZ;
+  constexpr int G = CFL ? TC_CORRECT_G : TC_CORRECT_KZ;
+  static_assert(KZ % G == 0, "cells per thread must be a multiple of the load group");
   const bool act = i <= nx && j <= ny;
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
   const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
@@ -121,87 +135,103 @@ correct_kernel(Geo g, Bc bc, Coefs cf, FieldsT<T> f, const double * __restrict__
   double ax = 0., ay = 0., az = 0.;   // |v| + 1e-8 of the corrected velocities (CFL)
   bool bad = false;
 #pragma unroll 1
-  for (int kz = 0; kz < KZ; kz++) {
-    const int k = blockIdx.z * KZ + kz + 1;
+  for (int k0 = 0; k0 < KZ; k0 += G) {
     if (act) {
-      // every input is loaded before the first store (the arrays are distinct,
-      // which the compiler cannot know), so a thread's loads are in flight together
+      // every input of the group is loaded before the first store (the arrays
+      // are distinct, which the compiler cannot know), so a thread's loads are
+      // in flight together
       const double * psi = f.psi;
-      const size_t qp = cidx(g, i, j, k);                                 // p, psi
-      const size_t qc = sidx_c<T>(g, i, j, k), qf = sidx_f<T>(g, i, j, k);  // ux, uy, uz
       const size_t sj = (size_t)(nx + 2), sk = (size_t)(nx + 2) * (ny + 2);
-      const double psi0 = __ldg(psi + qp);
-      const double psi_im = __ldg(psi + qp - 1);
-      const double psi_jm = __ldg(psi + qp - sj);
-      const double psi_km = __ldg(psi + qp - sk);
-      double psi_ip = 0., psi_jp = 0., psi_kp = 0.;
-      double ux0 = 0., uy0 = 0., uz0 = 0., p0 = 0.;
-      if (WHAT & CORRECT_VELOCITY) {
-        if (i >= 2) ux0 = f.ux[qf];
-        uy0 = f.uy[qc];
-        uz0 = f.uz[qc];
+      const int kb = blockIdx.z * KZ + k0 + 1;
+      double psi0[G], psi_im[G], psi_jm[G], psi_km[G], psi_ip[G], psi_jp[G], psi_kp[G];
+      double ux0[G], uy0[G], uz0[G], p0[G];
+#pragma unroll
+      for (int m = 0; m < G; m++) {
+        const size_t qp = cidx(g, i, j, kb + m);                                    // p, psi
+        const size_t qc = sidx_c<T>(g, i, j, kb + m), qf = sidx_f<T>(g, i, j, kb + m);  // ux, uy, uz
+        psi0[m] = __ldg(psi + qp);
+        psi_im[m] = __ldg(psi + qp - 1);
+        psi_jm[m] = __ldg(psi + qp - sj);
+        psi_km[m] = m == 0 ? __ldg(psi + qp - sk) : psi0[m - 1];
+        psi_ip[m] = psi_jp[m] = psi_kp[m] = 0.;
+        ux0[m] = uy0[m] = uz0[m] = p0[m] = 0.;
+        if (WHAT & CORRECT_VELOCITY) {
+          if (i >= 2) ux0[m] = f.ux[qf];
+          uy0[m] = f.uy[qc];
+          uz0[m] = f.uz[qc];
+        }
+        if (WHAT & CORRECT_PRESSURE) {
+          p0[m] = f.p[qp];
+          if (ix) psi_ip[m] = __ldg(psi + qp + 1);
+          if (iy) psi_jp[m] = __ldg(psi + qp + sj);
+          if (iz && m == G - 1) psi_kp[m] = __ldg(psi + qp + sk);
+        }
       }
       if (WHAT & CORRECT_PRESSURE) {
-        p0 = f.p[qp];
-        if (ix) psi_ip = __ldg(psi + qp + 1);
-        if (iy) psi_jp = __ldg(psi + qp + sj);
-        if (iz) psi_kp = __ldg(psi + qp + sk);
+#pragma unroll
+        for (int m = 0; m + 1 < G; m++)
+          if (iz) psi_kp[m] = psi0[m + 1];
       }
       const double dt = *dtp;
       const double pf = rk_gamma(rkstep) * dt;            // correct/main.c:21-22
       const double pp = 0.5 * rk_gamma(rkstep) * dt * nu;  // update_pressure.c:161-162
-      if (WHAT & CORRECT_VELOCITY) {
-        // ux, i = 2..nx (correct/ux.c:25-52); walls stay zero
-        const double vx = (i >= 2) ? ux0 - pf * __ldg(cf.c_invhxxf + i) * (-psi_im + psi0) : 0.;
-        f.ux[qf] = (T)vx;
-        for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx; });
-        if (i == nx) {
-          f.ux[qf + 1] = (T)0.;
-          for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.; });
+#pragma unroll
+      for (int m = 0; m < G; m++) {
+        const int k = kb + m;
+        if (WHAT & CORRECT_VELOCITY) {
+          const size_t qf = sidx_f<T>(g, i, j, k);
+          // ux, i = 2..nx (correct/ux.c:25-52); walls stay zero
+          const double vx = (i >= 2) ? ux0[m] - pf * __ldg(cf.c_invhxxf + i) * (-psi_im[m] + psi0[m]) : 0.;
+          f.ux[qf] = (T)vx;
+          for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx; });
+          if (i == nx) {
+            f.ux[qf + 1] = (T)0.;
+            for_images(j, k, ny, nz, [&](int jj, int kk) { f.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.; });
+          }
+          // uy (correct/uy.c:25-52), uz (correct/uz.c:15-44) with their walls
+          const double vy = uy0[m] - pf * __ldg(cf.c_invhyxc + i) * (-psi_jm[m] + psi0[m]);
+          const double vz = uz0[m] - pf * cf.inv_hz * (-psi_km[m] + psi0[m]);
+          auto put = [&](int jj, int kk) {
+            const size_t q = sidx_c<T>(g, i, jj, kk);
+            f.uy[q] = (T)vy;
+            f.uz[q] = (T)vz;
+            if (i == 1) { f.uy[q - 1] = (T)bc.uy_xm; f.uz[q - 1] = (T)0.; }
+            if (i == nx) { f.uy[q + 1] = (T)bc.uy_xp; f.uz[q + 1] = (T)0.; }
+          };
+          put(j, k);
+          for_images(j, k, ny, nz, put);
+          if (CFL) {
+            bad |= !isfinite(vx) || !isfinite(vy) || !isfinite(vz);
+            if (i >= 2) ax = fmax(ax, fabs(vx) + small);
+            ay = fmax(ay, fabs(vy) + small);
+            az = fmax(az, fabs(vz) + small);
+          }
         }
-        // uy (correct/uy.c:25-52), uz (correct/uz.c:15-44) with their walls
-        const double vy = uy0 - pf * __ldg(cf.c_invhyxc + i) * (-psi_jm + psi0);
-        const double vz = uz0 - pf * cf.inv_hz * (-psi_km + psi0);
-        auto put = [&](int jj, int kk) {
-          const size_t q = sidx_c<T>(g, i, jj, kk);
-          f.uy[q] = (T)vy;
-          f.uz[q] = (T)vz;
-          if (i == 1) { f.uy[q - 1] = (T)bc.uy_xm; f.uz[q - 1] = (T)0.; }
-          if (i == nx) { f.uy[q + 1] = (T)bc.uy_xp; f.uz[q + 1] = (T)0.; }
-        };
-        put(j, k);
-        for_images(j, k, ny, nz, put);
-        if (CFL) {
-          bad |= !isfinite(vx) || !isfinite(vy) || !isfinite(vz);
-          if (i >= 2) ax = fmax(ax, fabs(vx) + small);
-          ay = fmax(ay, fabs(vy) + small);
-          az = fmax(az, fabs(vz) + small);
+        // p += psi, then the implicit-direction corrections (update_pressure.c:23-136)
+        if (WHAT & CORRECT_PRESSURE) {
+          double val = p0[m] + psi0[m];   // p and psi are double in every storage mode
+          const double ijd = __ldg(cf.c_invjdxc + i);
+          if (ix) {
+            const double l = __ldg(cf.c_pxl + i), u = __ldg(cf.c_pxu + i), c = -l - u;
+            val -= 2. * pp * ijd * (l * psi_im[m] + c * psi0[m] + u * psi_ip[m]);
+          }
+          if (iy) {
+            const double l = __ldg(cf.c_pyl + i), c = -l - l;
+            val -= 2. * pp * ijd * (l * psi_jm[m] + c * psi0[m] + l * psi_jp[m]);
+          }
+          if (iz) {
+            const double l = __ldg(cf.c_pzl + i), c = -l - l;
+            val -= 2. * pp * ijd * (l * psi_km[m] + c * psi0[m] + l * psi_kp[m]);
+          }
+          auto put = [&](int jj, int kk) {
+            const size_t q = cidx(g, i, jj, kk);
+            f.p[q] = val;
+            if (i == 1) f.p[q - 1] = val;
+            if (i == nx) f.p[q + 1] = val;
+          };
+          put(j, k);
+          for_images(j, k, ny, nz, put);
         }
-      }
-      // p += psi, then the implicit-direction corrections (update_pressure.c:23-136)
-      if (WHAT & CORRECT_PRESSURE) {
-        double val = p0 + psi0;   // p and psi are double in every storage mode
-        const double ijd = __ldg(cf.c_invjdxc + i);
-        if (ix) {
-          const double l = __ldg(cf.c_pxl + i), u = __ldg(cf.c_pxu + i), c = -l - u;
-          val -= 2. * pp * ijd * (l * psi_im + c * psi0 + u * psi_ip);
-        }
-        if (iy) {
-          const double l = __ldg(cf.c_pyl + i), c = -l - l;
-          val -= 2. * pp * ijd * (l * psi_jm + c * psi0 + l * psi_jp);
-        }
-        if (iz) {
-          const double l = __ldg(cf.c_pzl + i), c = -l - l;
-          val -= 2. * pp * ijd * (l * psi_km + c * psi0 + l * psi_kp);
-        }
-        auto put = [&](int jj, int kk) {
-          const size_t q = cidx(g, i, jj, kk);
-          f.p[q] = val;
-          if (i == 1) f.p[q - 1] = val;
-          if (i == nx) f.p[q + 1] = val;
-        };
-        put(j, k);
-        for_images(j, k, ny, nz, put);
       }
     }
   }
@@ -215,7 +245,7 @@ template <int WHAT, int IMPL, bool CFL, class T>
 static void launch_correct_t(const Geo & g, const Bc & bc, const Coefs & cf, const FieldsT<T> & f, const double * dtp,
                              int rkstep, double nu, unsigned long long * dtmin, unsigned * status, cudaStream_t st) {
   dim3 block(32, 8, 1);
-  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz / (CFL ? TC_CFL_KZ : 1));   // nz: power of two >= 4
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz / (CFL ? TC_CFL_KZ : TC_CORRECT_KZ));   // nz: power of two >= 4
   correct_kernel<WHAT, IMPL, CFL, T><<<grid, block, 0, st>>>(g, bc, cf, f, dtp, rkstep, nu, dtmin, status);
 }
 
