@@ -39,6 +39,13 @@
 #ifndef TC_IFFTY_UNROLL
 #define TC_IFFTY_UNROLL 4   // spectrum loads in flight per thread, inverse y transform
 #endif
+// inverse y transform: strength-reduced psi stores (measured at 256 x 1024 x
+// 512: 0.95 -> 0.89 ms per launch; with the stores skipped 0.73 ms, the FFT
+// and the spectrum loads). A first FFT pass reading the spectrum straight into
+// registers instead of through shared memory measured 1.10 ms (spills).
+#ifndef TC_IFFTY_STREAM
+#define TC_IFFTY_STREAM 1
+#endif
 #ifndef TC_FFT_SMEM_MAX
 #define TC_FFT_SMEM_MAX (80 * 1024)   // dynamic shared memory the FFT kernels may ask for
 #endif
@@ -167,6 +174,11 @@ __device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict_
 #ifndef TC_FFT_TWIDDLE_PRODUCTS
 #define TC_FFT_TWIDDLE_PRODUCTS 1
 #endif
+// twiddle v[r] and v[r + 8] together (radix 16): the products are the same,
+// fewer of them are live at once
+#ifndef TC_FFT_TWIDDLE_PAIRED
+#define TC_FFT_TWIDDLE_PAIRED 1
+#endif
 template <int R, int SIGN>
 __device__ __forceinline__ void apply_twiddles(double2 * v, const double2 * __restrict__ tw, int step) {
   if (TC_FFT_TWIDDLE_PRODUCTS) {
@@ -180,19 +192,50 @@ __device__ __forceinline__ void apply_twiddles(double2 * v, const double2 * __re
       const int hb = 31 - __clz(r);
       low[r] = (r == (1 << hb)) ? p2[hb] : cmul(p2[hb], low[r - (1 << hb)]);
       v[r] = cmul(v[r], low[r]);
+#if TC_FFT_TWIDDLE_PAIRED
+      // w^(r+8) right away, so that low[r] dies with its last product
+      if (R == 16) v[r + 8] = cmul(v[r + 8], cmul(p2[3], low[r]));
+#endif
     }
+#if TC_FFT_TWIDDLE_PAIRED
+    if (R == 16) v[8] = cmul(v[8], p2[3]);
+#else
 #pragma unroll
     for (int r = 8; r < R; r++) v[r] = cmul(v[r], r == 8 ? p2[3] : cmul(p2[3], low[r - 8]));
+#endif
   } else {
 #pragma unroll
     for (int r = 1; r < R; r++) v[r] = cmul(v[r], twid<SIGN>(tw, r * step));
   }
 }
 
+// Barrier between the passes of one line's transform. LB: the caller's lines
+// are contiguous thread ranges (line p = threads p TPL .. p TPL + TPL - 1).
+// When TPL is then a multiple of 32 the line's warps wait only for each other
+// (named barrier 1 + line; the CTA holds at most 8 lines), so the lines of a
+// CTA advance independently; otherwise the whole CTA waits. A caller that
+// reads across lines after the transform synchronises the CTA itself.
+// Measured at 256 x 1024 x 512 (ms per launch, divergence + y / inverse y):
+// CTA barriers 1.29 / 0.89, line barriers 1.27 / 0.86, line barriers and
+// paired twiddles 1.26 / 0.83.
+#ifndef TC_FFT_LINE_BARRIER
+#define TC_FFT_LINE_BARRIER 1
+#endif
+template <bool LB>
+__device__ __forceinline__ void line_barrier(int TPL) {
+#if TC_FFT_LINE_BARRIER
+  if (LB && (TPL & 31) == 0 && (int)blockDim.x <= 8 * TPL) {
+    asm volatile("bar.sync %0, %1;" : : "r"(1 + (int)threadIdx.x / TPL), "r"(TPL) : "memory");
+    return;
+  }
+#endif
+  __syncthreads();
+}
+
 // One in-place Stockham pass of radix R over a padded line x of length N: the
 // thread owns butterflies j = t + b TPL (b < B); Ns is the product of the
 // radices already applied. All inputs are read before anything is written.
-template <int R, int B, int SIGN>
+template <int R, int B, int SIGN, bool LB>
 __device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t, int TPL,
                                               const double2 * __restrict__ tw) {
   double2 v[B][R];
@@ -203,7 +246,7 @@ __device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t,
 #pragma unroll
     for (int r = 0; r < R; r++) v[b][r] = x[pad(j + r * NR)];
   }
-  __syncthreads();
+  line_barrier<LB>(TPL);
 #pragma unroll
   for (int b = 0; b < B; b++) {
     const int j = t + b * TPL;
@@ -217,12 +260,12 @@ __device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t,
 #pragma unroll
     for (int r = 0; r < R; r++) x[pad(base + r * Ns)] = v[b][r];
   }
-  __syncthreads();
+  line_barrier<LB>(TPL);
 }
 
 // Full transform of the CTA's lines (N = 2^lg): EPT elements per thread,
 // radix-16 passes then the remainder; natural-order output in place.
-template <int EPT, int SIGN>
+template <int EPT, int SIGN, bool LB = false>
 __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const double2 * __restrict__ tw) {
   int Ns = 1;
   int left = lg;
@@ -231,17 +274,17 @@ __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const do
     constexpr int LGE = EPT >= 16 ? 4 : EPT >= 8 ? 3 : EPT >= 4 ? 2 : 1;
     const int rl = left >= LGE ? LGE : left;
     if (EPT == 16) {
-      if (rl == 4) stockham_pass<16, 1, SIGN>(x, N, Ns, t, TPL, tw);
-      else if (rl == 3) stockham_pass<8, 2, SIGN>(x, N, Ns, t, TPL, tw);
-      else if (rl == 2) stockham_pass<4, 4, SIGN>(x, N, Ns, t, TPL, tw);
-      else stockham_pass<2, 8, SIGN>(x, N, Ns, t, TPL, tw);
+      if (rl == 4) stockham_pass<16, 1, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else if (rl == 3) stockham_pass<8, 2, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else if (rl == 2) stockham_pass<4, 4, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 8, SIGN, LB>(x, N, Ns, t, TPL, tw);
     } else if (EPT == 8) {
-      if (rl == 3) stockham_pass<8, 1, SIGN>(x, N, Ns, t, TPL, tw);
-      else if (rl == 2) stockham_pass<4, 2, SIGN>(x, N, Ns, t, TPL, tw);
-      else stockham_pass<2, 4, SIGN>(x, N, Ns, t, TPL, tw);
+      if (rl == 3) stockham_pass<8, 1, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else if (rl == 2) stockham_pass<4, 2, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 4, SIGN, LB>(x, N, Ns, t, TPL, tw);
     } else {
-      if (rl == 2) stockham_pass<4, 1, SIGN>(x, N, Ns, t, TPL, tw);
-      else stockham_pass<2, 2, SIGN>(x, N, Ns, t, TPL, tw);
+      if (rl == 2) stockham_pass<4, 1, SIGN, LB>(x, N, Ns, t, TPL, tw);
+      else stockham_pass<2, 2, SIGN, LB>(x, N, Ns, t, TPL, tw);
     }
     Ns <<= rl;
     left -= rl;
@@ -253,7 +296,7 @@ __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const do
 // and last passes of a transform whose input or output lives elsewhere, so
 // the data crosses shared memory only between passes. A pass that reads and
 // writes the shared line synchronises like stockham_pass.
-template <int R, int B, int SIGN, bool IN, bool OUT, class Ld, class St>
+template <int R, int B, int SIGN, bool IN, bool OUT, bool LB, class Ld, class St>
 __device__ __forceinline__ void stockham_pass_io(double2 * x, const Ld & ld, const St & st, int N, int Ns, int t,
                                                  int TPL, const double2 * __restrict__ tw) {
   double2 v[B][R];
@@ -264,7 +307,7 @@ __device__ __forceinline__ void stockham_pass_io(double2 * x, const Ld & ld, con
 #pragma unroll
     for (int r = 0; r < R; r++) v[b][r] = IN ? ld(j + r * NR) : x[pad(j + r * NR)];
   }
-  if (!IN && !OUT) __syncthreads();
+  if (!IN && !OUT) line_barrier<LB>(TPL);
 #pragma unroll
   for (int b = 0; b < B; b++) {
     const int j = t + b * TPL;
@@ -281,13 +324,13 @@ __device__ __forceinline__ void stockham_pass_io(double2 * x, const Ld & ld, con
       else x[pad(base + r * Ns)] = v[b][r];
     }
   }
-  if (!OUT) __syncthreads();
+  if (!OUT) line_barrier<LB>(TPL);
 }
 
 // Full transform of one line (N = 2^lg) whose input comes from ld (IN_LD) or
 // the shared line x, and whose output goes to st (OUT_ST) or back to x; the
 // passes between go through x.
-template <int EPT, int SIGN, bool IN_LD, bool OUT_ST, class Ld, class St>
+template <int EPT, int SIGN, bool IN_LD, bool OUT_ST, bool LB = false, class Ld, class St>
 __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg, int t, int TPL,
                        const double2 * __restrict__ tw) {
   int Ns = 1;
@@ -295,10 +338,10 @@ __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg,
   auto pass = [&](auto rc, auto bc) {
     constexpr int R = decltype(rc)::value, B = decltype(bc)::value;
     const bool first = IN_LD && Ns == 1, last = OUT_ST && left == 0;
-    if (first && last) stockham_pass_io<R, B, SIGN, true, true>(x, ld, st, N, Ns, t, TPL, tw);
-    else if (first) stockham_pass_io<R, B, SIGN, true, false>(x, ld, st, N, Ns, t, TPL, tw);
-    else if (last) stockham_pass_io<R, B, SIGN, false, true>(x, ld, st, N, Ns, t, TPL, tw);
-    else stockham_pass_io<R, B, SIGN, false, false>(x, ld, st, N, Ns, t, TPL, tw);
+    if (first && last) stockham_pass_io<R, B, SIGN, true, true, LB>(x, ld, st, N, Ns, t, TPL, tw);
+    else if (first) stockham_pass_io<R, B, SIGN, true, false, LB>(x, ld, st, N, Ns, t, TPL, tw);
+    else if (last) stockham_pass_io<R, B, SIGN, false, true, LB>(x, ld, st, N, Ns, t, TPL, tw);
+    else stockham_pass_io<R, B, SIGN, false, false, LB>(x, ld, st, N, Ns, t, TPL, tw);
   };
   using I = int;
   while (left > 0) {
@@ -404,7 +447,8 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
   }
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  fft_inplace<EPT, -1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+  fft_inplace<EPT, -1, true>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+  if (TC_FFT_LINE_BARRIER) __syncthreads();
   // separate the two real transforms and store the ny/2+1 non-negative
   // wavenumbers: m < ny/2 for every radial index (power-of-two index
   // arithmetic), then the Nyquist terms
@@ -745,13 +789,46 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
     smem[(size_t)pp * LS + pad(m)] = z;
   }
   __syncthreads();
-  const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  fft_inplace<EPT, +1>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+  {
+    const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
+    fft_inplace<EPT, +1, true>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+  }
+  if (TC_FFT_LINE_BARRIER) __syncthreads();
   // one radial index per thread when TI divides the block size (ny >= 2 EPT),
   // else the plain element loop
   // (TI and the block size are powers of two)
   const int lgt = __ffs(TI) - 1;
   const bool fixed_i = blockDim.x % TI == 0;
+#if TC_IFFTY_STREAM
+  if (fixed_i) {
+    // the thread's radial index is fixed and its rows j advance by a constant
+    // stride: one pointer step per store, the images only on edge rows/planes
+    const int ii = threadIdx.x & (TI - 1), i = i0 + ii;
+    if (i > nx) return;
+    const int js = blockDim.x >> lgt;
+    const double2 * zs = smem + (size_t)(ii >> 1) * LS;
+    const bool hi = (ii & 1) != 0, kedge = k == 1 || k == nz;
+    int j = (threadIdx.x >> lgt) + 1;
+    double * out = psi + cidx(g, i, j, k);
+    const size_t step = (size_t)js * (nx + 2);
+#pragma unroll 4
+    for (int r = 0; r < 2 * EPT; r++, j += js, out += step) {
+      const double2 z = zs[pad(j - 1)];
+      const double val = hi ? z.y : z.x;
+      *out = val;
+      if (i == 1) out[-1] = val;
+      if (i == nx) out[1] = val;
+      if (kedge || j == 1 || j == ny)
+        for_images(j, k, ny, nz, [&](int jj, int kk) {
+          const size_t q = cidx(g, i, jj, kk);
+          psi[q] = val;
+          if (i == 1) psi[q - 1] = val;
+          if (i == nx) psi[q + 1] = val;
+        });
+    }
+    return;
+  }
+#endif
   const int nr = fixed_i ? 2 * EPT : (TI * ny + blockDim.x - 1) / blockDim.x;
 #pragma unroll 4
   for (int r = 0; r < nr; r++) {
