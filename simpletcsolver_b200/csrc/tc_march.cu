@@ -752,8 +752,12 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
 #ifndef TC_MARCH_JT
 #define TC_MARCH_JT 2
 #endif
+// Planes per CTA: each CTA's start (coefficients, barriers, the first planes'
+// copies) overlaps nothing at one CTA per SM, and its two halo planes are read
+// twice. Measured at 256 x 1024 x 512 (ms per launch): 16 7.01, 32 6.86, 64
+// 6.82, 128 6.81-7.03.
 #ifndef TC_MARCH_KC
-#define TC_MARCH_KC 32
+#define TC_MARCH_KC 64
 #endif
 
 template <int NW, class T>
