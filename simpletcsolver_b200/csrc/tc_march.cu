@@ -752,17 +752,54 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
 #ifndef TC_MARCH_JT
 #define TC_MARCH_JT 2
 #endif
-// Planes per CTA: each CTA's start (coefficients, barriers, the first planes'
-// copies) overlaps nothing at one CTA per SM, and its two halo planes are read
-// twice. Measured at 256 x 1024 x 512 (ms per launch): 16 7.01, 32 6.86, 64
-// 6.82, 128 6.81-7.03.
+// Planes per CTA, at most: each CTA's start (coefficients, barriers, the first
+// planes' copies) overlaps nothing at one CTA per SM, and its two halo planes
+// are read twice. Measured at 256 x 1024 x 512 (ms per launch): 16 7.01, 32
+// 6.86, 64 6.82, 128 6.81-7.03. Smaller grids take fewer planes per CTA when
+// the last wave of CTAs would leave SMs idle (march_planes).
 #ifndef TC_MARCH_KC
 #define TC_MARCH_KC 64
 #endif
 
+// The largest chunk of planes, from TC_MARCH_KC down to 16, whose last partial
+// wave of CTAs wastes at most 5% of the launch (at 256 x 512 x 128: 64 planes
+// are 3.5 waves, 32 planes 6.9).
 template <int NW, class T>
-void launch_march_nw(const MarchArgs<T> & A, const double * dtp, cudaStream_t st) {
+static int march_planes(const Geo & g) {
+  constexpr int JT = TC_MARCH_JT;
+  static int per_sm[16], sms[16];   // per device: resident CTAs of this instance, SM count
+  int dev = 0;
+  cudaGetDevice(&dev);
+  dev &= 15;
+  if (per_sm[dev] == 0) {
+    int b = 0, n = 0;
+    // a failed query falls back to one CTA on 148 SMs and clears its own error
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, march_predict_kernel<NW, JT, 1, T>,
+                                                      32 * NW * TC_MARCH_GROUPS, MarchLayout<NW, JT, T>::BYTES) !=
+        cudaSuccess) {
+      b = 0;
+      cudaGetLastError();
+    }
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      n = 0;
+      cudaGetLastError();
+    }
+    sms[dev] = n > 0 ? n : 148;
+    per_sm[dev] = b > 0 ? b : 1;
+  }
+  const long long slots = (long long)sms[dev] * per_sm[dev], lines = g.ny / JT;
+  int kc = g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC;
+  for (; kc > 16; kc >>= 1) {
+    const long long nblk = lines * (g.nz / kc), waves = (nblk + slots - 1) / slots;
+    if (waves * slots * 100 <= nblk * 105) break;
+  }
+  return kc;
+}
+
+template <int NW, class T>
+void launch_march_nw(MarchArgs<T> A, const double * dtp, cudaStream_t st) {
   constexpr int JT = TC_MARCH_JT;   // ny is a power of two >= 4
+  A.KC = march_planes<NW, T>(A.g);
   const long long nblk = (long long)(A.g.ny / JT) * (A.g.nz / A.KC);
   const int mask = (A.bc.implicit[0] ? 1 : 0) | (A.bc.implicit[1] ? 2 : 0) | (A.bc.implicit[2] ? 4 : 0);
   const unsigned grid = (unsigned)nblk, block = 32 * NW * TC_MARCH_GROUPS;
@@ -798,8 +835,7 @@ void launch_march_t(const Geo & g, const Bc & bc, const Coefs & cf, const XFacto
                     double kappa, const FieldBufs & in, const FieldBufs & out, const SrcBufs & ss,
                     const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
                     cudaStream_t st) {
-  MarchArgs<T> A{g, bc, cf, xf, nu, kappa, in.as<T>(), out.as<T>(), ss.as<T>(), ds, rkstep, mode,
-                 g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC, status};
+  MarchArgs<T> A{g, bc, cf, xf, nu, kappa, in.as<T>(), out.as<T>(), ss.as<T>(), ds, rkstep, mode, 0, status};
   switch (predict_warps(g.nx)) {
     case 1: launch_march_nw<1>(A, dtp, st); break;
     case 2: launch_march_nw<2>(A, dtp, st); break;
