@@ -103,7 +103,7 @@ __device__ inline void warp_cfl(double ax, double ay, double az, double hx, doub
 // (ms per launch, averaged over a step's three): blocks 6/5, 1 cell 2.23; 5/4
 // 2.15; 4/4 2.04 (the CFL kernel spills at 64 registers); 4/3 1.95 (no
 // spills); 3/3 with 2 cells 1.88; 4/4 with 2 cells 2.03; 4/2 with CFL groups
-// of 2 1.94. With all loads issued up front the registers holding them buy
+// of 2 1.94; 2/3 with 4 cells 1.96. With all loads issued up front the registers holding them buy
 // more than the extra warps.
 #ifndef TC_CORRECT_MB
 #define TC_CORRECT_MB 3
