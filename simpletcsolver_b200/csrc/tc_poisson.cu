@@ -66,6 +66,14 @@
 #ifndef TC_FFTZ_THREADS
 #define TC_FFTZ_THREADS 256
 #endif
+// z transforms: CTAs of neighbouring wavenumber groups launched back to back
+// (grid x over the groups, y over the radial index), so the 32-byte sectors
+// that two groups' columns share (rows of nyh = ny/2 + 1 complex values start
+// 16 bytes off a sector every other row) are still in L2 for the second.
+// Measured at 256 x 1024 x 512: 0.58 -> 0.53 ms per launch.
+#ifndef TC_FFTZ_MFAST
+#define TC_FFTZ_MFAST 1
+#endif
 #ifndef TC_FFTZ_MIN_BLOCKS
 #define TC_FFTZ_MIN_BLOCKS 3
 #endif
@@ -481,9 +489,15 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   const int nz = g.nz, nyh = ps.nyh;
   const int TPL = nz / EPT;
   const int LS = padded_len(nz);
+#if TC_FFTZ_MFAST
+  const int i = blockIdx.y;          // 0..nx-1
+  const int p = threadIdx.x % P, t = threadIdx.x / P;
+  const int m = blockIdx.x * P + p;
+#else
   const int i = blockIdx.x;          // 0..nx-1
   const int p = threadIdx.x % P, t = threadIdx.x / P;
   const int m = blockIdx.y * P + p;
+#endif
   Z * col = static_cast<Z *>(ps.spec) + (size_t)i * nz * nyh + m;
   const bool gv = m < nyh;
   auto ld = [&](int e) { return gv ? zget(col + (size_t)e * nyh) : make_double2(0., 0.); };
@@ -883,7 +897,11 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   const int Pz = lines_per_cta(g.nz, ps.nyh, EPTZ, TC_FFTZ_THREADS);
   const int tplz = g.nz / EPTZ;
   const size_t smz = sizeof(double2) * (size_t)Pz * padded_len(g.nz);
+#if TC_FFTZ_MFAST
+  dim3 gz((ps.nyh + Pz - 1) / Pz, g.nx);
+#else
   dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
+#endif
   fftz_kernel<EPTZ, -1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   mark(pm.k_fwd);
   if (!launch_tdm_lines<Z>(g, ps, st)) {
