@@ -657,9 +657,25 @@ void launch_tdm_factors(const Geo & g, const Poisson & ps, const double * tab_y,
 // each warp solves whole lines from shared memory with the affine-map scans
 // (E = n / 32 points per lane, in-register prefix + 5-level shuffle scan).
 constexpr int TDM_PT = 16;
+// resident CTAs per SM requested from the register allocator (0: the
+// allocator's own choice), and the factor rows loaded ahead of their use: the
+// warp's first w row with the tile, each line's v row before its forward scan.
+// Measured at 256 x 1024 x 512 (ms per launch): 0.58, prefetched 0.56; 3
+// resident CTAs (80 registers, 64 bytes spilled) 0.58.
+#ifndef TC_TDM_LINES_MB
+#define TC_TDM_LINES_MB 0
+#endif
+#if TC_TDM_LINES_MB > 0
+#define TC_TDM_LINES_BOUNDS __launch_bounds__(256, TC_TDM_LINES_MB)
+#else
+#define TC_TDM_LINES_BOUNDS __launch_bounds__(256)
+#endif
+#ifndef TC_TDM_LINES_PREFETCH
+#define TC_TDM_LINES_PREFETCH 1
+#endif
 
 template <int E, class Z>
-__global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
+__global__ void TC_TDM_LINES_BOUNDS tdm_lines_kernel(Geo g, Poisson ps) {
   constexpr int N = 32 * E, NT = 256, PER = N * TDM_PT / NT;
   extern __shared__ double2 tq[];
   const int nyh = ps.nyh;
@@ -668,6 +684,15 @@ __global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
   const int nt = (int)min((long long)TDM_PT, nlines - l0);
   const size_t st = (size_t)nlines;               // complex values between radial indices
   Z * spec = static_cast<Z *>(ps.spec);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#if TC_TDM_LINES_PREFETCH
+  double wq[E];   // w of the warp's first line, in flight with the tile
+  if (wid < nt) {
+    const double * w = ps.fw + (size_t)(l0 + wid) * N;
+#pragma unroll
+    for (int e = 0; e < E; e++) wq[e] = w[e * 32 + lane];
+  }
+#endif
   {
     double2 buf[PER];
 #pragma unroll
@@ -682,7 +707,6 @@ __global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
     }
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double ll[E];
 #pragma unroll
   for (int e = 0; e < E; e++) ll[e] = ps.tl[lane * E + e];
@@ -692,10 +716,19 @@ __global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
     const double * v = ps.fv + (size_t)l * N;
     const int sw = t ^ (lane & (TDM_PT - 1));
     double fa[E], bre[E], bim[E];
+#if TC_TDM_LINES_PREFETCH
+    double vq[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) vq[e] = v[e * 32 + lane];
+#endif
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const double2 qv = tq[(lane * E + e) * TDM_PT + sw];
+#if TC_TDM_LINES_PREFETCH
+      const double we = (t == wid) ? wq[e] : w[e * 32 + lane];
+#else
       const double we = w[e * 32 + lane];
+#endif
       fa[e] = -we * ll[e];
       bre[e] = we * qv.x;
       bim[e] = we * qv.y;
@@ -727,7 +760,11 @@ __global__ void __launch_bounds__(256) tdm_lines_kernel(Geo g, Poisson ps) {
     }
     // backward: x_i = y_i - v_i x_{i+1}, suffix maps
 #pragma unroll
+#if TC_TDM_LINES_PREFETCH
+    for (int e = 0; e < E; e++) fa[e] = -vq[e];
+#else
     for (int e = 0; e < E; e++) fa[e] = -v[e * 32 + lane];
+#endif
 #pragma unroll
     for (int d = 1; d < E; d <<= 1) {
 #pragma unroll
