@@ -96,6 +96,11 @@ _EXT_SIGS = {
     "tcgpu_get_storage": (C.c_int, [C.POINTER(FluidT)]),
     "tcgpu_last_error": (C.c_char_p, []),
     "tcgpu_selftest_wait": (C.c_int, [c_double_p]),
+    "tcgpu_set_device": (C.c_int, [C.c_int]),
+    "tcgpu_run_timed": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_int, C.c_int, c_double_p,
+                                  C.POINTER(C.c_float), C.c_double * 12, C.c_int * 12]),
+    "tcgpu_tdm_solve_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_bool, C.c_bool, c_double_p, c_double_p, c_double_p,
+                                          C.c_void_p]),
     "tcgpu_stream": (C.c_void_p, [C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_coarsen": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_closure_input": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 3, C.c_int, C.c_void_p]),
@@ -126,6 +131,18 @@ def declared_symbols(header: str = HEADER):
     names = set(re.findall(r"^\s*(?:extern\s+)?(?:const\s+)?[\w\s\*]+?\b(\w+)\s*\(", src, flags=re.M))
     names |= set(re.findall(r"^\s*extern\s+const\s+\w+\s+(\w+)", src, flags=re.M))
     return sorted(n for n in names if n not in ("if", "defined", "int", "double", "void"))
+
+
+def declared_functions(header: str = HEADER):
+    """Top-level function declarations of include/*.h: name -> number of
+    parameters (the function-pointer members of tdm_t are not top level)."""
+    src = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"^[ \t]*(?:extern\s+)?[A-Za-z_][\w \t\*]*?\b([A-Za-z_]\w*)\s*\(([^()]*)\)\s*;", src,
+                         flags=re.M):
+        params = " ".join(m.group(2).split())
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
 
 
 def _bind(lib, sigs):

@@ -22,6 +22,18 @@ def test_exports_every_declared_symbol(lib):
     assert not missing, missing
 
 
+def test_every_declared_function_has_a_binding():
+    """Every function include/tcgpu.h declares has a ctypes signature with the
+    header's number of parameters."""
+    fns = abi.declared_functions()
+    assert {"integrate", "tcgpu_run_timed", "tcgpu_tdm_solve_noalloc", "tcgpu_nn_conv3"} <= set(fns)
+    assert set(fns) <= set(abi.declared_symbols())
+    sigs = {**abi._SIGS, **abi._EXT_SIGS}
+    assert sorted(set(fns) - set(sigs)) == []
+    wrong = {n: (fns[n], len(sigs[n][1])) for n in fns if len(sigs[n][1]) != fns[n]}
+    assert wrong == {}
+
+
 def test_struct_layout_matches_header(tmp_path):
     prog = r'''
 #include <stdio.h>
