@@ -73,9 +73,13 @@ def test_oracle_tdm_bit_exact_with_reference(key):
 
 
 @pytest.mark.skipif(not have_ref("tc"), reason="reference build oracle/_ref absent")
-@pytest.mark.parametrize("build,nx,ny,nz", [("tc", 10, 16, 8), ("planar", 10, 8, 16)])
+@pytest.mark.parametrize("build,nx,ny,nz", [("tc", 10, 16, 8), ("tc", 12, 64, 16), ("tcexp", 12, 16, 8),
+                                             ("planar", 10, 8, 16)])
 def test_oracle_matches_reference_fresh_case(build, nx, ny, nz, tmp_path):
-    case = ic.taylor_couette(nx, ny, nz, 3400.0, seed=7) if build == "tc" else ic.plane_couette(nx, ny, nz, 2000.0, seed=7)
+    if build == "planar":
+        case = ic.plane_couette(nx, ny, nz, 2000.0, seed=7)
+    else:
+        case = ic.taylor_couette(nx, ny, nz, 3400.0, seed=7, implicit=(build == "tc", False, False))
     d0 = ic.write_ic(case, str(tmp_path / "ic"))
     out = str(tmp_path / "out")
     env = dict(os.environ, **ic.case_env(case))
