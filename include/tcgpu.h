@@ -181,10 +181,15 @@ int tcgpu_get_params(tcgpu_params_t * params);
 /* what the reference entry points copy back to the host besides the fields
  * they change (bit mask, per context) */
 #define TCGPU_SYNC_SRCS    1u  /* RK source terms after fluid_predict_field */
-#define TCGPU_SYNC_TENSORS 2u  /* velocity-gradient tensors after fluid_predict_field */
+#define TCGPU_SYNC_TENSORS 2u  /* velocity-gradient tensors after fluid_predict_field
+                                  and integrate (those of the substep-3 input, as the
+                                  reference leaves them) */
 #define TCGPU_NO_COHERENCE 4u  /* copy nothing: the caller uses tcgpu_push/pull */
 #define TCGPU_PIN_HOST     8u  /* page-lock the caller's six field arrays until
                                   tcgpu_release (faster host<->device copies) */
+/* A host that cannot call tcgpu_set_coherence (the reference's unmodified
+ * main.c) sets the environment variable TCGPU_SYNC_TENSORS=1 (and/or
+ * TCGPU_SYNC_SRCS=1): contexts created afterwards start with that flag. */
 int tcgpu_set_coherence(const domain_t * domain, fluid_t * fluid, unsigned flags);
 
 /* field masks for tcgpu_push / tcgpu_pull */
@@ -253,21 +258,54 @@ int tcgpu_get_storage(const fluid_t * fluid);
  * tensors of the current fields. */
 int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]);
 
+/* The same nine quantities with the reference's logging semantics
+ * (src/logging/main.c after integrate()): momentum injection and dissipation
+ * use the velocity-gradient tensors of the last predict's input fields, which
+ * is what src/fluid/predict/main.c:56-82 leaves in fluid_t for
+ * src/logging/injection.c:49-51 and dissipation.c; the wall velocity, the
+ * scalar terms, the divergence and the energies use the current fields.
+ * Before any predict, the tensors of the current fields. */
+int tcgpu_log_quantities(const domain_t * domain, fluid_t * fluid, double out[9]);
+
+/* Statistics of src/statistics.c:124-240 accumulated on the device (no
+ * counterpart entry points in the reference, which accumulates on the host).
+ * collect: adds one sample from the current fields (ux1, ux2, uy1, uy2, uz1,
+ * uz2, adv) and, for dif = lyx0 + lyx1 + lxy, from the fields the reference's
+ * tensors belong to (those of tcgpu_log_quantities); the accumulators are
+ * allocated on the first call. reset: zero them and the sample count. get:
+ * *num = samples so far, out[s] (host arrays, NULL to skip) = accumulator s in
+ * the order ux1 ux2 uy1 uy2 uz1 uz2 adv dif, laid out [k][j][i] over the
+ * interior j, k with i = 1..nx+1 (ux1, ux2, adv, dif: nx+1 values per row) or
+ * i = 0..nx+1 (uy1, uy2, uz1, uz2: nx+2). save: the reference's statistics
+ * directory (src/statistics.c:250-300): num.npy, the domain, and the eight
+ * arrays with those shapes (nothing is written when no sample was collected).
+ * mean_uy: profile[i], i = 0..nx+1, = mean of uy over j, k and the samples. */
+int tcgpu_statistics_collect(const domain_t * domain, fluid_t * fluid);
+int tcgpu_statistics_reset(const domain_t * domain, fluid_t * fluid);
+int tcgpu_statistics_get(const domain_t * domain, fluid_t * fluid, size_t * num, double * const out[8]);
+int tcgpu_statistics_save(const char dirname[], const domain_t * domain, fluid_t * fluid);
+int tcgpu_statistics_mean_uy(const domain_t * domain, fluid_t * fluid, double * profile);
+
 /* Allocation-free variant of tdm.solve(). No counterpart in the reference.
- * For callers that cannot allocate device memory or let a library do it
- * (inside CUDA graph capture, under a framework that owns the device memory
- * pool, or on hosts that reserve all device memory at start-up): the
- * elimination factors go to a fixed static device array of
+ * For callers that cannot allocate device memory or let a library do it: a
+ * framework that owns the whole device memory pool and forbids other
+ * allocators, a real-time host that reserves all device memory at start-up and
+ * may not allocate afterwards, or a plugin whose allocations belong to someone
+ * else. The elimination factors go to a fixed static device array of
  * 4 * TCGPU_TDM_NOALLOC_MAX_SIZE doubles (256 KiB) that every GPU which loads
  * this library holds until the process exits; nothing is cudaMalloc'd or freed.
  * l, c, u: host arrays of length size (lower, centre, upper diagonals as in
- * tdm.get_l/get_c/get_u); data: device memory with nrhs right-hand sides of
- * length size, contiguous (interleaved re/im when is_complex), solved in place
- * with the same arithmetic as tdm.solve(). size must lie in
- * [1, TCGPU_TDM_NOALLOC_MAX_SIZE] ([3, ...] when periodic); larger systems are
- * rejected with a non-zero return. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture. All calls share the one
+ * tdm.get_l/get_c/get_u); data: device memory of the current device with nrhs
+ * right-hand sides of length size, contiguous (interleaved re/im when
+ * is_complex), solved in place with the same arithmetic as tdm.solve(). size
+ * must lie in [1, TCGPU_TDM_NOALLOC_MAX_SIZE] ([3, ...] when periodic); larger
+ * systems, host memory and memory of another device are rejected with a
+ * non-zero return. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current. The work runs on the
+ * legacy default stream and the call returns only once it has finished, so data
+ * must be complete before the call: synchronise the stream that wrote it when
+ * that stream does not synchronise with the legacy default stream (a
+ * non-blocking stream, or per-thread default streams). All calls share the one
  * array and each rewrites every entry it reads; calls whose kernels could
  * overlap on the GPU (other threads, other streams) would race on it, so this
  * library serialises its own calls and synchronises before returning. */

@@ -4,7 +4,7 @@ TEST INFRASTRUCTURE ONLY. This module is the oracle that the CUDA library is
 checked against; it is imported by tests/, by the package's smoke check and by
 bench.py's CPU-baseline leg, never by the product path. It is itself pinned
 against the reference compiled from its own sources (oracle/Makefile) in
-tests/test_oracle_vs_reference.py.
+tests/test_oracle.py.
 
 Layout: every field is a numpy array A[k, j, i] holding the reference's index
 space including halos, i.e. i, j, k run over 0..n+1 and A[k, j, i] is the

@@ -91,6 +91,13 @@ _EXT_SIGS = {
     "tcgpu_pull": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_uint]),
     "tcgpu_run": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_int, c_double_p]),
     "tcgpu_diagnostics": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 9]),
+    "tcgpu_log_quantities": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 9]),
+    "tcgpu_statistics_collect": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT)]),
+    "tcgpu_statistics_reset": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT)]),
+    "tcgpu_statistics_get": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.POINTER(C.c_size_t),
+                                       c_double_p * 8]),
+    "tcgpu_statistics_save": (C.c_int, [C.c_char_p, C.POINTER(DomainT), C.POINTER(FluidT)]),
+    "tcgpu_statistics_mean_uy": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), c_double_p]),
     "tcgpu_release": (C.c_int, [C.POINTER(FluidT)]),
     "tcgpu_set_storage": (C.c_int, [C.c_int]),
     "tcgpu_get_storage": (C.c_int, [C.POINTER(FluidT)]),

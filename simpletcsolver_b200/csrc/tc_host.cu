@@ -45,6 +45,12 @@ static int fail(const char * fmt, ...) {
 static tcgpu_params_t g_params = {1.0, 0.0, 0.5, -0.5, 1, 0, 0, -1.0, -1.0};
 static std::mutex g_mutex;
 
+// a variable that is set to anything but "" or "0"
+static bool env_flag(const char * name) {
+  const char * s = getenv(name);
+  return s != nullptr && s[0] != '\0' && strcmp(s, "0") != 0;
+}
+
 static int env_double(const char * name, double * value) {
   // src/config.c:14-46
   const char * s = getenv(name);
@@ -89,6 +95,15 @@ struct Ctx {
   double * diag_part = nullptr;
   Tensors tn{};
   bool have_tn = false;
+  // fb[cur ^ 1] holds the input fields of the last predict: every predict
+  // writes the other buffer of the pair and leaves its input in place until the
+  // next predict, and nothing else writes that buffer. The reference's logging
+  // and statistics read the velocity-gradient tensors of exactly those fields
+  // (src/fluid/predict/main.c:56-82 is their only writer).
+  bool have_prev = false;
+  Stats stats{};              // device statistics (src/statistics.c), allocated on first use
+  size_t stat_num = 0;
+  double * stat_prof = nullptr;
   double coef_adv = 0., coef_dif = 0.;
   double Re = 0., Pr = 0., nu = 0., kappa = 0.;
   double caps_h[3] = {0., 0., 0.};
@@ -545,6 +560,10 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
   c->bc.implicit[0] = g_params.implicit_x ? 1 : 0;
   c->bc.implicit[1] = g_params.implicit_y ? 1 : 0;
   c->bc.implicit[2] = g_params.implicit_z ? 1 : 0;
+  // a host that cannot call tcgpu_set_coherence (the reference's own main.c)
+  // opts in to the extra copies through the environment
+  if (env_flag("TCGPU_SYNC_TENSORS")) c->coherence |= TCGPU_SYNC_TENSORS;
+  if (env_flag("TCGPU_SYNC_SRCS")) c->coherence |= TCGPU_SYNC_SRCS;
   auto bad = [&](const char * what) { fail("%s", what); destroy_ctx(c); return (Ctx *)nullptr; };
   if (resolve_coefs(*c)) { destroy_ctx(c); return nullptr; }
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) return bad("cudaStreamCreate failed");
@@ -668,6 +687,7 @@ static void enqueue_predict(Ctx & c, int rk) {
   const FieldBufs in = c.fb[c.cur];
   const FieldBufs out = c.fb[c.cur ^ 1];
   const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
+  c.have_prev = true;
   auto predict = [&](int mode) {
     launch_predict_march(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, mode, c.status, c.st);
   };
@@ -886,9 +906,14 @@ static int ensure_tensors(Ctx & c) {
   return 0;
 }
 
-static int pull_tensors(Ctx & c, fluid_t * fl) {
+// the fields the reference's tensors belong to: the last predict's input,
+// or the current fields before any predict
+static const FieldBufs & tensor_fields(Ctx & c) { return c.have_prev ? c.fb[c.cur ^ 1] : c.fb[c.cur]; }
+
+// the eleven tensors of fields f, copied into the caller's arrays
+static int pull_tensors(Ctx & c, fluid_t * fl, const FieldBufs & f) {
   if (ensure_tensors(c)) return 1;
-  launch_tensors(c.g, c.cf, c.f(), c.tn, c.st);
+  launch_tensors(c.g, c.cf, f, c.tn, c.st);
   const size_t nface = (size_t)(c.nx + 1) * (c.ny + 2) * (c.nz + 2);
   const size_t ncent = (size_t)c.nx * (c.ny + 2) * (c.nz + 2);
   array_t * dst[11] = {&fl->lxx, &fl->lxy, &fl->lxz, &fl->lyx0, &fl->lyx1, &fl->lyy0, &fl->lyy1, &fl->lyz,
@@ -997,7 +1022,7 @@ int tcgpu_pull(const domain_t * domain, fluid_t * fluid, unsigned fields) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
   if (pull_fields(*c, fluid, fields & TCGPU_FIELDS)) return 1;
-  if ((fields & TCGPU_TENSORS) && pull_tensors(*c, fluid)) return 1;
+  if ((fields & TCGPU_TENSORS) && pull_tensors(*c, fluid, tensor_fields(*c))) return 1;
   return finish(*c, "tcgpu_pull");
 }
 
@@ -1092,13 +1117,107 @@ int tcgpu_set_device(int device) {
   return 0;
 }
 
+static int diagnostics(Ctx & c, const FieldBufs & fs, double out[9], const char * what) {
+  launch_diagnostics(c.g, c.cf, c.bc, c.f(), fs, c.nu, c.kappa, c.diag_out, c.diag_part, c.st);
+  CK(cudaMemcpyAsync(c.h_scalar, c.diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  if (finish(c, what)) return 1;
+  memcpy(out, c.h_scalar, 9 * sizeof(double));
+  return 0;
+}
+
 int tcgpu_diagnostics(const domain_t * domain, fluid_t * fluid, double out[9]) {
   Ctx * c = get_ctx(domain, fluid);
   if (!c) return 1;
-  launch_diagnostics(c->g, c->cf, c->bc, c->f(), c->nu, c->kappa, c->diag_out, c->diag_part, c->st);
-  CK(cudaMemcpyAsync(c->h_scalar, c->diag_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-  if (finish(*c, "tcgpu_diagnostics")) return 1;
-  memcpy(out, c->h_scalar, 9 * sizeof(double));
+  return diagnostics(*c, c->f(), out, "tcgpu_diagnostics");
+}
+
+int tcgpu_log_quantities(const domain_t * domain, fluid_t * fluid, double out[9]) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  return diagnostics(*c, tensor_fields(*c), out, "tcgpu_log_quantities");
+}
+
+// ------------------------------------------------------------------ statistics
+static int ensure_stats(Ctx & c) {
+  if (c.stats.a[0]) return 0;
+  const size_t lines = (size_t)c.ny * c.nz;
+  for (int s = 0; s < 8; s++) {
+    const bool wide = s >= 2 && s <= 5;   // uy, uz: i = 0..nx+1
+    c.stats.a[s] = dalloc(c, (wide ? c.nx + 2 : c.nx + 1) * lines);
+    if (!c.stats.a[s]) return fail("cudaMalloc of the statistics failed");
+  }
+  c.stat_prof = dalloc(c, (size_t)c.nx + 2);
+  if (!c.stat_prof) return fail("cudaMalloc of the statistics failed");
+  return 0;
+}
+
+static size_t stat_count(const Ctx & c, int s) {
+  return (size_t)((s >= 2 && s <= 5) ? c.nx + 2 : c.nx + 1) * c.ny * c.nz;
+}
+
+int tcgpu_statistics_collect(const domain_t * domain, fluid_t * fluid) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (ensure_stats(*c)) return 1;
+  launch_statistics(c->g, c->cf, c->f(), tensor_fields(*c), c->stats, c->st);
+  CK(cudaGetLastError());
+  c->stat_num += 1;
+  return 0;
+}
+
+int tcgpu_statistics_reset(const domain_t * domain, fluid_t * fluid) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (c->stats.a[0]) {
+    for (int s = 0; s < 8; s++) CK(cudaMemsetAsync(c->stats.a[s], 0, stat_count(*c, s) * sizeof(double), c->st));
+  }
+  c->stat_num = 0;
+  return finish(*c, "tcgpu_statistics_reset");
+}
+
+int tcgpu_statistics_get(const domain_t * domain, fluid_t * fluid, size_t * num, double * const out[8]) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (ensure_stats(*c)) return 1;
+  if (num) *num = c->stat_num;
+  if (out) {
+    for (int s = 0; s < 8; s++) {
+      if (out[s] == nullptr) continue;
+      CK(cudaMemcpyAsync(out[s], c->stats.a[s], stat_count(*c, s) * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    }
+  }
+  return finish(*c, "tcgpu_statistics_get");
+}
+
+int tcgpu_io_write_statistics(const char dirname[], const domain_t * domain, size_t num, const double * const a[8]);
+
+int tcgpu_statistics_save(const char dirname[], const domain_t * domain, fluid_t * fluid) {
+  if (dirname == nullptr) return fail("tcgpu_statistics_save: dirname is NULL");
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (c->stat_num == 0) return 0;   // statistics.c:256-258: nothing collected, nothing saved
+  std::vector<std::vector<double>> host(8);
+  const double * ptrs[8];
+  for (int s = 0; s < 8; s++) {
+    host[s].resize(stat_count(*c, s));
+    CK(cudaMemcpyAsync(host[s].data(), c->stats.a[s], host[s].size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    ptrs[s] = host[s].data();
+  }
+  if (finish(*c, "tcgpu_statistics_save")) return 1;
+  return tcgpu_io_write_statistics(dirname, domain, c->stat_num, ptrs);
+}
+
+int tcgpu_statistics_mean_uy(const domain_t * domain, fluid_t * fluid, double * profile) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (profile == nullptr) return fail("tcgpu_statistics_mean_uy: profile is NULL");
+  if (c->stat_num == 0) return fail("tcgpu_statistics_mean_uy: no samples collected");
+  const double inv = 1. / ((double)c->stat_num * (double)c->ny * (double)c->nz);
+  launch_stat_profile(c->g, c->stats.a[2], inv, c->stat_prof, c->st);
+  std::vector<double> host((size_t)c->nx + 2);
+  CK(cudaMemcpyAsync(host.data(), c->stat_prof, host.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (finish(*c, "tcgpu_statistics_mean_uy")) return 1;
+  memcpy(profile, host.data(), host.size() * sizeof(double));
   return 0;
 }
 
@@ -1241,7 +1360,7 @@ int fluid_predict_field(const domain_t * domain, const size_t rkstep, const doub
   const int rk = (int)rkstep;
   if (coherent(*c) && push_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
   if (set_dt(*c, dt)) return 1;
-  if ((c->coherence & TCGPU_SYNC_TENSORS) && coherent(*c) && pull_tensors(*c, fluid)) return 1;
+  if ((c->coherence & TCGPU_SYNC_TENSORS) && coherent(*c) && pull_tensors(*c, fluid, c->f())) return 1;
   enqueue_factors(*c);
   enqueue_predict(*c, rk);
   if (coherent(*c)) {
@@ -1298,6 +1417,8 @@ int integrate(const domain_t * domain, fluid_t * fluid, double * dt) {
   if (finish(*c, "integrate")) return 1;
   if (coherent(*c)) {
     if (pull_fields(*c, fluid, TCGPU_FIELDS)) return 1;
+    // the tensors the reference leaves behind: those of the substep-3 input
+    if ((c->coherence & TCGPU_SYNC_TENSORS) && pull_tensors(*c, fluid, tensor_fields(*c))) return 1;
     // three predict calls swap the caller's alpha/beta source buffers three times
     array_t * arrs[4] = {fluid->srcux, fluid->srcuy, fluid->srcuz, fluid->srct};
     for (int v = 0; v < 4; v++) {

@@ -7,6 +7,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
+#include <sys/stat.h>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -267,6 +268,25 @@ int fluid_init(const char dirname_ic[], const domain_t * domain, fluid_t * fluid
     errno = 0;
     *dst[n] = strtod(s, nullptr);
     if (errno != 0) return err(std::string(names[n]) + ": invalid value as double");
+  }
+  return 0;
+}
+
+// The statistics directory of src/statistics.c:250-300: num, the domain, and
+// the eight accumulators as (nz, ny, nx + 1) or (nz, ny, nx + 2) arrays in the
+// order ux1 ux2 uy1 uy2 uz1 uz2 adv dif (array.c:155-222 writes the interior
+// j, k with x's additional cells, which is the device layout as it is). As in
+// the reference, a directory that cannot be created is not an error by itself.
+__attribute__((visibility("hidden"))) int tcgpu_io_write_statistics(const char dirname[], const domain_t * domain,
+                                                                    size_t num, const double * const arrays[8]) {
+  mkdir(dirname, 0755);
+  if (npy_write(dirname, "num", "'<u8'", {}, sizeof(size_t), &num)) return 1;
+  if (domain_save(dirname, domain)) return 1;
+  const size_t nx = domain->glsizes[0], ny = domain->glsizes[1], nz = domain->glsizes[2];
+  static const char * names[8] = {"ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "adv", "dif"};
+  for (int s = 0; s < 8; s++) {
+    const size_t rowlen = (s >= 2 && s <= 5) ? nx + 2 : nx + 1;
+    if (npy_write(dirname, names[s], "'<f8'", {nz, ny, rowlen}, sizeof(double), arrays[s])) return 1;
   }
   return 0;
 }

@@ -272,10 +272,21 @@ struct Tensors { double * a[11]; };  // lxx lxy lxz lyx0 lyx1 lyy0 lyy1 lyz lzx 
 void launch_tensors(const Geo & g, const Coefs & cf, const FieldBufs & f, const Tensors & tn, cudaStream_t st);
 
 // logging reductions (src/logging/*.c); out: 9 doubles on the device,
-// partial: DIAG_BLOCKS x 9 doubles of scratch
+// partial: DIAG_BLOCKS x 9 doubles of scratch; f: current fields, fs: the
+// fields the momentum injection / dissipation tensors are formed from
 constexpr int DIAG_BLOCKS_MAX = 296;
-void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, double nu, double kappa,
-                        double * out, double * partial, cudaStream_t st);
+void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, const FieldBufs & fs,
+                        double nu, double kappa, double * out, double * partial, cudaStream_t st);
+
+// statistics of src/statistics.c:124-240 accumulated on the device, in the
+// reference's dump layouts: ux1, ux2 [k][j][i = 1..nx+1]; uy1, uy2, uz1, uz2
+// [k][j][i = 0..nx+1]; adv, dif [k][j][i = 1..nx+1] (interior j, k only).
+// f: current fields (means, adv); fs: the fields dif's tensors are formed from
+struct Stats { double * a[8]; };     // ux1 ux2 uy1 uy2 uz1 uz2 adv dif
+void launch_statistics(const Geo & g, const Coefs & cf, const FieldBufs & f, const FieldBufs & fs, const Stats & s,
+                       cudaStream_t st);
+// mean of uy1 over j and k, divided by the sample count: nx + 2 values
+void launch_stat_profile(const Geo & g, const double * uy1, double inv_count, double * out, cudaStream_t st);
 
 // FP32-storage mode: rows of nref doubles in the reference's layout to and from
 // rows of pitch floats (element e at e + shift)

@@ -468,9 +468,15 @@ void launch_tensors(const Geo & g, const Coefs & cf, const FieldBufs & f, const 
 // partial[b][0..8]: max|div|, inj_m, inj_s, dis_m, dis_s, e_ux, e_uy, e_uz, e_t
 constexpr int DIAG_BLOCKS = 296;
 
+// f: the current fields (divergence, energies, the wall velocity of the
+// momentum injection, every scalar term); fs: the fields the velocity-gradient
+// tensors are formed from (injection and dissipation of momentum). The
+// reference logs tensors of the last predict's input fields
+// (src/fluid/predict/main.c:56-82, read by src/logging/injection.c:49-51 and
+// dissipation.c); fs = f gives the tensors of the current fields.
 template <class T>
 __global__ void __launch_bounds__(256)
-diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, double * partial) {
+diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, FieldsT<T> fs, double * partial) {
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const long long total = (long long)(nx + 1) * ny * nz;
   double acc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
@@ -478,6 +484,9 @@ diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, double * partial) {
   const T * uy = f.uy;
   const T * uz = f.uz;
   const T * t = f.t;
+  const T * sux = fs.ux;
+  const T * suy = fs.uy;
+  const T * suz = fs.uz;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
        c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % (nx + 1)) + 1;     // 1..nx+1
@@ -489,11 +498,12 @@ diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, double * partial) {
     // face quantities at i
     const double ih = __ldg(cf.c_invhxxf + i);
     const double uyim = (double)uy[sidx_c<T>(g, i - 1, j, k)], uyi = (double)uy[sidx_c<T>(g, i, j, k)];
-    const double lxy = ih * (-uyim + uyi);
-    const double lxz = ih * (-(double)uz[sidx_c<T>(g, i - 1, j, k)] + (double)uz[sidx_c<T>(g, i, j, k)]);
-    const double lyx = __ldg(cf.c_invhyxf + i) * (-(double)ux[sidx_f<T>(g, i, j - 1, k)] + (double)ux[sidx_f<T>(g, i, j, k)])
-                     + __ldg(cf.c_lyx1f + i) * (__ldg(cf.c_wm + i) * uyim + __ldg(cf.c_wp + i) * uyi);
-    const double lzx = cf.inv_hz * (-(double)ux[sidx_f<T>(g, i, j, k - 1)] + (double)ux[sidx_f<T>(g, i, j, k)]);
+    const double suyim = (double)suy[sidx_c<T>(g, i - 1, j, k)], suyi = (double)suy[sidx_c<T>(g, i, j, k)];
+    const double lxy = ih * (-suyim + suyi);
+    const double lxz = ih * (-(double)suz[sidx_c<T>(g, i - 1, j, k)] + (double)suz[sidx_c<T>(g, i, j, k)]);
+    const double lyx = __ldg(cf.c_invhyxf + i) * (-(double)sux[sidx_f<T>(g, i, j - 1, k)] + (double)sux[sidx_f<T>(g, i, j, k)])
+                     + __ldg(cf.c_lyx1f + i) * (__ldg(cf.c_wm + i) * suyim + __ldg(cf.c_wp + i) * suyi);
+    const double lzx = cf.inv_hz * (-(double)sux[sidx_f<T>(g, i, j, k - 1)] + (double)sux[sidx_f<T>(g, i, j, k)]);
     // dissipation.c:40-151 (face contributions)
     acc[3] += jdf * lyx * (lyx + lxy);
     acc[3] += jdf * lzx * (lzx + lxz);
@@ -530,12 +540,15 @@ diag_kernel(Geo g, Coefs cf, Bc bc, FieldsT<T> f, double * partial) {
           - __ldg(cf.c_e2 + i) * uz0 + __ldg(cf.c_e2 + i) * uz1);
       acc[0] = fmax(acc[0], fabs(div));
       // centre tensors and dissipation contributions
-      const double lxx = (1. / __ldg(g.hxxc + i)) * (-ux0 + ux1);
+      const double sux0 = (double)sux[sidx_f<T>(g, i, j, k)], sux1 = (double)sux[sidx_f<T>(g, i + 1, j, k)];
+      const double suy0 = suyi, suy1 = (double)suy[sidx_c<T>(g, i, j + 1, k)];
+      const double suz0 = (double)suz[sidx_c<T>(g, i, j, k)], suz1 = (double)suz[sidx_c<T>(g, i, j, k + 1)];
+      const double lxx = (1. / __ldg(g.hxxc + i)) * (-sux0 + sux1);
       const double ihy = __ldg(cf.c_invhyxc + i);
-      const double lyy = ihy * (-uy0 + uy1) + __ldg(cf.c_lyy1 + i) * (0.5 * ux0 + 0.5 * ux1);
-      const double lyz = ihy * (-(double)uz[sidx_c<T>(g, i, j - 1, k)] + uz0);
-      const double lzy = cf.inv_hz * (-(double)uy[sidx_c<T>(g, i, j, k - 1)] + uy0);
-      const double lzz = cf.inv_hz * (-uz0 + uz1);
+      const double lyy = ihy * (-suy0 + suy1) + __ldg(cf.c_lyy1 + i) * (0.5 * sux0 + 0.5 * sux1);
+      const double lyz = ihy * (-(double)suz[sidx_c<T>(g, i, j - 1, k)] + suz0);
+      const double lzy = cf.inv_hz * (-(double)suy[sidx_c<T>(g, i, j, k - 1)] + suy0);
+      const double lzz = cf.inv_hz * (-suz0 + suz1);
       acc[3] += jdc * lxx * (lxx + lxx);
       acc[3] += jdc * lyy * (lyy + lyy);
       acc[3] += jdc * lzy * (lzy + lyz);
@@ -584,11 +597,83 @@ __global__ void diag_final_kernel(const double * partial, int nblocks, double nu
   out[q] = v;
 }
 
-void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, double nu, double kappa,
-                        double * out, double * partial, cudaStream_t st) {
-  if (f.bytes == 4) diag_kernel<float><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<float>(), partial);
-  else diag_kernel<double><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<double>(), partial);
+void launch_diagnostics(const Geo & g, const Coefs & cf, const Bc & bc, const FieldBufs & f, const FieldBufs & fs,
+                        double nu, double kappa, double * out, double * partial, cudaStream_t st) {
+  if (f.bytes == 4) diag_kernel<float><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<float>(), fs.as<float>(), partial);
+  else diag_kernel<double><<<DIAG_BLOCKS, 256, 0, st>>>(g, cf, bc, f.as<double>(), fs.as<double>(), partial);
   diag_final_kernel<<<1, 32, 0, st>>>(partial, DIAG_BLOCKS, nu, kappa, out);
+}
+
+// --------------------------------------------------------------- statistics
+// src/statistics.c:124-240: one thread per (i = 0..nx+1, j, k) of the interior
+// j, k adds this sample to the eight accumulators. Products and sums are
+// rounded separately (no contraction), as the reference's C does, so the
+// accumulated values follow its arithmetic.
+template <class T>
+__global__ void stats_kernel(Geo g, Coefs cf, FieldsT<T> f, FieldsT<T> fs, Stats st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;   // 0..nx+1
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  const int nx = g.nx, ny = g.ny;
+  if (i > nx + 1 || j > ny) return;
+  const size_t line = (size_t)(j - 1) + (size_t)ny * (k - 1);
+  {  // uy, uz at i = 0..nx+1 (statistics.c:146-185)
+    const size_t q = (size_t)i + (size_t)(nx + 2) * line;
+    const double vy = (double)f.uy[sidx_c<T>(g, i, j, k)], vz = (double)f.uz[sidx_c<T>(g, i, j, k)];
+    st.a[2][q] = __dadd_rn(st.a[2][q], vy);
+    st.a[3][q] = __dadd_rn(st.a[3][q], __dmul_rn(vy, vy));
+    st.a[4][q] = __dadd_rn(st.a[4][q], vz);
+    st.a[5][q] = __dadd_rn(st.a[5][q], __dmul_rn(vz, vz));
+  }
+  if (i < 1) return;
+  const size_t q = (size_t)(i - 1) + (size_t)(nx + 1) * line;
+  const double vx = (double)f.ux[sidx_f<T>(g, i, j, k)];
+  st.a[0][q] = __dadd_rn(st.a[0][q], vx);                 // :126-144
+  st.a[1][q] = __dadd_rn(st.a[1][q], __dmul_rn(vx, vx));
+  {  // adv (:187-204): ux averaged to the y face times uy averaged to the x face
+    const double x = __dadd_rn(__dmul_rn(0.5, (double)f.ux[sidx_f<T>(g, i, j - 1, k)]), __dmul_rn(0.5, vx));
+    const double y = __dadd_rn(__dmul_rn(0.5, (double)f.uy[sidx_c<T>(g, i - 1, j, k)]),
+                               __dmul_rn(0.5, (double)f.uy[sidx_c<T>(g, i, j, k)]));
+    st.a[6][q] = __dadd_rn(st.a[6][q], __dmul_rn(x, y));
+  }
+  {  // dif (:206-223): lyx0 + lyx1 + lxy (predict/lyx.c:24-83, lxy.c:19-49) of fs
+    const double uym = (double)fs.uy[sidx_c<T>(g, i - 1, j, k)], uy0 = (double)fs.uy[sidx_c<T>(g, i, j, k)];
+    const double lyx0 = __dmul_rn(__ldg(cf.c_invhyxf + i),
+                                  __dadd_rn(-(double)fs.ux[sidx_f<T>(g, i, j - 1, k)], (double)fs.ux[sidx_f<T>(g, i, j, k)]));
+    const double lyx1 = __dmul_rn(__ldg(cf.c_lyx1f + i),
+                                  __dadd_rn(__dmul_rn(__ldg(cf.c_wm + i), uym), __dmul_rn(__ldg(cf.c_wp + i), uy0)));
+    const double lxy = __dmul_rn(__ldg(cf.c_invhxxf + i), __dadd_rn(-uym, uy0));
+    st.a[7][q] = __dadd_rn(st.a[7][q], __dadd_rn(__dadd_rn(lyx0, lyx1), lxy));
+  }
+}
+
+void launch_statistics(const Geo & g, const Coefs & cf, const FieldBufs & f, const FieldBufs & fs, const Stats & s,
+                       cudaStream_t st) {
+  dim3 block(64, 4, 1);
+  dim3 grid((g.nx + 2 + 63) / 64, (g.ny + 3) / 4, g.nz);
+  if (f.bytes == 4) stats_kernel<float><<<grid, block, 0, st>>>(g, cf, f.as<float>(), fs.as<float>(), s);
+  else stats_kernel<double><<<grid, block, 0, st>>>(g, cf, f.as<double>(), fs.as<double>(), s);
+}
+
+// mean uy(r): out[i] = inv_count * sum over j, k of uy1[k][j][i], one block per i
+__global__ void stat_profile_kernel(Geo g, const double * __restrict__ uy1, double inv_count, double * out) {
+  const int i = blockIdx.x;
+  const size_t lines = (size_t)g.ny * g.nz;
+  double acc = 0.;
+  for (size_t l = threadIdx.x; l < lines; l += blockDim.x) acc += uy1[(size_t)i + (size_t)(g.nx + 2) * l];
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w];
+    out[i] = v * inv_count;
+  }
+}
+
+void launch_stat_profile(const Geo & g, const double * uy1, double inv_count, double * out, cudaStream_t st) {
+  stat_profile_kernel<<<g.nx + 2, 256, 0, st>>>(g, uy1, inv_count, out);
 }
 
 // --------------------------------------------------------------- FP32 storage

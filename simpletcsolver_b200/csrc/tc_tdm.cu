@@ -235,12 +235,14 @@ extern "C" const tdm_t tdm = {
 
 // ---------------------------------------------------------------- allocation-free solve
 // For callers that must not allocate device memory themselves or have the
-// library do it: code running inside a CUDA graph capture or a memory-pool-
-// managed framework, embedded/real-time hosts that pre-reserve all device
-// memory up front, or plugins whose allocator belongs to someone else. The
+// library do it: a framework that owns the whole device memory pool, a
+// real-time host that reserves all device memory up front and may not allocate
+// afterwards, or a plugin whose allocator belongs to someone else. The
 // elimination-factor table that tdm.solve() keeps in cudaMalloc'd memory lives
 // here in a fixed static device array instead; the caller supplies the
-// coefficients (host) and the right-hand sides (device memory, solved in place).
+// coefficients (host) and the right-hand sides (device memory of the current
+// device, solved in place). The work is ordered on the legacy default stream
+// and finished before the call returns.
 namespace {
 
 constexpr int kNoAllocMax = TCGPU_TDM_NOALLOC_MAX_SIZE;
@@ -271,6 +273,8 @@ extern "C" int tcgpu_tdm_solve_noalloc(int size, int nrhs, bool is_periodic, boo
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
     return tcgpu_report_error("tcgpu_tdm_solve_noalloc: no current device");
+  if (attr.type == cudaMemoryTypeDevice && attr.device != dev)
+    return tcgpu_report_error("tcgpu_tdm_solve_noalloc: data is device memory of another device than the current one");
   if (g_noalloc_dev[dev] == nullptr) {
     // set-up once per device, with that device current: the symbol's device
     // address (the name itself is only a host-side stand-in)

@@ -147,6 +147,49 @@ class Solver:
                 "energy_ux", "energy_uy", "energy_uz", "energy_t")
         return dict(zip(keys, list(out)))
 
+    def log_quantities(self) -> dict:
+        """The nine logging quantities with the reference's semantics (tensors
+        of the last predict's input fields; src/logging/*.c after integrate())."""
+        out = (C.c_double * 9)()
+        self._check(self.lib.tcgpu_log_quantities(C.byref(self.domain), C.byref(self.fluid), out), "log_quantities")
+        keys = ("divmax", "injection_u", "injection_t", "dissipation_u", "dissipation_t",
+                "energy_ux", "energy_uy", "energy_uz", "energy_t")
+        return dict(zip(keys, list(out)))
+
+    # ---------------------------------------------------------------- statistics (src/statistics.c)
+    STAT_NAMES = ("ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "adv", "dif")
+
+    def stats_collect(self):
+        self._check(self.lib.tcgpu_statistics_collect(C.byref(self.domain), C.byref(self.fluid)), "statistics_collect")
+
+    def stats_reset(self):
+        self._check(self.lib.tcgpu_statistics_reset(C.byref(self.domain), C.byref(self.fluid)), "statistics_reset")
+
+    def stats(self) -> tuple[int, dict]:
+        """(samples, {name: array [k, j, i]}) of the device accumulators."""
+        arrays = {}
+        ptrs = (abi.c_double_p * 8)()
+        for s, name in enumerate(self.STAT_NAMES):
+            row = self.nx + 2 if name[:2] in ("uy", "uz") else self.nx + 1
+            arrays[name] = np.zeros((self.nz, self.ny, row))
+            ptrs[s] = arrays[name].ctypes.data_as(abi.c_double_p)
+        num = C.c_size_t(0)
+        self._check(self.lib.tcgpu_statistics_get(C.byref(self.domain), C.byref(self.fluid), C.byref(num), ptrs),
+                    "statistics_get")
+        return int(num.value), arrays
+
+    def stats_save(self, dirname: str):
+        os.makedirs(dirname, exist_ok=True)
+        self._check(self.lib.tcgpu_statistics_save(dirname.encode(), C.byref(self.domain), C.byref(self.fluid)),
+                    "statistics_save")
+
+    def mean_uy(self) -> np.ndarray:
+        """Mean azimuthal velocity profile uy(r), i = 0..nx+1, over j, k and the samples."""
+        out = np.zeros(self.nx + 2)
+        self._check(self.lib.tcgpu_statistics_mean_uy(C.byref(self.domain), C.byref(self.fluid),
+                                                      out.ctypes.data_as(abi.c_double_p)), "statistics_mean_uy")
+        return out
+
     def save(self, dirname: str, step: int = 0, time: float = 0.0):
         """Reference save layout (src/save.c:74-110): step, time, domain, fluid."""
         os.makedirs(dirname, exist_ok=True)

@@ -1,0 +1,239 @@
+"""Parity at the workloads' own kernel paths, the 1000-step Taylor-Couette
+run, and the energy properties the scheme guarantees.
+
+Reference runs use the reference compiled from its own sources
+(oracle/_ref/tcref_<cfg>) on the host; they start together, in the
+background, the first time a test needs one, and the GPU work of each test
+overlaps them.
+
+* Planar channel at 192x512x256 (Re 2000, implicit diffusion in x, y and z,
+  scalar): 5 steps, every field within 1e-10 relative L2 (p after removing
+  its mean).
+* Taylor-Couette at Re 1e4 with 1024 azimuthal points: 256x1024x128 (the
+  headline grid's predict kernel shape, 256 radial points, and its 64-plane
+  march chunk) and 64x1024x512 (the headline grid's 512-point axial
+  transforms): 5 steps each, 1e-10.
+* Taylor-Couette at 64x128x64, Re 3400: 1000 steps; 1e-10 after 100 steps;
+  the drift after 500 and 1000 steps is printed and bounded.
+* Energy: at the steady Taylor-vortex state of the reference's "typical"
+  example (Re 80, radius ratio 1/2, 64x8x32) energy injection equals
+  dissipation to round-off (README.md:81); with Re = 1e16 the loss of kinetic
+  energy over a fixed time scales as dt^3 (docs/source/example/energy).
+"""
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from simpletcsolver_b200 import ic
+from simpletcsolver_b200.solver import Solver
+from tests._helpers import REF_DIR, have_ref, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+RUNS = {
+    # name: (build, case, steps, saved step list)
+    "planar_192x512x256": ("planar", ic.PLANAR, 5, ""),
+    "tc_256x1024x128": ("tc", ic.taylor_couette(256, 1024, 128, 1.0e4), 5, ""),
+    "tc_64x1024x512": ("tc", ic.taylor_couette(64, 1024, 512, 1.0e4), 5, ""),
+    "tc_64x128x64_1000": ("tc", ic.TC_SMALL, 1000, "100,500"),
+}
+
+
+class RefRuns:
+    """The reference runs of this module, started together in the background."""
+
+    def __init__(self, root):
+        self.root = root
+        self.procs = {}
+        for name, (build, case, steps, saves) in RUNS.items():
+            d0 = ic.write_ic(case, os.path.join(root, name, "ic"))
+            out = os.path.join(root, name, "ref")
+            env = dict(os.environ, **ic.case_env(case))
+            args = [os.path.join(REF_DIR, f"tcref_{build}"), d0, "0", str(steps), out] + ([saves] if saves else [])
+            self.procs[name] = (subprocess.Popen(args, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                                 text=True), d0, out)
+
+    def ic(self, name):
+        return self.procs[name][1]
+
+    def result(self, name):
+        p, _, out = self.procs[name]
+        stdout, stderr = p.communicate(timeout=3000)
+        assert p.returncode == 0, stderr
+        return out
+
+    def close(self):
+        for p, _, _ in self.procs.values():
+            if p.poll() is None:
+                p.kill()
+                p.wait()
+
+
+@pytest.fixture(scope="module")
+def refs(tmp_path_factory):
+    if not (have_ref("tc") and have_ref("planar")):
+        pytest.skip("reference build oracle/_ref absent")
+    r = RefRuns(str(tmp_path_factory.mktemp("configs")))
+    yield r
+    r.close()
+
+
+def compare(s, out, tol):
+    """GPU state (pulled) against a reference save directory: relative L2 of
+    the interiors, p without its mean."""
+    errs = {}
+    for n in ("ux", "uy", "uz", "t"):
+        errs[n] = rel_l2(s.field(n)[1:-1, 1:-1], np.load(os.path.join(out, n + ".npy")))
+    gp = s.field("p")[1:-1, 1:-1]
+    rp = np.load(os.path.join(out, "p.npy"))
+    errs["p"] = rel_l2(gp - gp[:, :, 1:-1].mean(), rp - rp[:, :, 1:-1].mean())
+    bad = {k: v for k, v in errs.items() if not v < tol}
+    assert not bad, f"fields beyond {tol:g}: {bad}"
+    return errs
+
+
+@pytest.mark.parametrize("name", ["planar_192x512x256", "tc_256x1024x128", "tc_64x1024x512"])
+def test_five_steps_at_workload_kernel_paths(lib, refs, name):
+    build, case, steps, _ = RUNS[name]
+    s = Solver.from_ic(refs.ic(name), case=case, lib=lib)
+    try:
+        s.push()
+        dts = s.run(steps)
+        s.pull()
+        divmax = s.diagnostics()["divmax"]
+        out = refs.result(name)
+        errs = compare(s, out, 1e-10)
+        ref_time = float(np.load(os.path.join(out, "time.npy")))
+        assert float(np.sum(dts)) == pytest.approx(ref_time, rel=1e-13)
+        print(f"{name}: {steps} steps, relative L2 " + ", ".join(f"{k} {v:.2e}" for k, v in errs.items()) +
+              f", max|div| {divmax:.2e}")
+        xf = np.load(os.path.join(refs.ic(name), "xf.npy"))
+        assert divmax < 1e-13 / float(np.min(np.diff(xf)))   # round-off of the largest velocity gradient
+    finally:
+        s.release()
+
+
+def test_taylor_couette_1000_steps(lib, refs):
+    """The CPU-runnable workload for its full 1000 steps: within 1e-10 after
+    100 steps (the oracle bar); the drift after 500 and 1000 steps is
+    printed. The flow at Re 3400 is unsteady, so round-off differences grow;
+    they stay below 1e-7 over these 1000 steps."""
+    name = "tc_64x128x64_1000"
+    _, case, _, _ = RUNS[name]
+    s = Solver.from_ic(refs.ic(name), case=case, lib=lib)
+    try:
+        s.push()
+        states = {}
+        done = 0
+        for n in (100, 500, 1000):
+            s.run(n - done)
+            done = n
+            s.pull()
+            states[n] = {f: s.field(f).copy() for f in ("ux", "uy", "uz", "t", "p")}
+            states[n]["divmax"] = s.diagnostics()["divmax"]
+        out = refs.result(name)
+        drift = {}
+        for n in (100, 500, 1000):
+            d = out if n == 1000 else os.path.join(out, f"step{n:010d}")
+            st = states[n]
+            e = {f: rel_l2(st[f][1:-1, 1:-1], np.load(os.path.join(d, f + ".npy"))) for f in ("ux", "uy", "uz")}
+            gp, rp = st["p"][1:-1, 1:-1], np.load(os.path.join(d, "p.npy"))
+            e["p"] = rel_l2(gp - gp[:, :, 1:-1].mean(), rp - rp[:, :, 1:-1].mean())
+            drift[n] = e
+            assert st["divmax"] < 1e-12
+        print("1000-step drift (relative L2): " + "; ".join(
+            f"step {n}: " + ", ".join(f"{k} {v:.2e}" for k, v in e.items()) for n, e in drift.items()))
+        assert max(drift[100].values()) < 1e-10
+        assert max(drift[500].values()) < 1e-7 and max(drift[1000].values()) < 1e-7
+    finally:
+        s.release()
+
+
+# --------------------------------------------------------------------------- energy
+TYPICAL = ic.Case(is_curved=True, nx=64, ny=8, nz=32, lx=1.0, ly=math.pi / 8.0, lz=2.0, Re=80.0, Pr=1.0,
+                  noise_u=0.05, seed=3, coef_dt_adv=1.0, coef_dt_dif=1.0)
+
+
+def test_injection_balances_dissipation_at_steady_state(lib, tmp_path):
+    """docs/source/example/typical (exec.sh: Re 80, ri 1, ro 2, ly pi/8, lz 2,
+    64x8x32, CFL coefficients 1): run to t = 400, where the Taylor vortices
+    are steady; injection and dissipation of kinetic energy (and of the
+    scalar's squared norm) agree to round-off, while they differ at the
+    start."""
+    d0 = ic.write_ic(TYPICAL, str(tmp_path / "ic"))
+    s = Solver.from_ic(d0, case=TYPICAL, lib=lib)
+    try:
+        s.push()
+        q0 = s.log_quantities()
+        time, gaps = 0.0, []
+        while time < 400.0:
+            time += float(np.sum(s.run(64)))
+            q = s.log_quantities()
+            gaps.append((time, abs(q["injection_u"] - q["dissipation_u"]) / q["dissipation_u"],
+                         abs(q["injection_t"] - q["dissipation_t"]) / q["dissipation_t"]))
+        start = abs(q0["injection_u"] - q0["dissipation_u"]) / q0["dissipation_u"]
+        print(f"injection vs dissipation, relative: start {start:.2e}; " +
+              ", ".join(f"t {t:.0f}: {g:.2e} / {h:.2e}" for t, g, h in gaps[::max(1, len(gaps) // 8)]) +
+              f"; end {gaps[-1][1]:.2e} / {gaps[-1][2]:.2e}")
+        assert start > 1e-3
+        assert gaps[-1][1] < 1e-10 and gaps[-1][2] < 1e-10
+        assert q["divmax"] < 1e-12
+        # a steady state: the energy no longer changes
+        e1 = sum(q[k] for k in ("energy_ux", "energy_uy", "energy_uz"))
+        s.run(64)
+        q2 = s.log_quantities()
+        e2 = sum(q2[k] for k in ("energy_ux", "energy_uy", "energy_uz"))
+        assert abs(e2 - e1) / e1 < 1e-12
+    finally:
+        s.release()
+
+
+ENERGY = ic.Case(is_curved=True, nx=32, ny=16, nz=32, lx=1.0, ly=math.pi / 4.0, lz=2.0, Re=1.0e16, Pr=1.0,
+                 noise_u=0.05, seed=5, coef_dt_adv=1.0, coef_dt_dif=1.0)
+
+
+def test_energy_loss_is_third_order_in_dt(lib, tmp_path):
+    """docs/source/example/energy (exec.sh: Re 1e16, ri 1, ro 2, ly pi/4, lz
+    2, 32x16x32): develop the flow to t = 10, then run to t = 15 with
+    coef_dt_adv 0.1, 0.2, 0.4, 0.8 (coef_dt_dif 0.95). The discrete kinetic
+    energy is conserved by the spatial scheme, so its loss -dE/E0 comes from
+    the explicit Runge-Kutta steps and falls as dt^3 (energy.py:70)."""
+    d0 = ic.write_ic(ENERGY, str(tmp_path / "ic"))
+    s = Solver.from_ic(d0, case=ENERGY, lib=lib)
+    try:
+        s.push()
+        time = 0.0
+        while time < 10.0:
+            time += float(np.sum(s.run(16)))
+        s.pull()
+        dev = str(tmp_path / "developed")
+        s.save(dev, step=0, time=time)
+    finally:
+        s.release()
+    loss = {}
+    for factor in (0.1, 0.2, 0.4, 0.8):
+        case = ic.Case(**{**ENERGY.__dict__, "coef_dt_adv": factor, "coef_dt_dif": 0.95})
+        r = Solver.from_ic(dev, case=case, lib=lib)
+        try:
+            r.push()
+            q = r.log_quantities()
+            e0 = q["energy_ux"] + q["energy_uy"] + q["energy_uz"]
+            t = time
+            while True:                      # the reference loop stops once time passes timemax
+                dt = float(r.run(1)[0])
+                t += dt
+                if t > 15.0:
+                    break
+            q = r.log_quantities()
+            loss[factor] = 1.0 - (q["energy_ux"] + q["energy_uy"] + q["energy_uz"]) / e0
+        finally:
+            r.release()
+    f = np.array(sorted(loss))
+    y = np.array([loss[k] for k in f])
+    slope = float(np.polyfit(np.log(f), np.log(y), 1)[0])
+    print("energy loss -dE/E0 at t = 15: " + ", ".join(f"{k}: {loss[k]:.3e}" for k in f) + f"; slope {slope:.2f}")
+    assert np.all(y > 0)
+    assert 2.6 < slope < 3.4

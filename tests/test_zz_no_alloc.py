@@ -1,10 +1,10 @@
 """The allocation-free tri-diagonal solve (tcgpu_tdm_solve_noalloc).
 
 It exists for callers that may not allocate device memory, or have a library
-do so on their behalf: code running during CUDA graph capture, frameworks that
-own the device memory pool, or hosts that reserve all device memory up front.
-Its factor table lives in a fixed static device array instead of cudaMalloc'd
-memory. Here it is called through the C ABI and checked against the ordinary
+do so on their behalf: frameworks that own the whole device memory pool,
+real-time hosts that reserve all device memory up front, or plugins whose
+allocations belong to their host. Its factor table lives in a fixed static
+device array instead of cudaMalloc'd memory. Here it is called through the C ABI and checked against the ordinary
 tdm.solve() entry point on the same systems, for two calls in a row (the
 second with a different system, so nothing may carry over from the first).
 Both run the same arithmetic, so the answers must agree exactly, the same
