@@ -13,8 +13,8 @@ overlaps them.
   headline grid's predict kernel shape, 256 radial points, and its 64-plane
   march chunk) and 64x1024x512 (the headline grid's 512-point axial
   transforms): 5 steps each, 1e-10.
-* Taylor-Couette at 64x128x64, Re 3400: 1000 steps; 1e-10 after 100 steps;
-  the drift after 500 and 1000 steps is printed and bounded.
+* Taylor-Couette at 64x128x64, Re 3400: 1000 steps, 1e-10 after 100, 500
+  and 1000 steps; the drift at each is printed.
 * Energy: at the steady Taylor-vortex state of the reference's "typical"
   example (Re 80, radius ratio 1/2, 64x8x32) energy injection equals
   dissipation to round-off (README.md:81); with Re = 1e16 the loss of kinetic
@@ -118,9 +118,9 @@ def test_five_steps_at_workload_kernel_paths(lib, refs, name):
 
 def test_taylor_couette_1000_steps(lib, refs):
     """The CPU-runnable workload for its full 1000 steps: within 1e-10 after
-    100 steps (the oracle bar); the drift after 500 and 1000 steps is
-    printed. The flow at Re 3400 is unsteady, so round-off differences grow;
-    they stay below 1e-7 over these 1000 steps."""
+    100, 500 and 1000 steps (measured on a B200: at most 3e-14 after 100
+    steps and 9e-14 after 1000, p after removing its mean); the drift at each
+    checkpoint is printed."""
     name = "tc_64x128x64_1000"
     _, case, _, _ = RUNS[name]
     s = Solver.from_ic(refs.ic(name), case=case, lib=lib)
@@ -146,8 +146,8 @@ def test_taylor_couette_1000_steps(lib, refs):
             assert st["divmax"] < 1e-12
         print("1000-step drift (relative L2): " + "; ".join(
             f"step {n}: " + ", ".join(f"{k} {v:.2e}" for k, v in e.items()) for n, e in drift.items()))
-        assert max(drift[100].values()) < 1e-10
-        assert max(drift[500].values()) < 1e-7 and max(drift[1000].values()) < 1e-7
+        for n in (100, 500, 1000):
+            assert max(drift[n].values()) < 1e-10, n
     finally:
         s.release()
 
