@@ -215,13 +215,21 @@ def cpu_reference_run(steps: int, warmup: int):
             kind = "reference"
             runs = [subprocess.Popen([binary, d0, str(max(1, warmup)), str(steps)], env=env, stdout=subprocess.PIPE,
                                      stderr=subprocess.DEVNULL, text=True) for _ in range(procs)]
-            rates = []
+            rates, bounds, fft, total = [], [], 0.0, 0.0
             for r in runs:
                 out, _ = r.communicate(timeout=3600)
                 line = [x for x in out.splitlines() if x.startswith("{")][-1]
                 res = json.loads(line)
                 rates.append(res["cells"] * res["steps"] / res["seconds"] / 1e6)
+                # the same process with its transforms taking no time at all
+                bounds.append(res["cells"] * res["steps"] / (res["seconds"] - res["fft_seconds"]) / 1e6)
+                fft += res["fft_seconds"]
+                total += res["seconds"]
             value = sum(rates)
+            extra = {"fft_share": fft / total, "value_bound_free_fft": sum(bounds),
+                     "fft_note": ("FFTW is replaced by an FP64 radix-2 shim (oracle/shim/fftw_shim.c); "
+                                  "value_bound_free_fft is the throughput if the reference's transforms took no time, "
+                                  "an upper bound for any FFT library")}
             sample = (f"{procs} concurrent single-rank reference processes (oracle/_ref/tcref_tc, the reference's "
                       f"own C sources), each {nx}x{ny}x{nz} at Re=1e4, {warmup} warm-up + {steps} timed steps; "
                       f"rates summed")
@@ -239,7 +247,35 @@ def cpu_reference_run(steps: int, warmup: int):
             value = case.ncells * n / (time.perf_counter() - t0) / 1e6
             procs = 1
             sample = f"numpy restatement, 1 process, {nx}x{ny}x{nz}, {n} steps"
-    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample}
+    out = {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample}
+    if kind == "reference":
+        out.update(extra)
+    return out
+
+
+def start_planar_reference(d0, case):
+    """The reference's own integrate() on the planar workload's full grid,
+    one single-rank process (1 warm-up + 1 timed step), in the background."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "tcref_planar")
+    if not os.path.exists(binary):
+        return None
+    from simpletcsolver_b200 import ic
+    env = dict(os.environ, **ic.case_env(case))
+    return subprocess.Popen([binary, d0, "1", "1"], env=env, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                            text=True)
+
+
+def finish_planar_reference(proc, case):
+    if proc is None:
+        return None
+    out, _ = proc.communicate(timeout=3600)
+    if proc.returncode != 0:
+        return None
+    res = json.loads([x for x in out.splitlines() if x.startswith("{")][-1])
+    return {"value": res["cells"] * res["steps"] / res["seconds"] / 1e6, "unit": UNIT, "cores": 1,
+            "kind": "reference", "fft_share": res["fft_seconds"] / res["seconds"],
+            "sample": (f"oracle/_ref/tcref_planar on the full {case.nx}x{case.ny}x{case.nz} grid, one single-rank "
+                       f"process, 1 warm-up + 1 timed step (the reference cannot be decomposed here)")}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -464,6 +500,7 @@ def planar_arm(args, lib, world, peak):
     K, W = args.steps, args.warmup
     out = {"workload": f"planar channel {case.nx}x{case.ny}x{case.nz} Re=2000 Pr=1 implicit xyz",
            "steps": K, "bytes_per_cell_step_model": MODEL_BYTES_PER_CELL_STEP_PLANAR}
+    ref = start_planar_reference(d0, case) if (world == 1 and not args.no_cpu_baseline) else None
     for storage, key in ((8, "fp64"), (4, "fp32_storage")):
         s = Solver.from_ic(d0, case=case, lib=lib, storage=storage)
         try:
@@ -479,6 +516,11 @@ def planar_arm(args, lib, world, peak):
                                                / 1e9 / peak)
         finally:
             s.release()
+    cpu = finish_planar_reference(ref, case)
+    if cpu is not None:
+        # the same grid and configuration on both arms: one core of the reference against one GPU
+        out["cpu_reference_same_grid"] = cpu
+        out["fp64"]["vs_cpu_reference_1core"] = out["fp64"]["value"] / cpu["value"]
     return out
 
 

@@ -46,6 +46,10 @@ fftw_plan fftw_plan_many_dft(
     int sign, unsigned flags);
 
 void fftw_execute(const fftw_plan plan);
+
+/* not part of FFTW: wall seconds spent inside fftw_execute so far, so that a
+ * timing driver can state the transforms' share of a step */
+extern double tcref_fft_seconds;
 void fftw_destroy_plan(fftw_plan plan);
 
 #endif // TCREF_SHIM_FFTW3_H

@@ -7,17 +7,20 @@
 // implicit solve (src/tdm.c:17-50), and u + delta into the other buffer of the
 // pair with walls and periodic images (boundary/*.c, halo.c).
 //
-// Per CTA, a ring of three plane slots in shared memory holds the rows
-// j-1 .. j+JT of ux, uy, uz, t, j-1 .. j+JT-1 of p and the previous
-// substep's source terms of the CTA's lines for planes k and k+1, while plane
-// k+2 streams in: one bulk asynchronous copy (cp.async.bulk, completion counted
-// in bytes on an mbarrier) per row, issued one plane ahead by one thread.
-// Values a cell needs from plane k-1 (ux at faces i, i+1; uy at rows j, j+1;
-// uz, p, t at j) are the ones the same thread read one plane earlier and stay
-// in registers; the metric coefficients depend on i only, are folded into one
-// product per stencil term on the host (the P_* tables) and are loaded once
-// per thread. The radial systems of the JT lines are solved one per warp with
-// shuffle scans of affine maps.
+// Per CTA, a ring of four plane slots in shared memory holds the rows
+// j-1 .. j+JT of ux, uy, uz, t and j-1 .. j+JT-1 of p for planes k and k+1,
+// while planes k+2 and k+3 stream in: one bulk asynchronous copy
+// (cp.async.bulk, completion counted in bytes on an mbarrier) per row, issued
+// two planes ahead by one thread; the previous substep's source terms of the
+// CTA's lines arrive one plane ahead into a buffer of their own. Values a cell
+// needs from plane k-1 (ux at faces i, i+1; uy at rows j, j+1; uz, p, t at j)
+// are the ones the same thread read one plane earlier and stay in registers;
+// the metric coefficients depend on i only, are folded into one product per
+// stencil term on the host (the P_* tables) and are loaded once per thread.
+// The radial systems are solved by a warpgroup of their own (one warp per
+// variable, shuffle scans of affine maps) while the other warps form the next
+// plane's right-hand sides; the roles split the register file unevenly
+// (setmaxnreg) and meet only at mbarriers.
 //
 // Row copies start and end on 16-byte boundaries as bulk copies require: a row
 // of n doubles starting at element s is copied from s & ~1 up to the even
@@ -94,49 +97,46 @@ enum SlotField { SF_UX = 0, SF_UY = 1, SF_UZ = 2, SF_T = 3, SF_P = 4 };
 // (P_* tables); each is spelled out below where it is used.
 struct CoefA {
   double xa1, xa2, xa3, yb1, yb2, zc1, zc2, h1, h2;   // ux advection
-  double lxl, lxc, lxu, lyl, lyc, lyu;                // ux Laplacian, x and y
+  double lxl, lxu, ly;                                // ux Laplacian, x and y (carry 2 nu, nu)
   double cy1, cy2, ca1, ca2, cz1, px;                 // ux cross diffusion, pressure gradient
   double tx0, tx1, ty, tz;                            // t advection
-  double clxl, clxc, clxu, clyl, clyc, clyu;          // t Laplacian, x and y
 };
 struct CoefB {
   double a1, a2, b, c, h;                             // uy / uz advection
-  double lxl, lxc, lxu, lyl, lyc, lyu;                // centred Laplacian, x and y
+  double lxl, lxu, ly;                                // centred Laplacian, x and y (carry nu; t: x kappa/nu)
   double p1, p2, qm, q0, qp, yk, yz, py;              // uy cross diffusion, pressure gradient
   double zx0, zx1, zy;                                // uz cross diffusion
 };
+// The Laplacians in x and y are applied as differences from the centre value:
+// the centre coefficients of the tables are the negated sums of the others
+// (F_LXC = -F_LXL - F_LXU, F_LYC = -2 F_LYL = -2 F_LYU, likewise for C_*), so
+// l a + c b + u d = l (a - b) + u (d - b) and only l and u are held.
 
 __device__ __forceinline__ void load_coefs(CoefA & q, const Coefs & cf, int i) {
   const double * __restrict__ b = cf.tab + i;
 #define CF(T) LD(b + (T) * CSTRIDE)
   q.xa1 = CF(P_XA1); q.xa2 = CF(P_XA2); q.xa3 = CF(P_XA3); q.yb1 = CF(P_YB1); q.yb2 = CF(P_YB2);
   q.zc1 = CF(P_ZC1); q.zc2 = CF(P_ZC2); q.h1 = CF(P_H1); q.h2 = CF(P_H2);
-  q.lxl = CF(F_LXL); q.lxc = CF(F_LXC); q.lxu = CF(F_LXU); q.lyl = CF(F_LYL); q.lyc = CF(F_LYC); q.lyu = CF(F_LYU);
+  q.lxl = CF(F_LXL); q.lxu = CF(F_LXU); q.ly = CF(F_LYL);
   q.cy1 = CF(P_CY1); q.cy2 = CF(P_CY2); q.ca1 = CF(P_CA1); q.ca2 = CF(P_CA2); q.cz1 = CF(P_CZ1);
   q.px = CF(C_INVHXXF);
   q.tx0 = CF(P_TX0); q.tx1 = CF(P_TX1); q.ty = CF(P_TY); q.tz = CF(P_TZ);
-  q.clxl = CF(C_LXL); q.clxc = CF(C_LXC); q.clxu = CF(C_LXU); q.clyl = CF(C_LYL); q.clyc = CF(C_LYC);
-  q.clyu = CF(C_LYU);
 #undef CF
 }
 __device__ __forceinline__ void load_coefs(CoefB & q, const Coefs & cf, int i) {
   const double * __restrict__ b = cf.tab + i;
 #define CF(T) LD(b + (T) * CSTRIDE)
   q.a1 = CF(P_UA1); q.a2 = CF(P_UA2); q.b = CF(P_UB); q.c = CF(P_UC); q.h = CF(P_UH);
-  q.lxl = CF(C_LXL); q.lxc = CF(C_LXC); q.lxu = CF(C_LXU); q.lyl = CF(C_LYL); q.lyc = CF(C_LYC); q.lyu = CF(C_LYU);
+  q.lxl = CF(C_LXL); q.lxu = CF(C_LXU); q.ly = CF(C_LYL);
   q.p1 = CF(P_P1); q.p2 = CF(P_P2); q.qm = CF(P_QM); q.q0 = CF(P_Q0); q.qp = CF(P_QP);
   q.yk = CF(P_YK); q.yz = CF(P_YZ); q.py = CF(C_INVHYXC);
   q.zx0 = CF(P_ZX0); q.zx1 = CF(P_ZX1); q.zy = CF(P_ZY);
 #undef CF
 }
 
-// values of plane k-1 a cell needs, carried from the previous plane
-struct PrevA { double ux0, t0; };
-struct PrevB { double ux0, ux1, uy0, uyjp, uz0, p0; };
-
-// A cell's view of two plane slots (k and k+1): base pointers already moved to
-// the cell's radial index and, for rows of odd parity, to the widened copy's
-// offset. Field rows hold the storage type T (ux at element i - 1 in the
+// A cell's view of three plane slots (k-1, k and k+1): base pointers already
+// moved to the cell's radial index and, for rows of odd parity, to the widened
+// copy's offset. Field rows hold the storage type T (ux at element i - 1 in the
 // reference layout, at element i in the FP32 layout); p rows are double.
 template <class T>
 struct SlotView {
@@ -148,8 +148,14 @@ struct SlotView {
   const T * nbo;
   const T * nf;        // plane k+1, ux
   const T * nfo;
+  const T * mb;        // plane k-1, centre fields
+  const T * mbo;
+  const T * mf;        // plane k-1, ux
+  const T * mfo;
   const double * pb;   // plane k, p
   const double * pbo;  // plane k, p, odd rows
+  const double * mp;   // plane k-1, p
+  const double * mpo;
 };
 
 // Slot rows: field f, row r (j - 1 + r for the CTA's first line j) starts at
@@ -167,6 +173,11 @@ struct SlotView {
 #define NUY(DI) (ODD_(0) ? V.nbo : V.nb)[ROW_(SF_UY, 0) + (DI)]
 #define NUZ(DI, DJ) (ODD_(DJ) ? V.nbo : V.nb)[ROW_(SF_UZ, DJ) + (DI)]
 #define NTT(DI) (ODD_(0) ? V.nbo : V.nb)[ROW_(SF_T, 0) + (DI)]
+#define MUX(DI) (ODD_(0) ? V.mfo : V.mf)[ROW_(SF_UX, 0) + (DI)]
+#define MUY(DJ) (ODD_(DJ) ? V.mbo : V.mb)[ROW_(SF_UY, DJ)]
+#define MUZ() (ODD_(0) ? V.mbo : V.mb)[ROW_(SF_UZ, 0)]
+#define MTT() (ODD_(0) ? V.mbo : V.mb)[ROW_(SF_T, 0)]
+#define MPP() (ODD_(0) ? V.mpo : V.mp)[(JL + 1) * RL]
 // diffusion in direction D goes to the implicit part when D is implicit
 #define ROUTE(D, V_) do { if (D) gi += (V_); else e += (V_); } while (0)
 
@@ -175,10 +186,9 @@ struct SlotView {
 // dl[0] (ux, 0 at i = 1 where ux has no unknown) and dl[1] (t), current
 // values u0[0] (ux) and u0[1] (t).
 template <int JT, int RL, int JL, int IMPL, class T>
-__device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, PrevA & pv, const Bc & bc,
-                                       const Coefs & cf, double nu, double kappa, int i, size_t qf, size_t qc,
-                                       const SrcSetT<T> & ss, double ca, double cb, double cg, double old_x,
-                                       double old_t, double dl[2], double u0[2]) {
+__device__ __forceinline__ void cell_a(const CoefA & q, const CoefB & qc_, const SlotView<T> & V, const Bc & bc, const Coefs & cf, double nu, double kappa, double rpr, int i,
+                                       size_t qf, size_t qc, const SrcSetT<T> & ss, double ca, double cb, double cg,
+                                       double old_x, double old_t, double dl[2], double u0[2]) {
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
   const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
   const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
@@ -189,7 +199,7 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
   if (i >= 2) {
     const double ux_m = UX(-1, 0);
     const double ux_jm = UX(0, -1), ux_jp = UX(0, 1);
-    const double ux_km = pv.ux0, ux_kp = NUX(0);
+    const double ux_km = MUX(0), ux_kp = NUX(0);
     const double uy_m0 = UY(-1, 0), uy_m1 = UY(-1, 1);
     const double uz_m0 = UZ(-1, 0), uz_m1 = NUZ(-1, 0);
     double e, gi;
@@ -207,8 +217,8 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
          q.ca2 * (ux_0 + ux_p) + q.cz1 * ((uz_01 - uz_m1) - (uz_00 - uz_m0));   // coefficients carry nu
     // pressure gradient (:377-394)
     gi = -q.px * (PP(0, 0) - PP(-1, 0));
-    ROUTE(ix, q.lxl * ux_m + q.lxc * ux_0 + q.lxu * ux_p);          // carries 2 nu
-    ROUTE(iy, q.lyl * ux_jm + q.lyc * ux_0 + q.lyu * ux_jp);          // carries nu
+    ROUTE(ix, q.lxl * (ux_m - ux_0) + q.lxu * (ux_p - ux_0));        // carries 2 nu
+    ROUTE(iy, q.ly * ((ux_jm - ux_0) + (ux_jp - ux_0)));             // carries nu
     ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUX][qf];   // closure forcing
     ss.new_[VUX][qf] = (T)e;
@@ -217,29 +227,27 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const SlotView<T> & V, P
   {
     const double t_0 = TT(0, 0);
     const double tim = TT(-1, 0), tip = TT(1, 0), tjm = TT(0, -1), tjp = TT(0, 1);
-    const double tkm = pv.t0, tkp = NTT(0);
+    const double tkm = MTT(), tkp = NTT(0);
     double e, gi = 0.;
     // advection (t.c:88-116) with face velocities ux_0, ux_p, uy_00, uy_01, uz_00, uz_01
     e = q.tx0 * ux_0 * (tim - t_0) - q.tx1 * ux_p * (tip - t_0);
     e += q.ty * uy_00 * (tjm - t_0) - q.ty * uy_01 * (tjp - t_0);
     e += q.tz * uz_00 * (tkm - t_0) - q.tz * uz_01 * (tkp - t_0);
-    ROUTE(ix, q.clxl * tim + q.clxc * t_0 + q.clxu * tip);            // carry kappa
-    ROUTE(iy, q.clyl * tjm + q.clyc * t_0 + q.clyu * tjp);
+    ROUTE(ix, rpr * (qc_.lxl * (tim - t_0) + qc_.lxu * (tip - t_0)));   // nu kappa/nu
+    ROUTE(iy, rpr * (qc_.ly * ((tjm - t_0) + (tjp - t_0))));
     ROUTE(iz, kappa * (cf.lz_l * tkm + cf.lz_c * t_0 + cf.lz_u * tkp));
     ss.new_[VT][qc] = (T)e;
     dl[1] = ca * e + cb * old_t + cg * gi;
     u0[1] = t_0;
-    pv.t0 = t_0;
   }
   u0[0] = ux_0;
-  pv.ux0 = ux_0;
 }
 
 // Group B: right-hand sides of uy (src/fluid/predict/uy.c) and uz (uz.c) at
 // centre i of cell (i, j, k); increments dl[0] (uy), dl[1] (uz), current
 // values u0[0], u0[1].
 template <int JT, int RL, int JL, int IMPL, class T>
-__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, PrevB & pv, const Bc & bc,
+__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, const Bc & bc,
                                        const Coefs & cf, double nu, int i, size_t qc, const SrcSetT<T> & ss,
                                        double ca, double cb, double cg, double old_y, double old_z, double dl[2],
                                        double u0[2]) {
@@ -252,7 +260,7 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
   const double p_0 = PP(0, 0);
   {  // uy
     const double uy_im = UY(-1, 0), uy_ip = UY(1, 0), uy_jm = UY(0, -1);
-    const double uy_km = pv.uy0, uy_kp = NUY(0);
+    const double uy_km = MUY(0), uy_kp = NUY(0);
     const double ux_0m = UX(0, -1), ux_1m = UX(1, -1);
     const double uz_jm = UZ(0, -1), uz_jmkp = NUZ(0, -1);
     double e, gi;
@@ -267,8 +275,8 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     e += q.p1 * (ux_0 - ux_0m) + q.p2 * (ux_1 - ux_1m) + q.qm * uy_im + q.q0 * uy_0 + q.qp * uy_ip +
          q.yk * ((ux_0 + ux_1) - (ux_0m + ux_1m)) + q.yz * ((uz_kp - uz_jmkp) - (uz_0 - uz_jm));   // carry nu
     gi = -q.py * (p_0 - PP(0, -1));
-    ROUTE(ix, q.lxl * uy_im + q.lxc * uy_0 + q.lxu * uy_ip);          // carry nu
-    ROUTE(iy, 2. * (q.lyl * uy_jm + q.lyc * uy_0 + q.lyu * uy_jp));
+    ROUTE(ix, q.lxl * (uy_im - uy_0) + q.lxu * (uy_ip - uy_0));      // carry nu
+    ROUTE(iy, 2. * (q.ly * ((uy_jm - uy_0) + (uy_jp - uy_0))));
     ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUY][qc];
     ss.new_[VUY][qc] = (T)e;
@@ -276,9 +284,9 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
   }
   {  // uz
     const double uz_im = UZ(-1, 0), uz_ip = UZ(1, 0), uz_jm = UZ(0, -1), uz_jp = UZ(0, 1);
-    const double uz_km = pv.uz0;
-    const double uy_km = pv.uy0, uy_jpkm = pv.uyjp;
-    const double ux_0k = pv.ux0, ux_1k = pv.ux1;
+    const double uz_km = MUZ();
+    const double uy_km = MUY(0), uy_jpkm = MUY(1);
+    const double ux_0k = MUX(0), ux_1k = MUX(1);
     double e, gi;
     // advection (uz.c:88-180), as differences from uz_0
     e = q.a1 * (ux_0k + ux_0) * (uz_im - uz_0) - q.a2 * (ux_1k + ux_1) * (uz_ip - uz_0);
@@ -286,9 +294,9 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
     e += q.c * (uz_km + uz_0) * (uz_km - uz_0) - q.c * (uz_0 + uz_kp) * (uz_kp - uz_0);
     // diffusion_x1 (lzx at faces i, i+1), diffusion_y1 (lzy at j, j+1)
     e += q.zx1 * (ux_1 - ux_1k) - q.zx0 * (ux_0 - ux_0k) + q.zy * ((uy_jp - uy_jpkm) - (uy_0 - uy_km));   // carry nu
-    gi = -cf.inv_hz * (p_0 - pv.p0);
-    ROUTE(ix, q.lxl * uz_im + q.lxc * uz_0 + q.lxu * uz_ip);
-    ROUTE(iy, q.lyl * uz_jm + q.lyc * uz_0 + q.lyu * uz_jp);
+    gi = -cf.inv_hz * (p_0 - MPP());
+    ROUTE(ix, q.lxl * (uz_im - uz_0) + q.lxu * (uz_ip - uz_0));
+    ROUTE(iy, q.ly * ((uz_jm - uz_0) + (uz_jp - uz_0)));
     ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
     if constexpr (IMPL == -2) e += ss.frc[VUZ][qc];
     ss.new_[VUZ][qc] = (T)e;
@@ -296,12 +304,6 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
   }
   u0[0] = uy_0;
   u0[1] = uz_0;
-  pv.ux0 = ux_0;
-  pv.ux1 = ux_1;
-  pv.uy0 = uy_0;
-  pv.uyjp = uy_jp;
-  pv.uz0 = uz_0;
-  pv.p0 = p_0;
 }
 #undef ROW_
 #undef ODD_
@@ -314,6 +316,11 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, P
 #undef NUY
 #undef NUZ
 #undef NTT
+#undef MPP
+#undef MTT
+#undef MUZ
+#undef MUY
+#undef MUX
 #undef ROUTE
 
 template <int E>
@@ -332,25 +339,34 @@ __device__ __forceinline__ void load_chunk(double (&r)[E], const double * __rest
 }
 
 // Radial Thomas solve of one line by one warp (src/tdm.c:24-48): lane t owns
-// elements tE .. tE+E-1, composes their affine maps, a 5-level shuffle scan
-// supplies the value entering its chunk, then the recurrences run in the
-// reference's form q = w (r - l q_prev) and x = q - v x_next. The factor rows
-// hold w[0] = 1 / c[0] and l[0] = 0, and zeros from n on; the staging line is
+// elements tE .. tE+E-1. The forward sweep q_m = w_m (r_m - l_m q_{m-1}) is the
+// affine map q_{m-1} -> fa_m q_{m-1} + fb_m with fa = -w l, fb = w r; each lane
+// composes its maps, a 5-level shuffle scan supplies the value entering its
+// chunk, and the chunk's q follow from (fa, fb). The back substitution
+// x_m = q_m - v_m x_{m+1} runs the same way from the other end. The factor rows
+// have w[0] = 1 / c[0] and l[0] = 0, and zeros from n on; the staging line is
 // zero from n on as well, so elements past the end map to zero without tests.
+// Only (fa, fb), then (q, v), stay live across a scan.
 template <int E>
-__device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int rkstep, int var, int lane) {
-  const size_t fo = (size_t)(rkstep * 4 + var) * xf.stride;
-  double q[E], ll[E], ww[E];
-  load_chunk<E>(ll, xf.lo + fo, lane);
-  load_chunk<E>(ww, xf.w + fo, lane);
+__device__ __forceinline__ void solve_line(double * sb, const double * __restrict__ lrow,
+                                           const double * __restrict__ wrow, const double * __restrict__ vrow,
+                                           int lane) {
+  double fa[E], fb[E];
+  {
+    double ll[E], ww[E];
+    load_chunk<E>(ll, lrow, lane);
+    load_chunk<E>(ww, wrow, lane);
 #pragma unroll
-  for (int m = 0; m < E; m++) q[m] = sb[spad<E>(lane * E + m)];
+    for (int m = 0; m < E; m++) {
+      fa[m] = -ww[m] * ll[m];
+      fb[m] = ww[m] * sb[spad<E>(lane * E + m)];
+    }
+  }
   Aff acc{1., 0.};
 #pragma unroll
   for (int m = 0; m < E; m++) {
-    const double fa = -ww[m] * ll[m], fb = ww[m] * q[m];
-    acc.b = fa * acc.b + fb;
-    acc.a = fa * acc.a;
+    acc.b = fa[m] * acc.b + fb[m];
+    acc.a = fa[m] * acc.a;
   }
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
@@ -360,14 +376,14 @@ __device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int
   }
   double qin = __shfl_up_sync(0xffffffffu, acc.b, 1);
   if (lane == 0) qin = 0.;
+  double * q = fb;
 #pragma unroll
   for (int m = 0; m < E; m++) {
-    const double r = ww[m] * (q[m] - ll[m] * qin);
-    q[m] = r;
-    qin = r;
+    q[m] = fa[m] * qin + fb[m];
+    qin = q[m];
   }
   double vv[E];
-  load_chunk<E>(vv, xf.v + fo, lane);
+  load_chunk<E>(vv, vrow, lane);
   Aff bac{1., 0.};
 #pragma unroll
   for (int m = E - 1; m >= 0; m--) {
@@ -390,27 +406,51 @@ __device__ __forceinline__ void solve_line(double * sb, const XFactors & xf, int
   }
 }
 
-// Shared-memory layout in bytes, shared by the kernel and its launcher. Row
-// buffers are sized for the widest radial line of the warp count (nx <= 32 NW),
-// so every stencil offset is a compile-time constant. A slot holds the field
-// rows (storage type T), the p rows (double) and the previous substep's source
-// terms (T).
+// Thread roles. The CTA is NRW "field" warps (one thread per radial index,
+// whole warpgroups) followed by one warpgroup of four "solve" warps (warp v
+// solves variable v of the CTA's lines). Per plane k the field warps form the
+// right-hand sides and increments of every cell and hand them to the solve
+// warps through a double-buffered staging area (mbarrier full[k & 1]); while
+// the solve warps run the radial systems of plane k, the field warps go on to
+// plane k + 1 and then take plane k's solutions back (mbarrier done[k & 1]) to
+// add them to the values they kept and store the new fields. So no block-wide
+// barrier separates the right-hand sides from the solves.
+//
+// Shared memory, in bytes, shared by the kernel and its launcher. Row buffers
+// are sized for the widest radial line of the warp count (nx <= 32 NW), so
+// every stencil offset is a compile-time constant. A ring slot holds the field
+// rows (storage type T) and the p rows (double) of one plane; the previous
+// substep's source terms of the CTA's lines arrive one plane ahead by bulk
+// copies into a two-plane buffer of their own.
 template <int NW, int JT, class T>
 struct MarchLayout {
-  static_assert(JT == 2 || JT == 4, "line groups start at odd j, so rows of even index have even j");
+  static_assert(JT == 2, "line pairs start at odd j, so rows of even index have even j");
   static constexpr int E = NW;
+  static constexpr int NSLOT = 4;                             // planes k .. k+3 in the ring
   static constexpr int RL = 32 * NW + 4;                      // values per row: >= nx + 4, multiple of 4
+  static constexpr int NRW = NW < 4 ? 4 : NW;                 // field warps
+  static constexpr int NRT = 32 * NRW;
+  static constexpr int THREADS = NRT + 128;                   // + the solve warpgroup
   static constexpr int NFROW = 4 * (JT + 2);                  // ux, uy, uz, t: JT + 2 rows each
   static constexpr size_t POFF = (size_t)NFROW * RL * sizeof(T);          // p: JT + 1 rows of double
-  static constexpr size_t OLDOFF = POFF + (size_t)(JT + 1) * RL * sizeof(double);
-  static constexpr size_t SLOT = OLDOFF + (size_t)4 * JT * RL * sizeof(T);  // JT lines per variable
+  static constexpr size_t SLOT = POFF + (size_t)(JT + 1) * RL * sizeof(double);
   static constexpr int SL = 32 * E + (E > 1 ? 32 : 0);        // staging line (padded for the solves)
   static constexpr size_t STAGE = NSLOT * SLOT;               // [2][JT][4][SL] doubles after the ring
-  static constexpr size_t BAR = STAGE + sizeof(double) * 2 * JT * 4 * SL;   // NSLOT mbarriers
-  static constexpr size_t BYTES = BAR + NSLOT * sizeof(unsigned long long);
+  static constexpr int OL = 32 * NW;                          // old source terms per line and variable
+  static constexpr size_t OLDS = STAGE + sizeof(double) * 2 * JT * 4 * SL;   // [2][4][JT OL] T
+  static constexpr size_t BAR = OLDS + sizeof(T) * 2 * 4 * JT * OL;
+  // mbarriers: NSLOT ring slots, full[2], done[2], olds[2]; then the abort
+  // flag, the last plane issued and a release counter per slot
+  static constexpr int NBAR = NSLOT + 6;
+  static constexpr size_t BYTES = BAR + NBAR * sizeof(unsigned long long) + 8 + 4 * NSLOT;
+  // registers per thread at launch, and after the split (field, solve): the
+  // warpgroups' shares add up to the launch total (THREADS x REGS)
+  static constexpr int REGS = NRW == 8 ? 168 : 0;
+  static constexpr int REGS_FIELD = 200, REGS_SOLVE = 104;
+  static_assert(REGS == 0 || NRT * REGS_FIELD + 128 * REGS_SOLVE <= THREADS * REGS, "register split");
 };
 
-// Everything a group's march needs besides its coefficients.
+// Everything the roles need besides their coefficients.
 template <class T>
 struct MarchArgs {
   Geo g;
@@ -425,22 +465,36 @@ struct MarchArgs {
   unsigned * status;
 };
 
-// The plane loop of one thread group: G = 0 computes ux and t, G = 1 uy and
-// uz, G = 2 all four (one group per line). With two groups both pass the same
-// barriers in the same order.
-template <int NW, int JT, int IMPL, int G, class T>
-__device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring, double * stage,
-                                            unsigned long long * bar, int j0, int k0, int k1, double dt) {
+__device__ __forceinline__ void mbar_arrive(unsigned long long * bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// barrier among the field warps only (id 1; id 0 is __syncthreads)
+template <int N>
+__device__ __forceinline__ void field_barrier() {
+  asm volatile("bar.sync 1, %0;" ::"n"(N) : "memory");
+}
+
+// the slot of plane kp and the parity of its fill (planes k0 - 1 .. k1 pass
+// through the NSLOT slots in turn)
+__device__ __forceinline__ int slot_of(int kp, int k0, int nslot) { return (kp - k0 + 1) % nslot; }
+__device__ __forceinline__ unsigned fill_parity(int kp, int k0, int nslot) { return ((kp - k0 + 1) / nslot) & 1u; }
+
+// The field warps: one thread per radial index i of the CTA's JT lines.
+template <int NW, int JT, int IMPL, class T>
+__device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring, double * stage, T * olds,
+                                             unsigned long long * bar, volatile int * abort_flag,
+                                             int * release_cnt, volatile int * issued_p, int j0, int k0, int k1,
+                                             double dt) {
   using L = MarchLayout<NW, JT, T>;
-  constexpr int E = L::E, RL = L::RL, SL = L::SL, NT = 32 * NW;
-  constexpr bool GA = G != 1, GB = G != 0;   // group computes ux and t / uy and uz
-  constexpr int NGRP = G == 2 ? 1 : 2;
+  constexpr int E = L::E, RL = L::RL, SL = L::SL, NS = L::NSLOT, OL = L::OL;
   const Geo & g = A.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x;
-  const int lane = tx & 31, wid = tx >> 5;
-  const int i = tx - (G == 1 ? NT : 0) + 1;
+  const int i = tx + 1;
   const bool act = i <= nx;
+  unsigned long long * full = bar + NS;
+  unsigned long long * done = bar + NS + 2;
+  unsigned long long * obar = bar + NS + 4;
   // element offsets of odd rows in their widened copies: ux / centre fields
   // (none in the FP32 layout, whose rows start on 16-byte boundaries) and p
   constexpr bool D64 = sizeof(T) == 8;
@@ -449,19 +503,12 @@ __device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring,
   const size_t sjc = (size_t)ny + 2;
   auto frow = [&](char * slot, int f, int r) { return reinterpret_cast<T *>(slot) + (size_t)(f * (JT + 2) + r) * RL; };
   auto prow = [&](char * slot, int r) { return reinterpret_cast<double *>(slot + L::POFF) + (size_t)r * RL; };
-  auto orow = [&](char * slot, int v) { return reinterpret_cast<T *>(slot + L::OLDOFF) + (size_t)v * JT * RL; };
 
-  // Copies of plane kp into slot sl: the field rows and, for planes that are
-  // computed in a substep with beta != 0, the source terms of the previous
-  // substep at the JT lines (consecutive in the packed layout, 16-byte
-  // aligned as JT is even).
-  const bool use_old = A.rkstep != 0;
+  // Copies of plane kp into slot sl: every row of the five arrays (4 = p, in
+  // double), widened to 16-byte bounds; one thread counts the bytes, expects
+  // them on the slot's mbarrier and issues the copies.
   auto issue = [&](int kp, int sl) {
     char * base = ring + (size_t)sl * L::SLOT;
-    const bool olds = use_old && kp >= k0 && kp < k1;
-    // every row of the five arrays (4 = p, in double), widened to 16-byte
-    // bounds: counts the bytes or issues the copies. With 8-byte storage the
-    // p rows continue the field rows' layout.
     const char * src[5] = {reinterpret_cast<const char *>(A.in.ux), reinterpret_cast<const char *>(A.in.uy),
                            reinterpret_cast<const char *>(A.in.uz), reinterpret_cast<const char *>(A.in.t),
                            reinterpret_cast<const char *>(A.in.p)};
@@ -482,100 +529,137 @@ __device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring,
     };
     unsigned total = 0;
     all(false, total);
-    if (olds) total += (unsigned)(JT * (D64 ? 4 * nx - 1 : 4 * spitch32(nx)) * sizeof(T));
     mbar_expect_tx(&bar[sl], total);
-    if (olds) {
-      for (int v = 0; v < 4; v++) {
-        const int ni = (v == VUX) ? nx - 1 : nx;
-        const int li = D64 ? ni : spitch32(nx);   // packed line length (sline)
-        bulk_g2s(orow(base, v), A.ss.old_[v] + pidx(li, ny, 0, j0, kp), (unsigned)(JT * li * sizeof(T)), &bar[sl]);
-      }
-    }
     all(true, total);
   };
-  if (tx == 0) {
-    issue(k0 - 1, 0);
-    issue(k0, 1);
-    issue(k0 + 1, 2);
-  }
-  unsigned par[NSLOT] = {0u, 0u, 0u};
-  bool late = false;
-  auto wait_slot = [&](int sl) {
-    if (!mbar_wait(&bar[sl], par[sl])) late = true;
-    par[sl] ^= 1u;
+  // bounded wait; after any wait of the CTA has given up, no thread waits any
+  // more (the CTA runs to its end without storing anything)
+  auto wait = [&](unsigned long long * b, unsigned parity) {
+    if (*abort_flag) return false;
+    if (mbar_wait(b, parity)) return true;
+    *abort_flag = 1;
+    return false;
   };
+  if (tx == 0) {
+    for (int s = 0; s < NS && k0 - 1 + s <= k1; s++) issue(k0 - 1 + s, s);
+    *issued_p = k0 - 2 + (k1 - k0 + 2 < NS ? k1 - k0 + 2 : NS);
+  }
+
+  // the previous substep's source terms of the CTA's lines, one plane ahead:
+  // the JT lines of a variable are consecutive in the packed layout and start
+  // on a 16-byte boundary (even line index), so one bulk copy per variable
+  const bool use_old = A.rkstep != 0;
+  const int lf = D64 ? nx - 1 : spitch32(nx), lc = D64 ? nx : spitch32(nx);   // source-term lines (sline)
+  auto fetch_olds = [&](int kp, int buf) {
+    const unsigned total = (unsigned)((size_t)JT * (lf + 3 * lc) * sizeof(T));
+    mbar_expect_tx(&obar[buf], total);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      const int li = v == VUX ? lf : lc;
+      bulk_g2s(olds + (size_t)(buf * 4 + v) * JT * OL, A.ss.old_[v] + pidx(li, ny, 0, j0, kp),
+               (unsigned)((size_t)JT * li * sizeof(T)), &obar[buf]);
+    }
+  };
+  if (tx == 0 && use_old) {
+    fetch_olds(k0, 0);
+    if (k0 + 1 < k1) fetch_olds(k0 + 1, 1);
+  }
 
   CoefA qa;
   CoefB qb;
-  if constexpr (GA) load_coefs(qa, A.cf, act ? i : 1);
-  if constexpr (GB) load_coefs(qb, A.cf, act ? i : 1);
+  load_coefs(qa, A.cf, act ? i : 1);
+  load_coefs(qb, A.cf, act ? i : 1);
   // the diffusivities folded into the per-thread coefficients once, so the
   // cell updates multiply by them no more (the z Laplacian, a shared scalar
   // set, keeps its factor)
-  if constexpr (GA) {
-    const double nu = A.nu, n2 = 2. * A.nu, ka = A.kappa;
-    qa.lxl *= n2; qa.lxc *= n2; qa.lxu *= n2;
-    qa.lyl *= nu; qa.lyc *= nu; qa.lyu *= nu;
+  {
+    const double nu = A.nu, n2 = 2. * A.nu;
+    qa.lxl *= n2; qa.lxu *= n2; qa.ly *= nu;
     qa.cy1 *= nu; qa.cy2 *= nu; qa.ca1 *= nu; qa.ca2 *= nu; qa.cz1 *= nu;
-    qa.clxl *= ka; qa.clxc *= ka; qa.clxu *= ka; qa.clyl *= ka; qa.clyc *= ka; qa.clyu *= ka;
-  }
-  if constexpr (GB) {
-    const double nu = A.nu;
-    qb.lxl *= nu; qb.lxc *= nu; qb.lxu *= nu; qb.lyl *= nu; qb.lyc *= nu; qb.lyu *= nu;
+    qb.lxl *= nu; qb.lxu *= nu; qb.ly *= nu;
     qb.p1 *= nu; qb.p2 *= nu; qb.qm *= nu; qb.q0 *= nu; qb.qp *= nu; qb.yk *= nu; qb.yz *= nu;
     qb.zx0 *= nu; qb.zx1 *= nu; qb.zy *= nu;
   }
+  const double rpr = A.kappa / A.nu;   // the scalar's Laplacians use the centred tables with kappa
   const int rk = A.rkstep;
   const double ca = rk_alpha(rk) * dt, cb = rk_beta(rk) * dt, cg = rk_gamma(rk) * dt;
 
-  // plane k0 - 1: the carried values
-  wait_slot(0);
-  wait_slot(1);
-  PrevA pa[JT];
-  PrevB pb[JT];
-  if (act) {
+  // planes k0 - 1 and k0
+  wait(&bar[0], 0);
+  wait(&bar[1], 0);
+
+  // u += delta into the other buffer, walls (boundary/*.c) and images
+  // (halo.c); or the increments themselves (planar y / z solves follow)
+  auto store = [&](int k, const double (&dl)[JT][4], const double (&u0)[JT][4]) {
+    if (!act || *abort_flag) return;
 #pragma unroll
     for (int jl = 0; jl < JT; jl++) {
-      const int r1 = jl + 1, r2 = jl + 2;   // rows j and j + 1
-      const int o1c = (r1 & 1) ? oc : 0, o1f = (r1 & 1) ? of : 0, o2c = (r2 & 1) ? oc : 0;
-      const int o1p = (r1 & 1) ? op : 0;
-      const T * ux1 = frow(ring, SF_UX, r1) + o1f + i - FSH;
-      if constexpr (GA) {
-        pa[jl].ux0 = ux1[0];
-        pa[jl].t0 = frow(ring, SF_T, r1)[o1c + i];
+      const int j = j0 + jl;
+      if (A.mode == PREDICT_DELTA) {
+        const size_t qc = pidx(nx, ny, i - 1, j, k);
+        if (i >= 2) A.ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] = dl[jl][VUX];
+        A.ds.d[VT][qc] = dl[jl][VT];
+        A.ds.d[VUY][qc] = dl[jl][VUY];
+        A.ds.d[VUZ][qc] = dl[jl][VUZ];
+        continue;
       }
-      if constexpr (GB) {
-        pb[jl].ux0 = ux1[0];
-        pb[jl].ux1 = ux1[1];
-        pb[jl].uy0 = frow(ring, SF_UY, r1)[o1c + i];
-        pb[jl].uyjp = frow(ring, SF_UY, r2)[o2c + i];
-        pb[jl].uz0 = frow(ring, SF_UZ, r1)[o1c + i];
-        pb[jl].p0 = prow(ring, r1)[o1p + i];
-      }
+      const double vx = (i < 2) ? 0. : u0[jl][VUX] + dl[jl][VUX];
+      const double vt = u0[jl][VT] + dl[jl][VT];
+      const double vy = u0[jl][VUY] + dl[jl][VUY];
+      const double vz = u0[jl][VUZ] + dl[jl][VUZ];
+      auto put = [&](int jj, int kk) {
+        A.out.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx;
+        A.out.t[sidx_c<T>(g, i, jj, kk)] = (T)vt;
+        A.out.uy[sidx_c<T>(g, i, jj, kk)] = (T)vy;
+        A.out.uz[sidx_c<T>(g, i, jj, kk)] = (T)vz;
+        if (i == 1) {
+          A.out.t[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.t_xm;
+          A.out.uy[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.uy_xm;
+          A.out.uz[sidx_c<T>(g, 0, jj, kk)] = (T)0.;
+        }
+        if (i == nx) {
+          A.out.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.;
+          A.out.t[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.t_xp;
+          A.out.uy[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.uy_xp;
+          A.out.uz[sidx_c<T>(g, nx + 1, jj, kk)] = (T)0.;
+        }
+      };
+      put(j, k);
+      for_images(j, k, ny, nz, put);
     }
-  }
-  __syncthreads();
+  };
+  // staging positions: ux unknowns are faces 2..nx (element i - 2), the
+  // centred ones cells 1..nx (element i - 1)
+  auto stage_pos = [&](int v) { return v == VUX ? spad<E>(i - 2) : spad<E>(i - 1); };
+  // plane k's solutions from the solve warps, added to the values kept
+  auto finish_plane = [&](int k, int step, const double (&u0)[JT][4]) {
+    const int b = step & 1;
+    wait(&done[b], (unsigned)(step >> 1) & 1u);
+    double x[JT][4];
+    const double * sdb = stage + (size_t)b * JT * 4 * SL;
+#pragma unroll
+    for (int jl = 0; jl < JT; jl++)
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        x[jl][v] = (act && (v != VUX || i >= 2)) ? sdb[(size_t)(jl * 4 + v) * SL + stage_pos(v)] : 0.;
+    store(k, x, u0);
+  };
 
   const bool solve_x = IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0;
+  double up[JT][4];   // values of the previous plane's cells, until its solutions arrive
   for (int k = k0; k < k1; k++) {
     const int step = k - k0;
-    const int cur = (step + 1) % NSLOT, nxt = (step + 2) % NSLOT, fre = step % NSLOT;
-    // plane k + 2 into the slot of plane k - 1, which every thread finished
-    // reading before the previous plane's first barrier
-    if (tx == 0 && k + 2 <= k1) {
-      fence_async_smem();
-      issue(k + 2, fre);
-    }
-    wait_slot(nxt);
-    double * sdb = stage + (size_t)(step & 1) * JT * 4 * SL;
+    wait(&bar[slot_of(k + 1, k0, NS)], fill_parity(k + 1, k0, NS));
+    if (use_old) wait(&obar[step & 1], (unsigned)(step >> 1) & 1u);
     double dl[JT][4], u0[JT][4];   // indexed by Var
 #pragma unroll
     for (int jl = 0; jl < JT; jl++)
 #pragma unroll
       for (int v = 0; v < 4; v++) dl[jl][v] = u0[jl][v] = 0.;
     if (act) {
-      char * cs = ring + (size_t)cur * L::SLOT;
-      char * ns = ring + (size_t)nxt * L::SLOT;
+      char * ms = ring + (size_t)slot_of(k - 1, k0, NS) * L::SLOT;
+      char * cs = ring + (size_t)slot_of(k, k0, NS) * L::SLOT;
+      char * ns = ring + (size_t)slot_of(k + 1, k0, NS) * L::SLOT;
       SlotView<T> V;
       V.cb = reinterpret_cast<const T *>(cs) + i;
       V.cbo = V.cb + oc;
@@ -585,168 +669,168 @@ __device__ __forceinline__ void march_group(const MarchArgs<T> & A, char * ring,
       V.nbo = V.nb + oc;
       V.nf = V.nb - FSH;
       V.nfo = V.nf + of;
+      V.mb = reinterpret_cast<const T *>(ms) + i;
+      V.mbo = V.mb + oc;
+      V.mf = V.mb - FSH;
+      V.mfo = V.mf + of;
       if constexpr (D64) {   // p rows follow the field rows: same base registers, constant offsets
         V.pb = reinterpret_cast<const double *>(V.cb) + L::NFROW * RL;
         V.pbo = reinterpret_cast<const double *>(V.cbo) + L::NFROW * RL;
+        V.mp = reinterpret_cast<const double *>(V.mb) + L::NFROW * RL;
+        V.mpo = reinterpret_cast<const double *>(V.mbo) + L::NFROW * RL;
       } else {
         V.pb = prow(cs, 0) + i;
         V.pbo = V.pb + op;
+        V.mp = prow(ms, 0) + i;
+        V.mpo = V.mp + op;
       }
-      const int lf = D64 ? nx - 1 : spitch32(nx), lc = D64 ? nx : spitch32(nx);   // source-term lines (sline)
       const size_t qf = pidx(lf, ny, i - 2, j0, k), qc = pidx(lc, ny, i - 1, j0, k);
-      const T * ob = orow(cs, 0);   // old source terms of plane k
+      const T * ob = olds + (size_t)(step & 1) * 4 * JT * OL;   // this plane's old terms
       auto cells = [&](auto jlc) {
         constexpr int JL = decltype(jlc)::value;
         double d2[2], w2[2];
-        auto old = [&](int v, int e) {
-          return use_old ? (double)ob[v * JT * RL + JL * (v == VUX ? lf : lc) + e] : 0.;
+        auto old = [&](int v) {
+          return use_old ? (double)ob[(size_t)v * JT * OL + JL * (v == VUX ? lf : lc) + (v == VUX ? i - 2 : i - 1)] : 0.;
         };
-        if constexpr (GA) {
-          cell_a<JT, RL, JL, IMPL>(qa, V, pa[JL], A.bc, A.cf, A.nu, A.kappa, i, qf + (size_t)JL * lf,
-                                   qc + (size_t)JL * lc, A.ss, ca, cb, cg, i >= 2 ? old(VUX, i - 2) : 0.,
-                                   old(VT, i - 1), d2, w2);
-          dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
-        }
-        if constexpr (GB) {
-          cell_b<JT, RL, JL, IMPL>(qb, V, pb[JL], A.bc, A.cf, A.nu, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
-                                   old(VUY, i - 1), old(VUZ, i - 1), d2, w2);
-          dl[JL][VUY] = d2[0]; dl[JL][VUZ] = d2[1]; u0[JL][VUY] = w2[0]; u0[JL][VUZ] = w2[1];
-        }
+        cell_a<JT, RL, JL, IMPL>(qa, qb, V, A.bc, A.cf, A.nu, A.kappa, rpr, i, qf + (size_t)JL * lf,
+                                 qc + (size_t)JL * lc, A.ss, ca, cb, cg, i >= 2 ? old(VUX) : 0., old(VT), d2, w2);
+        dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
+        cell_b<JT, RL, JL, IMPL>(qb, V, A.bc, A.cf, A.nu, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
+                                 old(VUY), old(VUZ), d2, w2);
+        dl[JL][VUY] = d2[0]; dl[JL][VUZ] = d2[1]; u0[JL][VUY] = w2[0]; u0[JL][VUZ] = w2[1];
       };
       cells(std::integral_constant<int, 0>());
       cells(std::integral_constant<int, 1>());
-      if constexpr (JT == 4) {
-        cells(std::integral_constant<int, 2>());
-        cells(std::integral_constant<int, 3>());
+    }
+    // This warp is done with the slot of plane k - 1 and with the old terms'
+    // buffer of plane k; the last field warp to get here refills them with
+    // planes k + 3 and k + 2 (no warp waits for the others).
+    __syncwarp();
+    if ((tx & 31) == 0) {
+      __threadfence_block();
+      int * cnt = release_cnt + slot_of(k - 1, k0, NS);
+      if (atomicAdd(cnt, 1) == L::NRW - 1) {
+        *cnt = 0;
+        __threadfence_block();
+        if (!*abort_flag) {
+          fence_async_smem();
+          if (k + 3 <= k1) {
+            issue(k + 3, slot_of(k + 3, k0, NS));
+            *issued_p = k + 3;
+          }
+          if (use_old && k + 2 < k1) fetch_olds(k + 2, step & 1);
+        }
       }
     }
-    // staging positions: ux unknowns are faces 2..nx (element i - 2), the
-    // centred ones cells 1..nx (element i - 1)
     if (solve_x) {
+      const int b = step & 1;
+      double * sdb = stage + (size_t)b * JT * 4 * SL;
       if (act) {
 #pragma unroll
-        for (int jl = 0; jl < JT; jl++) {
-          double * s = sdb + (size_t)jl * 4 * SL;
-          if constexpr (GA) {
-            if (i >= 2) s[VUX * SL + spad<E>(i - 2)] = dl[jl][VUX];
-            s[VT * SL + spad<E>(i - 1)] = dl[jl][VT];
-          }
-          if constexpr (GB) {
-            s[VUY * SL + spad<E>(i - 1)] = dl[jl][VUY];
-            s[VUZ * SL + spad<E>(i - 1)] = dl[jl][VUZ];
-          }
-        }
-      }
-      __syncthreads();
-      for (int s = wid; s < 4 * JT; s += NGRP * NW) solve_line<E>(sdb + (size_t)s * SL, A.xf, rk, s & 3, lane);
-      __syncthreads();
-      if (act) {
+        for (int jl = 0; jl < JT; jl++)
 #pragma unroll
-        for (int jl = 0; jl < JT; jl++) {
-          const double * s = sdb + (size_t)jl * 4 * SL;
-          if constexpr (GA) {
-            dl[jl][VUX] = (i >= 2) ? s[VUX * SL + spad<E>(i - 2)] : 0.;
-            dl[jl][VT] = s[VT * SL + spad<E>(i - 1)];
-          }
-          if constexpr (GB) {
-            dl[jl][VUY] = s[VUY * SL + spad<E>(i - 1)];
-            dl[jl][VUZ] = s[VUZ * SL + spad<E>(i - 1)];
-          }
-        }
+          for (int v = 0; v < 4; v++)
+            if (v != VUX || i >= 2) sdb[(size_t)(jl * 4 + v) * SL + stage_pos(v)] = dl[jl][v];
       }
+      mbar_arrive(&full[b]);
+      if (step > 0) finish_plane(k - 1, step - 1, up);
+#pragma unroll
+      for (int jl = 0; jl < JT; jl++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) up[jl][v] = u0[jl][v];
     } else {
-      // no radial solve: this barrier alone orders the plane's slot reads
-      // before the copy into that slot two planes on
-      __syncthreads();
-    }
-    if (!act) continue;
-#pragma unroll
-    for (int jl = 0; jl < JT; jl++) {
-      const int j = j0 + jl;
-      if (A.mode == PREDICT_DELTA) {
-        const size_t qc = pidx(nx, ny, i - 1, j, k);
-        if constexpr (GA) {
-          if (i >= 2) A.ds.d[VUX][pidx(nx - 1, ny, i - 2, j, k)] = dl[jl][VUX];
-          A.ds.d[VT][qc] = dl[jl][VT];
-        }
-        if constexpr (GB) {
-          A.ds.d[VUY][qc] = dl[jl][VUY];
-          A.ds.d[VUZ][qc] = dl[jl][VUZ];
-        }
-        continue;
-      }
-      // u += delta into the other buffer, walls (boundary/*.c) and images (halo.c)
-      const double vx = (i < 2) ? 0. : u0[jl][VUX] + dl[jl][VUX];
-      const double vt = u0[jl][VT] + dl[jl][VT];
-      const double vy = u0[jl][VUY] + dl[jl][VUY];
-      const double vz = u0[jl][VUZ] + dl[jl][VUZ];
-      auto put = [&](int jj, int kk) {
-        if constexpr (GA) {
-          A.out.ux[sidx_f<T>(g, i, jj, kk)] = (T)vx;
-          A.out.t[sidx_c<T>(g, i, jj, kk)] = (T)vt;
-          if (i == 1) A.out.t[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.t_xm;
-          if (i == nx) {
-            A.out.ux[sidx_f<T>(g, nx + 1, jj, kk)] = (T)0.;
-            A.out.t[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.t_xp;
-          }
-        }
-        if constexpr (GB) {
-          A.out.uy[sidx_c<T>(g, i, jj, kk)] = (T)vy;
-          A.out.uz[sidx_c<T>(g, i, jj, kk)] = (T)vz;
-          if (i == 1) {
-            A.out.uy[sidx_c<T>(g, 0, jj, kk)] = (T)A.bc.uy_xm;
-            A.out.uz[sidx_c<T>(g, 0, jj, kk)] = (T)0.;
-          }
-          if (i == nx) {
-            A.out.uy[sidx_c<T>(g, nx + 1, jj, kk)] = (T)A.bc.uy_xp;
-            A.out.uz[sidx_c<T>(g, nx + 1, jj, kk)] = (T)0.;
-          }
-        }
-      };
-      put(j, k);
-      for_images(j, k, ny, nz, put);
+      store(k, dl, u0);
     }
   }
-  if (late) atomicOr(A.status, ST_TIMEOUT);
+  if (solve_x) finish_plane(k1 - 1, k1 - 1 - k0, up);
+  field_barrier<L::NRT>();   // every issue is done
+  if (*abort_flag && tx == 0) {
+    // copies may still be in flight into the ring and the olds buffers: wait,
+    // bounded, for the latest fill of each before the CTA exits
+    const int issued = *issued_p;
+    for (int kp = (issued - NS + 1 > k0 - 1 ? issued - NS + 1 : k0 - 1); kp <= issued; kp++)
+      mbar_wait(&bar[slot_of(kp, k0, NS)], fill_parity(kp, k0, NS));
+    if (use_old) {
+      for (int kp = k1 - 2 > k0 ? k1 - 2 : k0; kp < k1; kp++)
+        mbar_wait(&obar[(kp - k0) & 1], (unsigned)((kp - k0) >> 1) & 1u);
+    }
+  }
 }
 
-// Thread groups per line. With 2, ux and t are computed by one thread and uy
-// and uz by another, so the coefficients of each fit in 128 registers and twice
-// as many warps are resident; measured at 256 x 1024 x 512 the single group
-// (up to 255 registers, 8 warps per SM) is faster (7.9 against 9.4 ms per
-// launch, the two groups waiting on each other at the barriers).
-#ifndef TC_MARCH_GROUPS
-#define TC_MARCH_GROUPS 1
-#endif
-// NG groups of 32 NW threads, one thread per radial index in each; CTA = JT
-// lines (j0 .. j0+JT-1) x KC planes.
+// The solve warpgroup: warp v solves variable v of the CTA's JT lines, plane
+// after plane.
+template <int NW, int JT, class T>
+__device__ __forceinline__ void march_solves(const MarchArgs<T> & A, double * stage, unsigned long long * bar,
+                                             volatile int * abort_flag, int KC) {
+  using L = MarchLayout<NW, JT, T>;
+  constexpr int E = L::E, SL = L::SL, NS = L::NSLOT;
+  const int lane = threadIdx.x & 31;
+  const int v = (threadIdx.x - L::NRT) >> 5;
+  unsigned long long * full = bar + NS;
+  unsigned long long * done = bar + NS + 2;
+  const size_t fo = (size_t)(A.rkstep * 4 + v) * A.xf.stride;
+  for (int step = 0; step < KC; step++) {
+    const int b = step & 1;
+    if (!*abort_flag && !mbar_wait(&full[b], (unsigned)(step >> 1) & 1u)) *abort_flag = 1;
+    double * sdb = stage + (size_t)b * JT * 4 * SL;
+    // one line at a time; the factor rows (6 KB per variable) stay in L1
+#pragma unroll 1
+    for (int jl = 0; jl < JT; jl++)
+      solve_line<E>(sdb + (size_t)(jl * 4 + v) * SL, A.xf.lo + fo, A.xf.w + fo, A.xf.v + fo, lane);
+    mbar_arrive(&done[b]);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void regs_inc() { asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(R)); }
+template <int R>
+__device__ __forceinline__ void regs_dec() { asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(R)); }
+
+// CTA = JT lines (j0 .. j0+JT-1) x KC planes; field warps and the solve
+// warpgroup as above.
 template <int NW, int JT, int IMPL, class T>
-__global__ void __launch_bounds__(32 * NW * TC_MARCH_GROUPS, 1)
+__global__ void __launch_bounds__(MarchLayout<NW, JT, T>::THREADS, 1)
 march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
   using L = MarchLayout<NW, JT, T>;
   extern __shared__ __align__(16) double sm[];
   char * ring = reinterpret_cast<char *>(sm);
   double * stage = reinterpret_cast<double *>(ring + L::STAGE);
+  T * olds = reinterpret_cast<T *>(ring + L::OLDS);
   unsigned long long * bar = reinterpret_cast<unsigned long long *>(ring + L::BAR);
+  volatile int * abort_flag = reinterpret_cast<volatile int *>(bar + L::NBAR);
+  volatile int * issued_p = abort_flag + 1;
+  int * release_cnt = const_cast<int *>(abort_flag + 2);
   const int tx = threadIdx.x;
   const int njg = A.g.ny / JT;
   const int j0 = (int)(blockIdx.x % njg) * JT + 1;   // odd
   const int k0 = (int)(blockIdx.x / njg) * A.KC + 1;
   const int k1 = k0 + A.KC;   // planes k0 .. k1-1 are computed; k0-1 .. k1 are read
   if (tx == 0) {
-    for (int s = 0; s < NSLOT; s++) mbar_init(&bar[s], 1);
+    for (int s = 0; s < L::NSLOT; s++) mbar_init(&bar[s], 1);
+    mbar_init(&bar[L::NSLOT + 0], L::NRT);   // full: every field thread
+    mbar_init(&bar[L::NSLOT + 1], L::NRT);
+    mbar_init(&bar[L::NSLOT + 2], 128);      // done: every solve thread
+    mbar_init(&bar[L::NSLOT + 3], 128);
+    mbar_init(&bar[L::NSLOT + 4], 1);        // olds: the issuing thread's expected bytes
+    mbar_init(&bar[L::NSLOT + 5], 1);
+    *abort_flag = 0;
+    for (int sl = 0; sl < L::NSLOT; sl++) release_cnt[sl] = 0;
     fence_mbar_init();
   }
   // staging lines are zero past each line's unknowns for the whole march
   for (int e = tx; e < 2 * JT * 4 * L::SL; e += blockDim.x) stage[e] = 0.;
   __syncthreads();
   const double dt = *dtp;
-  if constexpr (TC_MARCH_GROUPS == 1) {
-    march_group<NW, JT, IMPL, 2>(A, ring, stage, bar, j0, k0, k1, dt);
+  if (tx < L::NRT) {
+    if constexpr (L::REGS > 0) regs_inc<L::REGS_FIELD>();
+    march_fields<NW, JT, IMPL, T>(A, ring, stage, olds, bar, abort_flag, release_cnt, issued_p, j0, k0, k1, dt);
   } else {
-    if (tx < 32 * NW) march_group<NW, JT, IMPL, 0>(A, ring, stage, bar, j0, k0, k1, dt);
-    else march_group<NW, JT, IMPL, 1>(A, ring, stage, bar, j0, k0, k1, dt);
+    if constexpr (L::REGS > 0) regs_dec<L::REGS_SOLVE>();
+    const bool solve_x = IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0;
+    if (solve_x) march_solves<NW, JT, T>(A, stage, bar, abort_flag, A.KC);
   }
+  __syncthreads();
+  if (tx == 0 && *abort_flag) atomicOr(A.status, ST_TIMEOUT);
 }
 
 #ifndef TC_MARCH_JT
@@ -754,9 +838,8 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
 #endif
 // Planes per CTA, at most: each CTA's start (coefficients, barriers, the first
 // planes' copies) overlaps nothing at one CTA per SM, and its two halo planes
-// are read twice. Measured at 256 x 1024 x 512 (ms per launch): 16 7.01, 32
-// 6.86, 64 6.82, 128 6.81-7.03. Smaller grids take fewer planes per CTA when
-// the last wave of CTAs would leave SMs idle (march_planes).
+// are read twice. Smaller grids take fewer planes per CTA when the last wave
+// of CTAs would leave SMs idle (march_planes).
 #ifndef TC_MARCH_KC
 #define TC_MARCH_KC 64
 #endif
@@ -767,6 +850,7 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
 template <int NW, class T>
 static int march_planes(const Geo & g) {
   constexpr int JT = TC_MARCH_JT;
+  using L = MarchLayout<NW, JT, T>;
   static int per_sm[16], sms[16];   // per device: resident CTAs of this instance, SM count
   int dev = 0;
   cudaGetDevice(&dev);
@@ -774,8 +858,7 @@ static int march_planes(const Geo & g) {
   if (per_sm[dev] == 0) {
     int b = 0, n = 0;
     // a failed query falls back to one CTA on 148 SMs and clears its own error
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, march_predict_kernel<NW, JT, 1, T>,
-                                                      32 * NW * TC_MARCH_GROUPS, MarchLayout<NW, JT, T>::BYTES) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, march_predict_kernel<NW, JT, 1, T>, L::THREADS, L::BYTES) !=
         cudaSuccess) {
       b = 0;
       cudaGetLastError();
@@ -799,11 +882,12 @@ static int march_planes(const Geo & g) {
 template <int NW, class T>
 void launch_march_nw(MarchArgs<T> A, const double * dtp, cudaStream_t st) {
   constexpr int JT = TC_MARCH_JT;   // ny is a power of two >= 4
+  using L = MarchLayout<NW, JT, T>;
   A.KC = march_planes<NW, T>(A.g);
   const long long nblk = (long long)(A.g.ny / JT) * (A.g.nz / A.KC);
   const int mask = (A.bc.implicit[0] ? 1 : 0) | (A.bc.implicit[1] ? 2 : 0) | (A.bc.implicit[2] ? 4 : 0);
-  const unsigned grid = (unsigned)nblk, block = 32 * NW * TC_MARCH_GROUPS;
-  const size_t smem = MarchLayout<NW, JT, T>::BYTES;
+  const unsigned grid = (unsigned)nblk, block = L::THREADS;
+  const size_t smem = L::BYTES;
   if constexpr (sizeof(T) == 8) {   // IMPL -2: run-time implicit flags plus the closure forcing
     if (A.ss.frc[0]) {
       march_predict_kernel<NW, JT, -2, T><<<grid, block, smem, st>>>(A, dtp);

@@ -175,6 +175,9 @@ def test_tdm_bit_exact_with_reference(lib, key):
 def test_boundary_entry_points_match_oracle(lib, tmp_path):
     case = ic.taylor_couette(12, 8, 8, 3400.0)
     d0 = ic.write_ic(case, str(tmp_path / "ic"))
+    # the wall values are the library's parameters, which earlier tests may have changed
+    from simpletcsolver_b200.solver import params_of as solver_params
+    assert lib.tcgpu_set_params(C.byref(solver_params(case))) == 0
     d = abi.DomainT()
     assert lib.domain_init(d0.encode(), C.byref(d)) == 0
     od = tn.load_domain(d0)
