@@ -91,12 +91,13 @@ def parse_args(argv=None):
                     help="steps of the FP32-storage vs FP64 accuracy runs (0: skip)")
     ap.add_argument("--no-closure", action="store_true", help="skip the learned-closure arm")
     ap.add_argument("--no-planar", action="store_true", help="skip the planar-channel workload")
-    ap.add_argument("--closure-pairs", type=int, default=48, help="training pairs from the fine run")
+    ap.add_argument("--closure-pairs", type=int, default=200, help="training pairs from the fine run")
     ap.add_argument("--closure-epochs", type=int, default=60)
     ap.add_argument("--closure-warm", type=int, default=200,
                     help="fine steps before the first pair (lets the initial noise decay)")
-    ap.add_argument("--closure-window", type=int, default=240,
+    ap.add_argument("--closure-window", type=int, default=1200,
                     help="fine steps of the torque comparison window")
+    ap.add_argument("--closure-batch", type=int, default=8)
     return ap.parse_args(argv)
 
 
@@ -337,8 +338,9 @@ def gpu_arm(args, rank, world, local):
     nx, ny, nz = parse_grid(args.grid)
     case = ic.taylor_couette(nx, ny, nz, 1.0e4)
     td = tempfile.mkdtemp(prefix="tcbench")
-    d0 = ic.write_ic(case, os.path.join(td, "ic"))
-    s = Solver.from_ic(d0, case=case, lib=lib)
+    d0 = os.path.join(td, "ic")
+    # the seeded initial field generated on the device (no 1.1 GB NPY per field)
+    s = Solver.from_case(case, d0, lib=lib)
     s.set_coherence(abi.PIN_HOST)
     s.push()
     K, W = args.steps, args.warmup
@@ -383,6 +385,18 @@ def gpu_arm(args, rank, world, local):
         nc = (nx + 2) * (ny + 2) * (nz + 2)
         e2e = {"value": e_units / e_el / 1e6, "unit": UNIT, "h2d_bytes_per_step": (nf + 4 * nc) * 8,
                "d2h_bytes_per_step": (nf + 5 * nc) * 8, "timing": "host wall clock around synchronous integrate()"}
+        # the resident API end to end: the state stays on the device for K steps
+        # (tcgpu_run), then every field comes back once, as before a save
+        s.set_coherence(abi.NO_COHERENCE | abi.PIN_HOST)
+        s.push()
+        t0 = time.perf_counter()
+        s.run(K)
+        s.pull(abi.FIELDS)
+        el = time.perf_counter() - t0
+        r_el, r_units = aggregate(el, ncell * K, world)
+        e2e["resident_api"] = {"value": r_units / r_el / 1e6, "unit": UNIT, "steps": K,
+                               "d2h_bytes": (nf + 5 * nc) * 8,
+                               "timing": "host wall clock around tcgpu_run(K steps) + one tcgpu_pull of all fields"}
     s.release()
     gpu_launches = sum(launches)
 
@@ -406,7 +420,7 @@ def gpu_arm(args, rank, world, local):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": elapsed * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field (no dataset involved)",
+            "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field generated on the device (no dataset involved)",
             "config": {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz], "Re": 1.0e4,
                        "coef_dt_adv": case.coef_dt_adv, "implicit": "x", "parallelism": f"replicas{world}",
                        "l2": "no flush: every field (1.09 GB at 256x1024x512) exceeds the 126 MB L2"},
@@ -436,7 +450,7 @@ def fp32_storage_arm(args, lib, d0, case, world, peak, value64):
     from simpletcsolver_b200.solver import Solver
     K, W = args.steps, args.warmup
     ncell = case.ncells
-    s = Solver.from_ic(d0, case=case, lib=lib, storage=4)
+    s = Solver.from_case(case, d0, lib=lib, storage=4)
     s.push()
     s.run(W)
     ms, _, launches = run_timed(lib, s, K, 0)
@@ -456,7 +470,7 @@ def fp32_storage_arm(args, lib, d0, case, world, peak, value64):
     if n > 0:
         runs = {}
         for storage in (8, 4):
-            s = Solver.from_ic(d0, case=case, lib=lib, storage=storage)
+            s = Solver.from_case(case, d0, lib=lib, storage=storage)
             try:
                 s.push()
                 dts = s.run(n)
@@ -539,13 +553,14 @@ def closure_arm(args, lib, d0, case, peaks):
     td = os.path.dirname(d0)
     dc = closure.write_coarse_ic(case, os.path.join(td, "coarse"))
     cc = closure.coarse_case(case)
-    fine = Solver.from_ic(d0, case=case, lib=lib)
+    fine = Solver.from_case(case, d0, lib=lib)
     ca = Solver.from_ic(dc, case=cc, lib=lib)
     cb = Solver.from_ic(dc, case=cc, lib=lib)
     cf = Solver.from_ic(dc, case=cc, lib=lib)     # the fine run restricted, for the coarse-grid diagnostics
+    cd = Solver.from_ic(dc, case=cc, lib=lib)     # closure forcing recomputed every RK substep
     out = {"grid_fine": [case.nx, case.ny, case.nz], "grid_coarse": [cc.nx, cc.ny, cc.nz]}
     try:
-        for s in (fine, ca, cb, cf):
+        for s in (fine, ca, cb, cf, cd):
             closure.resident(s)
         fine.run(args.closure_warm)
         in_scale = (0.05, 1.0, 0.05)
@@ -559,8 +574,19 @@ def closure_arm(args, lib, d0, case, peaks):
         before = closure.relative_error(net, data, held)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        batch = 4
+        batch = args.closure_batch
         hist = closure.train(net, data, train, epochs=args.closure_epochs, batch=batch, lr=2e-3)
+        # the learned wall model (near-wall reconstruction for the torque), fitted
+        # on the same training pairs; its injection formula checked against the
+        # fine solver's own on the fine field
+        wm = closure.WallModel.fit(data, train, fine, ca)
+        fine_formula = closure.WallModel.fine_injection(wm, fine.radial_slab("uy", 1, 1))
+        fine_diag = fine.diagnostics()["injection_u"]
+        held_err = []
+        for q in held:
+            pred = wm.predict(data.wall_x[q])
+            tgt = closure.block_mean(data.wall_y[q], ca).ravel()
+            held_err.append(float(np.sqrt(np.mean((pred - tgt) ** 2)) / np.sqrt(np.mean(tgt ** 2))))
         train_s = time.perf_counter() - t0
         err_train = closure.relative_error(net, data, train)
         err_held = closure.relative_error(net, data, held)
@@ -578,15 +604,16 @@ def closure_arm(args, lib, d0, case, peaks):
         tflops = CLOSURE_FLOP_PER_CELL * net.ncell / (fwd_ms / 1e3) / 1e12
         peak = float(peaks.get("bf16_tflops", 1590.0))
         # torque window: fine, coarse with and without the closure from one state
-        for s in (ca, cb):
+        for s in (ca, cb, cd):
             s._check(lib.tcgpu_coarsen(C.byref(fine.domain), C.byref(fine.fluid), C.byref(s.domain),
                                        C.byref(s.fluid)), "coarsen")
         def restricted_torque():
             cf._check(lib.tcgpu_coarsen(C.byref(fine.domain), C.byref(fine.fluid), C.byref(cf.domain),
                                         C.byref(cf.fluid)), "coarsen")
-            return cf.diagnostics()["injection_u"]
+            return cf.diagnostics()["injection_u"], wm.torque(cf)
 
-        ft, fq, rq = [0.0], [fine.diagnostics()["injection_u"]], [restricted_torque()]
+        r0 = restricted_torque()
+        ft, fq, rq, rw = [0.0], [fine.diagnostics()["injection_u"]], [r0[0]], [r0[1]]
         fine_s = 0.0
         for _ in range(max(1, args.closure_window // 10)):
             torch.cuda.synchronize()
@@ -594,18 +621,29 @@ def closure_arm(args, lib, d0, case, peaks):
             ft.append(ft[-1] + float(np.sum(fine.run(10))))
             fine_s += time.perf_counter() - t0
             fq.append(fine.diagnostics()["injection_u"])
-            rq.append(restricted_torque())
+            r = restricted_torque()
+            rq.append(r[0])
+            rw.append(r[1])
+        # the coarse runs from the window's start state: closure forcing per step
+        # (timed, its per-step diagnostics included), no closure, forcing per RK substep
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        at, aq = closure.run_coarse(ca, ft[-1], net, in_scale, t_scale)
+        at, aq, aw = closure.run_coarse(ca, ft[-1], net, in_scale, t_scale, wall_model=wm)
+        torch.cuda.synchronize()
         coarse_s = time.perf_counter() - t0
-        bt, bq = closure.run_coarse(cb, ft[-1])
+        bt, bq, bw = closure.run_coarse(cb, ft[-1], wall_model=wm)
+        dtm, dq, dw = closure.run_coarse(cd, ft[-1], net, in_scale, t_scale, wall_model=wm, per_substep=True)
         tq_f = closure.time_average(ft, fq)
         tq_r = closure.time_average(ft, rq)
         tq_c = closure.time_average(at, aq)
         tq_p = closure.time_average(bt, bq)
+        tw_r = closure.time_average(ft, rw)
+        tw_c = closure.time_average(at, aw)
+        tw_p = closure.time_average(bt, bw)
+        tw_d = closure.time_average(dtm, dw)
         # mean azimuthal velocity profile at the end of the window (coarse grid)
         prof = {}
-        for name, s in (("restricted_fine", cf), ("closure", ca), ("plain", cb)):
+        for name, s in (("restricted_fine", cf), ("closure", ca), ("plain", cb), ("closure_per_substep", cd)):
             s.pull(abi.UY)
             prof[name] = s.field("uy")[1:-1, 1:-1, 1:-1].mean(axis=(0, 1))
         perr = lambda a: float(np.linalg.norm(a - prof["restricted_fine"]) / np.linalg.norm(prof["restricted_fine"]))
@@ -618,24 +656,32 @@ def closure_arm(args, lib, d0, case, peaks):
             "forward": {"ms": fwd_ms, "tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
                         "flop_per_cell": CLOSURE_FLOP_PER_CELL,
                         "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
+            "wall_model": {"weights": [float(v) for v in wm.w], "fit_samples": wm.samples,
+                           "fit_rms": wm.fit_rms, "held_out_rel_rms": float(np.mean(held_err)),
+                           "formula_vs_fine_injection": abs(fine_formula - fine_diag) / abs(fine_diag)},
             "torque_window": {
                 "sim_time": ft[-1], "fine_steps": 10 * (len(ft) - 1), "coarse_steps": len(at) - 1,
-                "fine": tq_f, "restricted_fine": tq_r, "coarse_closure": tq_c, "coarse_plain": tq_p,
-                "rel_err_closure": abs(tq_c - tq_f) / abs(tq_f), "rel_err_plain": abs(tq_p - tq_f) / abs(tq_f),
-                "rel_err_closure_vs_restricted": abs(tq_c - tq_r) / abs(tq_r),
-                "rel_err_plain_vs_restricted": abs(tq_p - tq_r) / abs(tq_r),
-                # the coarse grid's wall-gradient estimator calibrated once, at the
-                # window start, by the ratio fine / restricted-fine torque
-                "estimator_calibration": fq[0] / rq[0],
-                "rel_err_closure_calibrated": abs(tq_c * fq[0] / rq[0] - tq_f) / abs(tq_f),
-                "rel_err_plain_calibrated": abs(tq_p * fq[0] / rq[0] - tq_f) / abs(tq_f),
-                "mean_uy_profile_rel_err": {"closure": perr(prof["closure"]), "plain": perr(prof["plain"])},
+                "fine": tq_f,
+                # the coarse grid's torque with the learned wall model (the closure's estimator)
+                "restricted_fine": tw_r, "coarse_closure": tw_c, "coarse_plain": tw_p,
+                "coarse_closure_per_substep": tw_d,
+                "rel_err_closure": abs(tw_c - tq_f) / abs(tq_f), "rel_err_plain": abs(tw_p - tq_f) / abs(tq_f),
+                "rel_err_closure_per_substep": abs(tw_d - tq_f) / abs(tq_f),
+                "rel_err_restricted_fine": abs(tw_r - tq_f) / abs(tq_f),
+                # the reference's injection formula applied on the coarse grid as it is
+                "raw_estimator": {
+                    "restricted_fine": tq_r, "coarse_closure": tq_c, "coarse_plain": tq_p,
+                    "rel_err_closure": abs(tq_c - tq_f) / abs(tq_f), "rel_err_plain": abs(tq_p - tq_f) / abs(tq_f),
+                    "rel_err_closure_vs_restricted": abs(tq_c - tq_r) / abs(tq_r),
+                    "rel_err_plain_vs_restricted": abs(tq_p - tq_r) / abs(tq_r)},
+                "mean_uy_profile_rel_err": {"closure": perr(prof["closure"]), "plain": perr(prof["plain"]),
+                                            "closure_per_substep": perr(prof["closure_per_substep"])},
                 "wall_s_fine": fine_s, "wall_s_coarse_closure": coarse_s,
                 "speedup_vs_fine": (fine_s / ft[-1]) / (coarse_s / max(at[-1], 1e-30)),
             },
         })
     finally:
-        for s in (fine, ca, cb, cf):
+        for s in (fine, ca, cb, cf, cd):
             s.release()
     return out
 

@@ -280,6 +280,31 @@ int tcgpu_log_quantities(const domain_t * domain, fluid_t * fluid, double out[9]
  * directory (src/statistics.c:250-300): num.npy, the domain, and the eight
  * arrays with those shapes (nothing is written when no sample was collected).
  * mean_uy: profile[i], i = 0..nx+1, = mean of uy over j, k and the samples. */
+/* A seeded initial field generated on the device, in place of fluid_init for
+ * grids whose NPY files would be large (no counterpart in the reference, whose
+ * initial_condition/main.py writes NPY files). Allocates the fluid_t arrays as
+ * fluid_init does (Re and Pr from the environment), creates the device context
+ * and fills it: uy the laminar profile (circular Couette A r + B / r between
+ * the wall speeds of tcgpu_set_params when the domain is curved, linear when
+ * planar), t linear between its wall values, p = 0, plus uniform noise in
+ * [-noise_u, noise_u) on ux (interior faces), uy and uz and in
+ * [-noise_t, noise_t) on t; each value's noise depends only on the seed, the
+ * field and the cell. Boundary values and periodic images as after fluid_init;
+ * the caller's host arrays receive the same field. */
+typedef struct {
+  uint64_t seed;
+  double noise_u, noise_t;
+} tcgpu_ic_t;
+int tcgpu_fluid_init_generated(const domain_t * domain, fluid_t * fluid, const tcgpu_ic_t * ic);
+
+/* Values of one field (TCGPU_UX ... TCGPU_T) at the radial indices i0 ..
+ * i0 + count - 1 of the reference's index space (ux: faces 1 .. nx+1, the
+ * others 0 .. nx+1) over the interior j, k of the current device state, into
+ * the host array out[((k - 1) ny + j - 1) count + c]. No counterpart in the
+ * reference; for wall-layer diagnostics that need a few radial planes without
+ * copying the whole field. */
+int tcgpu_radial_slab(const domain_t * domain, fluid_t * fluid, unsigned field, int i0, int count, double * out);
+
 int tcgpu_statistics_collect(const domain_t * domain, fluid_t * fluid);
 int tcgpu_statistics_reset(const domain_t * domain, fluid_t * fluid);
 int tcgpu_statistics_get(const domain_t * domain, fluid_t * fluid, size_t * num, double * const out[8]);

@@ -40,6 +40,10 @@ class FluidT(C.Structure):
                 ("lzz", ArrayT), ("Re", C.c_double), ("Pr", C.c_double)]
 
 
+class IcT(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("noise_u", C.c_double), ("noise_t", C.c_double)]
+
+
 class ParamsT(C.Structure):
     _fields_ = [("uy_xm", C.c_double), ("uy_xp", C.c_double), ("t_xm", C.c_double), ("t_xp", C.c_double),
                 ("implicit_x", C.c_int), ("implicit_y", C.c_int), ("implicit_z", C.c_int),
@@ -92,6 +96,9 @@ _EXT_SIGS = {
     "tcgpu_run": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_int, c_double_p]),
     "tcgpu_diagnostics": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 9]),
     "tcgpu_log_quantities": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_double * 9]),
+    "tcgpu_fluid_init_generated": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.POINTER(IcT)]),
+    "tcgpu_radial_slab": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.c_uint, C.c_int, C.c_int,
+                                    c_double_p]),
     "tcgpu_statistics_collect": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_statistics_reset": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT)]),
     "tcgpu_statistics_get": (C.c_int, [C.POINTER(DomainT), C.POINTER(FluidT), C.POINTER(C.c_size_t),

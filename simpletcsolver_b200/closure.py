@@ -207,6 +207,10 @@ class Dataset:
         self.T = torch.zeros(nmax, ncell * NOUT, dtype=torch.float32, device="cuda")
         self.tau = []
         self.n = 0
+        # wall-model pairs: the restricted state's first WALL_DEPTH radial cells
+        # of uy at the inner wall, and the fine state's first-cell uy there
+        self.wall_x = []
+        self.wall_y = []
 
 
 def generate(fine, coarse_a, coarse_b, nsamples: int, gap: int, in_scale, data: Dataset | None = None,
@@ -231,6 +235,8 @@ def generate(fine, coarse_a, coarse_b, nsamples: int, gap: int, in_scale, data: 
         x = data.X[data.n + len(raw)]
         coarse_a._check(lib.tcgpu_closure_input(C.byref(coarse_a.domain), C.byref(coarse_a.fluid),
                                                 _d3(in_scale), NIN, _p(x)), "closure_input")
+        data.wall_x.append(coarse_a.radial_slab("uy", 1, WALL_DEPTH))
+        data.wall_y.append(fine.radial_slab("uy", 1, 1)[:, :, 0])
         dt_c = coarse_a.decide_dt()
         dt_f = fine.decide_dt()
         n = int(max(1, min(max_sub, math.floor(dt_c / dt_f))))
@@ -249,6 +255,78 @@ def generate(fine, coarse_a, coarse_b, nsamples: int, gap: int, in_scale, data: 
         data.T[data.n].copy_(torch.from_numpy((r / np.asarray(t_scale, np.float32)[None, :]).ravel()))
         data.n += 1
     return data, np.asarray(t_scale, dtype=np.float64)
+
+
+# ---------------------------------------------------------------- wall model
+WALL_DEPTH = 3   # coarse radial cells the wall model reads
+
+
+class WallModel:
+    """Learned near-wall reconstruction for the coarse grid's torque.
+
+    The energy injection at the inner wall (src/logging/injection.c:55-73) is,
+    per wall face, affine in the first cell's uy: with ux = 0 on the wall face
+    lyx0 vanishes, lyx1 = c1 uy(1) (lyx.c:70-83, the wall weight of uy(0) is 0)
+    and lxy = (uy(1) - uy(0)) / hx (lxy.c:19-49), so
+        face = nu (-J / hx) uy(0) [(c1 + 1 / hx) uy(1) - uy(0) / hx]
+    with J = JDXF(1), hx = HXXF(1) of the grid it is evaluated on. A coarse
+    face covers 4 x 4 fine faces; the coarse grid's own first-cell value
+    (a mean over 4 fine cells in x) misses the wall gradient the fine cells
+    resolve. The model predicts the mean fine first-cell uy over the 16 fine
+    faces of each coarse face from the coarse uy(1..WALL_DEPTH) there, linear
+    with an intercept, fitted by least squares on the training pairs (coarse
+    state = the restricted fine state, target = the fine state at the same
+    time). The torque of a coarse state is then the fine-grid injection of the
+    predicted first-cell values. The outer wall is at rest (uy(nx+1) = 0), so
+    its term is zero."""
+
+    def __init__(self, fine, coarse, weights):
+        self.w = np.asarray(weights, dtype=np.float64)
+        d = fine.domain
+        self.nu = 1.0 / fine.fluid.Re
+        J, hx = d.jdxf[0], d.hxxf[0]   # JDXF(1), HXXF(1): face arrays start at face 1 (array_macros/domain)
+        c1 = -0.5 / J * (-d.jdxc[0] / d.hxxc[0] + d.jdxc[1] / d.hxxc[1])
+        self.uw = fine_wall_velocity(fine)
+        k = self.nu * (-J / hx) * self.uw
+        self.a = k * (-self.uw / hx)         # per fine face: a + b uy(1)
+        self.b = k * (c1 + 1.0 / hx)
+        self.ratio = (fine.ny // coarse.ny) * (fine.nz // coarse.nz)
+
+    @staticmethod
+    def fine_injection(model, uy1) -> float:
+        return float(model.a * uy1.size + model.b * np.sum(uy1))
+
+    @classmethod
+    def fit(cls, data: "Dataset", idx, fine, coarse):
+        X = np.concatenate([data.wall_x[s].reshape(-1, WALL_DEPTH) for s in idx])
+        y = np.concatenate([block_mean(data.wall_y[s], coarse).ravel() for s in idx])
+        A = np.hstack([X, np.ones((X.shape[0], 1))])
+        w, *_ = np.linalg.lstsq(A, y, rcond=None)
+        m = cls(fine, coarse, w)
+        m.fit_rms = float(np.sqrt(np.mean((A @ w - y) ** 2)))
+        m.samples = int(X.shape[0])
+        return m
+
+    def predict(self, feats) -> np.ndarray:
+        return feats.reshape(-1, WALL_DEPTH) @ self.w[:WALL_DEPTH] + self.w[WALL_DEPTH]
+
+    def torque(self, s) -> float:
+        """Inner-wall energy injection of the coarse state s with the predicted
+        fine first-cell values."""
+        pred = self.predict(s.radial_slab("uy", 1, WALL_DEPTH))
+        return float(self.ratio * (self.a * pred.size + self.b * np.sum(pred)))
+
+
+def fine_wall_velocity(s) -> float:
+    """uy on the inner wall (the solver's wall value, read from the device)."""
+    return float(s.radial_slab("uy", 0, 1)[0, 0, 0])
+
+
+def block_mean(a, coarse):
+    """Mean over the fine (k, j) blocks of each coarse wall face."""
+    nz, ny = a.shape
+    fz, fy = nz // coarse.nz, ny // coarse.ny
+    return a.reshape(coarse.nz, fz, coarse.ny, fy).mean(axis=(1, 3))
 
 
 def train(net: ClosureNet, data: Dataset, idx, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0,
@@ -295,30 +373,54 @@ def relative_error(net: ClosureNet, data: Dataset, idx) -> float:
     return num / den
 
 
-def run_coarse(s, t_end: float, net: ClosureNet | None = None, in_scale=None, t_scale=None, max_steps: int = 100000):
+def run_coarse(s, t_end: float, net: ClosureNet | None = None, in_scale=None, t_scale=None, max_steps: int = 100000,
+               wall_model: WallModel | None = None, per_substep: bool = False):
     """Adaptive steps of the device-resident coarse solver s until its time
-    reaches t_end, with the network's forcing (computed from the state at the
-    start of each step, held over the step) when net is given. Returns the
-    times and the energy injection (inner-wall torque) after every step."""
+    reaches t_end, with the network's forcing when net is given: computed from
+    the state at the start of each step and held over the step, or, with
+    per_substep, computed again from the state at the start of every RK
+    substep (the step then runs through the reference's stage entry points).
+    Returns the times, the energy injection (inner-wall torque, the
+    reference's estimator on this grid) after every step and, with
+    wall_model, the wall model's torque after every step."""
     lib = s.lib
     st = stream_of(s)
     times, torque = [0.0], [s.diagnostics()["injection_u"]]
+    wall = [wall_model.torque(s)] if wall_model is not None else None
+
+    def forcing():
+        s._check(lib.tcgpu_closure_input(C.byref(s.domain), C.byref(s.fluid), _d3(in_scale), NIN,
+                                         _p(net.a[0])), "closure_input")
+        net.forward(stream=st, keep=False)
+        s._check(lib.tcgpu_set_forcing(C.byref(s.domain), C.byref(s.fluid), _p(net.out), NOUT, _d3(t_scale)),
+                 "set_forcing")
+
     t = 0.0
     for _ in range(max_steps):
         if t >= t_end:
             break
-        if net is not None:
-            s._check(lib.tcgpu_closure_input(C.byref(s.domain), C.byref(s.fluid), _d3(in_scale), NIN,
-                                             _p(net.a[0])), "closure_input")
-            net.forward(stream=st, keep=False)
-            s._check(lib.tcgpu_set_forcing(C.byref(s.domain), C.byref(s.fluid), _p(net.out), NOUT, _d3(t_scale)),
-                     "set_forcing")
-        t += float(s.run(1)[0])
+        if net is not None and per_substep:
+            dt = s.decide_dt()
+            for rk in range(3):
+                forcing()
+                s.predict(rk, dt)
+                s.compute_potential(rk, dt)
+                s.correct_velocity(rk, dt)
+                s.update_pressure(rk, dt)
+            t += dt
+        else:
+            if net is not None:
+                forcing()
+            t += float(s.run(1)[0])
         times.append(t)
         torque.append(s.diagnostics()["injection_u"])
+        if wall is not None:
+            wall.append(wall_model.torque(s))
     if net is not None:
         s._check(lib.tcgpu_set_forcing(C.byref(s.domain), C.byref(s.fluid), None, NOUT, _d3((1, 1, 1))),
                  "set_forcing")
+    if wall is not None:
+        return np.asarray(times), np.asarray(torque), np.asarray(wall)
     return np.asarray(times), np.asarray(torque)
 
 

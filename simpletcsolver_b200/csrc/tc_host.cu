@@ -101,6 +101,8 @@ struct Ctx {
   // and statistics read the velocity-gradient tensors of exactly those fields
   // (src/fluid/predict/main.c:56-82 is their only writer).
   bool have_prev = false;
+  double * slab = nullptr;    // tcgpu_radial_slab staging, slab_n doubles
+  size_t slab_n = 0;
   Stats stats{};              // device statistics (src/statistics.c), allocated on first use
   size_t stat_num = 0;
   double * stat_prof = nullptr;
@@ -1187,6 +1189,65 @@ int tcgpu_statistics_get(const domain_t * domain, fluid_t * fluid, size_t * num,
     }
   }
   return finish(*c, "tcgpu_statistics_get");
+}
+
+int tcgpu_io_fluid_alloc(const domain_t * domain, fluid_t * fluid);
+
+int tcgpu_fluid_init_generated(const domain_t * domain, fluid_t * fluid, const tcgpu_ic_t * ic) {
+  if (domain == nullptr || fluid == nullptr || ic == nullptr) return fail("tcgpu_fluid_init_generated: NULL argument");
+  if (!(ic->noise_u >= 0.) || !(ic->noise_t >= 0.)) return fail("tcgpu_fluid_init_generated: negative noise");
+  if (check_domain(domain)) return 1;
+  if (tcgpu_io_fluid_alloc(domain, fluid)) return 1;
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  // radial profiles at the cell centres i = 0..nx+1 (the walls included, as
+  // initial_condition/main.py lays out xc): circular Couette A r + B / r when
+  // curved, linear when planar; the scalar linear between its wall values
+  const int nx = c->nx;
+  std::vector<double> prof(2 * ((size_t)nx + 2));
+  const double ri = domain->xf[0], ro = domain->xf[nx], lx = ro - ri;
+  const double ui = c->bc.uy_xm, uo = c->bc.uy_xp;
+  const double A = (uo * ro - ui * ri) / (ro * ro - ri * ri), B = (ui - A * ri) * ri;
+  for (int i = 0; i <= nx + 1; i++) {
+    const double r = domain->xc[i];
+    prof[i] = domain->is_curved ? A * r + B / r : ui + (uo - ui) * (r - ri) / lx;
+    prof[nx + 2 + i] = c->bc.t_xm + (c->bc.t_xp - c->bc.t_xm) * (r - ri) / lx;
+  }
+  double * dprof = dalloc(*c, prof.size());
+  if (!dprof) return fail("tcgpu_fluid_init_generated: cudaMalloc failed");
+  CK(cudaMemcpyAsync(dprof, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+  invalidate_dt(*c);
+  launch_initial_field(c->g, c->f(), dprof, dprof + nx + 2, ic->seed, ic->noise_u, ic->noise_t, c->st);
+  CK(cudaGetLastError());
+  apply_bcs(*c, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T);
+  // the caller's arrays hold the same field, as after fluid_init
+  if (pull_fields(*c, fluid, TCGPU_UX | TCGPU_UY | TCGPU_UZ | TCGPU_P | TCGPU_T)) return 1;
+  const int rc = finish(*c, "tcgpu_fluid_init_generated");
+  cudaFree(dprof);
+  c->allocs.erase(std::remove(c->allocs.begin(), c->allocs.end(), static_cast<void *>(dprof)), c->allocs.end());
+  return rc;
+}
+
+int tcgpu_radial_slab(const domain_t * domain, fluid_t * fluid, unsigned field, int i0, int count, double * out) {
+  Ctx * c = get_ctx(domain, fluid);
+  if (!c) return 1;
+  if (out == nullptr) return fail("tcgpu_radial_slab: out is NULL");
+  if (field != TCGPU_UX && field != TCGPU_UY && field != TCGPU_UZ && field != TCGPU_P && field != TCGPU_PSI &&
+      field != TCGPU_T)
+    return fail("tcgpu_radial_slab: field must be one of TCGPU_UX, _UY, _UZ, _P, _PSI, _T");
+  const int lo = field == TCGPU_UX ? 1 : 0;
+  if (count < 1 || i0 < lo || i0 + count - 1 > c->nx + 1)
+    return fail("tcgpu_radial_slab: radial range %d..%d outside %d..%d", i0, i0 + count - 1, lo, c->nx + 1);
+  const size_t n = (size_t)count * c->ny * c->nz;
+  if (n > c->slab_n) {
+    c->slab = dalloc(*c, n);
+    if (!c->slab) return fail("tcgpu_radial_slab: cudaMalloc failed");
+    c->slab_n = n;
+  }
+  launch_slab(c->g, dev_field(*c, field), field_bytes(*c, field), field == TCGPU_UX, i0, count, c->slab, c->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, c->slab, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return finish(*c, "tcgpu_radial_slab");
 }
 
 int tcgpu_io_write_statistics(const char dirname[], const domain_t * domain, size_t num, const double * const a[8]);

@@ -230,7 +230,26 @@ int domain_save(const char dirname[], const domain_t * domain) {
   return 0;
 }
 
+// the host arrays of fluid_t (src/fluid/init.c:42-68) and Re, Pr from the
+// environment (:112-122); shared by fluid_init and the device-generated
+// initial field
+__attribute__((visibility("hidden"))) int tcgpu_io_fluid_alloc(const domain_t * domain, fluid_t * fluid);
+
 int fluid_init(const char dirname_ic[], const domain_t * domain, fluid_t * fluid) {
+  if (domain == nullptr || fluid == nullptr) return err("fluid_init: NULL argument");
+  if (tcgpu_io_fluid_alloc(domain, fluid)) return 1;
+  if (load_field(domain, dirname_ic, "ux", &fluid->ux) || load_field(domain, dirname_ic, "uy", &fluid->uy) ||
+      load_field(domain, dirname_ic, "uz", &fluid->uz) || load_field(domain, dirname_ic, "p", &fluid->p) ||
+      load_field(domain, dirname_ic, "t", &fluid->t))
+    return 1;
+  if (fluid_update_boundaries_ux(domain, &fluid->ux) || fluid_update_boundaries_uy(domain, &fluid->uy) ||
+      fluid_update_boundaries_uz(domain, &fluid->uz) || fluid_update_boundaries_p(domain, &fluid->p) ||
+      fluid_update_boundaries_t(domain, &fluid->t))
+    return 1;
+  return 0;
+}
+
+__attribute__((visibility("hidden"))) int tcgpu_io_fluid_alloc(const domain_t * domain, fluid_t * fluid) {
   if (domain == nullptr || fluid == nullptr) return err("fluid_init: NULL argument");
   // array_macros/fluid/*.h NADDS
   static const int C[3][2] = {{1, 1}, {1, 1}, {1, 1}};
@@ -252,14 +271,6 @@ int fluid_init(const char dirname_ic[], const domain_t * domain, fluid_t * fluid
         prepare(domain, SC, &fluid->srcuz[n]) || prepare(domain, SC, &fluid->srct[n]))
       return 1;
   }
-  if (load_field(domain, dirname_ic, "ux", &fluid->ux) || load_field(domain, dirname_ic, "uy", &fluid->uy) ||
-      load_field(domain, dirname_ic, "uz", &fluid->uz) || load_field(domain, dirname_ic, "p", &fluid->p) ||
-      load_field(domain, dirname_ic, "t", &fluid->t))
-    return 1;
-  if (fluid_update_boundaries_ux(domain, &fluid->ux) || fluid_update_boundaries_uy(domain, &fluid->uy) ||
-      fluid_update_boundaries_uz(domain, &fluid->uz) || fluid_update_boundaries_p(domain, &fluid->p) ||
-      fluid_update_boundaries_t(domain, &fluid->t))
-    return 1;
   const char * names[2] = {"Re", "Pr"};
   double * dst[2] = {&fluid->Re, &fluid->Pr};
   for (int n = 0; n < 2; n++) {

@@ -288,6 +288,16 @@ void launch_statistics(const Geo & g, const Coefs & cf, const FieldBufs & f, con
 // mean of uy1 over j and k, divided by the sample count: nx + 2 values
 void launch_stat_profile(const Geo & g, const double * uy1, double inv_count, double * out, cudaStream_t st);
 
+// seeded initial field on the device: uy_prof[i], t_prof[i] (i = 0..nx+1,
+// device arrays) plus uniform noise of amplitude amp_u (ux, uy, uz) and amp_t (t)
+void launch_initial_field(const Geo & g, const FieldBufs & f, const double * uy_prof, const double * t_prof,
+                          unsigned long long seed, double amp_u, double amp_t, cudaStream_t st);
+
+// values of one field at radial indices i0 .. i0+count-1 over the interior
+// j, k into out[((k-1) ny + j-1) count + c] (doubles; a: 8 or 4 bytes per value)
+void launch_slab(const Geo & g, const void * a, int bytes, bool face, int i0, int count, double * out,
+                 cudaStream_t st);
+
 // FP32-storage mode: rows of nref doubles in the reference's layout to and from
 // rows of pitch floats (element e at e + shift)
 void launch_pack32(const double * src, float * dst, size_t rows, int nref, int pitch, int shift, cudaStream_t st);

@@ -195,8 +195,10 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const CoefB & qc_, const
   const double ux_0 = UX(0, 0), ux_p = UX(1, 0);
   const double uy_00 = UY(0, 0), uy_01 = UY(0, 1);
   const double uz_00 = UZ(0, 0), uz_01 = NUZ(0, 0);
-  dl[0] = 0.;
-  if (i >= 2) {
+  // ux has no unknown at i = 1 (face 1 is the wall): its value there is
+  // formed from in-bounds shared-memory neighbours and discarded, so the
+  // whole cell stays one branch-free block the scheduler can interleave
+  {
     const double ux_m = UX(-1, 0);
     const double ux_jm = UX(0, -1), ux_jp = UX(0, 1);
     const double ux_km = MUX(0), ux_kp = NUX(0);
@@ -220,9 +222,9 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const CoefB & qc_, const
     ROUTE(ix, q.lxl * (ux_m - ux_0) + q.lxu * (ux_p - ux_0));        // carries 2 nu
     ROUTE(iy, q.ly * ((ux_jm - ux_0) + (ux_jp - ux_0)));             // carries nu
     ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
-    if constexpr (IMPL == -2) e += ss.frc[VUX][qf];   // closure forcing
-    ss.new_[VUX][qf] = (T)e;
-    dl[0] = ca * e + cb * old_x + cg * gi;
+    if constexpr (IMPL == -2) e += (i >= 2) ? ss.frc[VUX][qf] : 0.;   // closure forcing
+    if (i >= 2) ss.new_[VUX][qf] = (T)e;
+    dl[0] = (i >= 2) ? ca * e + cb * old_x + cg * gi : 0.;
   }
   {
     const double t_0 = TT(0, 0);
@@ -692,8 +694,9 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
         auto old = [&](int v) {
           return use_old ? (double)ob[(size_t)v * JT * OL + JL * (v == VUX ? lf : lc) + (v == VUX ? i - 2 : i - 1)] : 0.;
         };
+        // old(VUX) at i = 1 reads the shared-memory word before the line (discarded)
         cell_a<JT, RL, JL, IMPL>(qa, qb, V, A.bc, A.cf, A.nu, A.kappa, rpr, i, qf + (size_t)JL * lf,
-                                 qc + (size_t)JL * lc, A.ss, ca, cb, cg, i >= 2 ? old(VUX) : 0., old(VT), d2, w2);
+                                 qc + (size_t)JL * lc, A.ss, ca, cb, cg, old(VUX), old(VT), d2, w2);
         dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
         cell_b<JT, RL, JL, IMPL>(qb, V, A.bc, A.cf, A.nu, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
                                  old(VUY), old(VUZ), d2, w2);

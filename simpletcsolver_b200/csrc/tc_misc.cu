@@ -676,6 +676,71 @@ void launch_stat_profile(const Geo & g, const double * uy1, double inv_count, do
   stat_profile_kernel<<<g.nx + 2, 256, 0, st>>>(g, uy1, inv_count, out);
 }
 
+// --------------------------------------------------------------- initial field
+// A seeded initial field generated on the device: uy and t from radial profiles
+// (one value per i, formed on the host), plus uniform noise in [-amp, amp) on
+// ux (interior faces), uy, uz and t. The noise of value q of field f is a
+// function of (seed, f, q) alone (SplitMix64 finaliser of a counter), so the
+// field does not depend on the launch shape. p = 0. Halos are left to the
+// boundary kernels.
+__device__ __forceinline__ double noise(unsigned long long seed, unsigned f, unsigned long long q, double amp) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (q + 1ull + ((unsigned long long)f << 58));
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const double u = (double)(z >> 11) * 0x1.0p-53;   // [0, 1)
+  return amp * (2. * u - 1.);
+}
+
+template <class T>
+__global__ void initial_field_kernel(Geo g, FieldsT<T> f, const double * __restrict__ uy_prof,
+                                     const double * __restrict__ t_prof, unsigned long long seed, double amp_u,
+                                     double amp_t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;   // 0..nx+1
+  const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int k = blockIdx.z + 1;
+  const int nx = g.nx, ny = g.ny;
+  if (i > nx + 1 || j > ny) return;
+  const unsigned long long q = (unsigned long long)i + (unsigned long long)(nx + 2) * ((unsigned long long)(j - 1) +
+                               (unsigned long long)ny * (unsigned long long)(k - 1));
+  f.uy[sidx_c<T>(g, i, j, k)] = (T)(uy_prof[i] + noise(seed, 1, q, amp_u));
+  f.uz[sidx_c<T>(g, i, j, k)] = (T)noise(seed, 2, q, amp_u);
+  f.t[sidx_c<T>(g, i, j, k)] = (T)(t_prof[i] + (amp_t > 0. ? noise(seed, 3, q, amp_t) : 0.));
+  f.p[sidx_c<T>(g, i, j, k)] = 0.;
+  if (i >= 1) f.ux[sidx_f<T>(g, i, j, k)] = (T)((i == 1 || i == nx + 1) ? 0. : noise(seed, 0, q, amp_u));
+}
+
+void launch_initial_field(const Geo & g, const FieldBufs & f, const double * uy_prof, const double * t_prof,
+                          unsigned long long seed, double amp_u, double amp_t, cudaStream_t st) {
+  dim3 block(64, 4, 1);
+  dim3 grid((g.nx + 2 + 63) / 64, (g.ny + 3) / 4, g.nz);
+  if (f.bytes == 4)
+    initial_field_kernel<float><<<grid, block, 0, st>>>(g, f.as<float>(), uy_prof, t_prof, seed, amp_u, amp_t);
+  else
+    initial_field_kernel<double><<<grid, block, 0, st>>>(g, f.as<double>(), uy_prof, t_prof, seed, amp_u, amp_t);
+}
+
+// --------------------------------------------------------------- radial slabs
+// out[((k - 1) ny + j - 1) count + c] = a(i0 + c, j, k) over the interior j, k
+template <class T>
+__global__ void slab_kernel(Geo g, const T * __restrict__ a, bool face, int i0, int count, double * __restrict__ out) {
+  const size_t n = (size_t)count * g.ny * g.nz;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(q % count);
+    const size_t line = q / count;
+    const int j = (int)(line % g.ny) + 1, k = (int)(line / g.ny) + 1;
+    out[q] = (double)a[face ? sidx_f<T>(g, i0 + c, j, k) : sidx_c<T>(g, i0 + c, j, k)];
+  }
+}
+
+void launch_slab(const Geo & g, const void * a, int bytes, bool face, int i0, int count, double * out,
+                 cudaStream_t st) {
+  const size_t n = (size_t)count * g.ny * g.nz;
+  const unsigned blocks = (unsigned)((n + 255) / 256 < 2368 ? (n + 255) / 256 : 2368);
+  if (bytes == 4) slab_kernel<float><<<blocks, 256, 0, st>>>(g, static_cast<const float *>(a), face, i0, count, out);
+  else slab_kernel<double><<<blocks, 256, 0, st>>>(g, static_cast<const double *>(a), face, i0, count, out);
+}
+
 // --------------------------------------------------------------- FP32 storage
 // rows of nref doubles (the reference's layout) <-> rows of pitch floats with
 // element e of a row at e + shift (the FP32 layout: shift 1 for ux, whose face

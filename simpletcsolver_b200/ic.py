@@ -132,8 +132,9 @@ def initial_fields(case: Case, xf=None, xc=None):
     return dict(ux=ux, uy=uy, uz=uz, p=p, t=t)
 
 
-def write_ic(case: Case, dest: str, step: int = 0, time: float = 0.0) -> str:
-    """Write an initial-condition directory that both solvers load."""
+def write_domain(case: Case, dest: str, step: int = 0, time: float = 0.0) -> str:
+    """The small files of an initial-condition directory (step, time and the
+    domain: src/main.c:46-52, src/domain.c:28-55), without the fields."""
     os.makedirs(dest, exist_ok=True)
     xf, xc = radial_grid(case)
     np.save(os.path.join(dest, "step.npy"), np.array(step, dtype=np.uint64))
@@ -143,6 +144,13 @@ def write_ic(case: Case, dest: str, step: int = 0, time: float = 0.0) -> str:
     np.save(os.path.join(dest, "lengths.npy"), np.array([case.lx, case.ly, case.lz], dtype=np.float64))
     np.save(os.path.join(dest, "xf.npy"), xf)
     np.save(os.path.join(dest, "xc.npy"), xc)
+    return dest
+
+
+def write_ic(case: Case, dest: str, step: int = 0, time: float = 0.0) -> str:
+    """Write an initial-condition directory that both solvers load."""
+    write_domain(case, dest, step, time)
+    xf, xc = radial_grid(case)
     for name, arr in initial_fields(case, xf, xc).items():
         np.save(os.path.join(dest, f"{name}.npy"), np.ascontiguousarray(arr, dtype=np.float64))
     return dest

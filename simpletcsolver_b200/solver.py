@@ -70,6 +70,32 @@ class Solver:
             lib.tcgpu_set_storage(previous)
         return s
 
+    @classmethod
+    def from_case(cls, case: Case, dirname: str, lib=None, coherence: int = 0, storage: int = 8) -> "Solver":
+        """The case's seeded initial field generated on the device
+        (tcgpu_fluid_init_generated); only the small domain files are written
+        to dirname (ic.write_domain), no field NPYs."""
+        from .ic import write_domain
+        lib = lib or abi.load()
+        os.environ.update(case_env(case))
+        lib.tcgpu_set_params(C.byref(params_of(case)))
+        write_domain(case, dirname)
+        domain = abi.DomainT()
+        fluid = abi.FluidT()
+        if lib.domain_init(dirname.encode(), C.byref(domain)) != 0:
+            raise SolverError(f"domain_init failed: {abi.last_error(lib)}")
+        s = cls(lib, domain, fluid)
+        previous = lib.tcgpu_get_storage(None)
+        s._check(lib.tcgpu_set_storage(storage), "set_storage")
+        try:
+            icp = abi.IcT(case.seed, case.noise_u, case.noise_t)
+            s._check(lib.tcgpu_fluid_init_generated(C.byref(domain), C.byref(fluid), C.byref(icp)),
+                     "fluid_init_generated")
+        finally:
+            lib.tcgpu_set_storage(previous)
+        s.set_coherence(coherence)
+        return s
+
     @property
     def storage(self) -> int:
         return self.lib.tcgpu_get_storage(C.byref(self.fluid))
@@ -155,6 +181,14 @@ class Solver:
         keys = ("divmax", "injection_u", "injection_t", "dissipation_u", "dissipation_t",
                 "energy_ux", "energy_uy", "energy_uz", "energy_t")
         return dict(zip(keys, list(out)))
+
+    def radial_slab(self, name: str, i0: int, count: int) -> np.ndarray:
+        """Device values of a field at radial indices i0 .. i0+count-1 over the
+        interior j, k: array [k, j, c]."""
+        out = np.zeros((self.nz, self.ny, count))
+        self._check(self.lib.tcgpu_radial_slab(C.byref(self.domain), C.byref(self.fluid), FIELD_BITS[name], i0, count,
+                                               out.ctypes.data_as(abi.c_double_p)), "radial_slab")
+        return out
 
     # ---------------------------------------------------------------- statistics (src/statistics.c)
     STAT_NAMES = ("ux1", "ux2", "uy1", "uy2", "uz1", "uz2", "adv", "dif")

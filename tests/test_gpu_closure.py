@@ -238,3 +238,35 @@ def test_trained_closure_beats_no_closure_on_held_out_pairs(lib, tmp_path):
     finally:
         for s in (fine, ca, cb):
             s.release()
+
+
+def test_wall_model_reproduces_the_injection_formula_and_learns(lib, tmp_path):
+    """The wall model's per-face injection (injection.c:55-73 with the wall
+    values of lyx.c and lxy.c) summed over the fine wall equals the fine
+    solver's own energy injection; a model fitted on restricted/fine pairs
+    predicts the fine first-cell velocity of held-out pairs better than the
+    coarse first-cell value itself, and the radial slab entry point returns
+    the device field's values."""
+    case = ic.taylor_couette(64, 128, 64, 3400.0)
+    _, cc, (fine, ca, cb) = _three_solvers(lib, tmp_path, case)
+    try:
+        fine.run(50)
+        # slab against the pulled field
+        fine.pull(abi.UY)
+        slab = fine.radial_slab("uy", 0, 3)
+        np.testing.assert_array_equal(slab, fine.field("uy")[1:-1, 1:-1, 0:3])
+        data, _ = closure.generate(fine, ca, cb, 16, 2, in_scale=(0.05, 1.0, 0.05))
+        train = [s for s in range(16) if s % 4]
+        held = [s for s in range(16) if s % 4 == 0]
+        wm = closure.WallModel.fit(data, train, fine, ca)
+        got = closure.WallModel.fine_injection(wm, fine.radial_slab("uy", 1, 1))
+        ref = fine.diagnostics()["injection_u"]
+        assert abs(got - ref) <= 1e-11 * abs(ref)
+        for q in held:
+            tgt = closure.block_mean(data.wall_y[q], ca).ravel()
+            err_model = np.sqrt(np.mean((wm.predict(data.wall_x[q]) - tgt) ** 2))
+            err_raw = np.sqrt(np.mean((data.wall_x[q][:, :, 0].ravel() - tgt) ** 2))
+            assert err_model < 0.5 * err_raw
+    finally:
+        for s in (fine, ca, cb):
+            s.release()
