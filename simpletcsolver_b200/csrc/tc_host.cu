@@ -151,7 +151,6 @@ static void destroy_ctx(Ctx * c) {
   delete c;
 }
 
-static bool is_pow2(size_t n) { return n >= 4 && (n & (n - 1)) == 0; }
 
 // metric accessors of the reference's domain_t (array_macros/domain/*.h)
 struct Metric {
@@ -535,8 +534,10 @@ static int check_domain(const domain_t * d) {
   }
   const size_t nx = d->glsizes[0], ny = d->glsizes[1], nz = d->glsizes[2];
   if (nx < 2 || nx > 256) return fail("nx = %zu outside the supported range [2, 256]", nx);
-  if (!is_pow2(ny) || !is_pow2(nz) || ny > 2048 || nz > 2048)
-    return fail("ny = %zu and nz = %zu must be powers of two in [4, 2048]", ny, nz);
+  // any even ny and any nz that is a multiple of 4 (powers of two take the
+  // FFT kernels, other lengths direct transforms)
+  if (ny < 4 || ny > 2048 || ny % 2 || nz < 4 || nz > 2048 || nz % 4)
+    return fail("ny = %zu must be even and nz = %zu a multiple of 4, both in [4, 2048]", ny, nz);
   if (!d->hxxf || !d->hxxc || !d->hyxf || !d->hyxc || !d->jdxf || !d->jdxc)
     return fail("domain metric arrays are not initialised");
   return 0;

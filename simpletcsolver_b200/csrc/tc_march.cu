@@ -874,17 +874,29 @@ static int march_planes(const Geo & g) {
     per_sm[dev] = b > 0 ? b : 1;
   }
   const long long slots = (long long)sms[dev] * per_sm[dev], lines = g.ny / JT;
+  // chunks divide nz: the largest divisor of nz up to TC_MARCH_KC, then
+  // smaller divisors down to 16 while the last wave is too empty (for a power
+  // of two nz: halving)
+  auto below = [&](int c) {   // the largest divisor of nz below c, or 0
+    for (int d = c - 1; d >= 1; d--)
+      if (g.nz % d == 0) return d;
+    return 0;
+  };
   int kc = g.nz < TC_MARCH_KC ? g.nz : TC_MARCH_KC;
-  for (; kc > 16; kc >>= 1) {
+  if (g.nz % kc) kc = below(kc);
+  for (;;) {
     const long long nblk = lines * (g.nz / kc), waves = (nblk + slots - 1) / slots;
     if (waves * slots * 100 <= nblk * 105) break;
+    const int next = below(kc);
+    if (kc <= 16 || next < 16) break;
+    kc = next;
   }
   return kc;
 }
 
 template <int NW, class T>
 void launch_march_nw(MarchArgs<T> A, const double * dtp, cudaStream_t st) {
-  constexpr int JT = TC_MARCH_JT;   // ny is a power of two >= 4
+  constexpr int JT = TC_MARCH_JT;   // ny is even
   using L = MarchLayout<NW, JT, T>;
   A.KC = march_planes<NW, T>(A.g);
   const long long nblk = (long long)(A.g.ny / JT) * (A.g.nz / A.KC);

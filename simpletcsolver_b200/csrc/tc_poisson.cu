@@ -902,7 +902,110 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   }
 }
 
+// --------------------------------------------------------------- direct DFTs
+// Lengths that are not powers of two (even ny, nz a multiple of 4, as FFTW
+// plans any length: compute_potential.c:247-309) take direct transforms: each
+// output wavenumber is the sum over the line with twiddles tw[(j m) mod N] =
+// exp(-2 pi i (j m mod N) / N) from the same tables. O(N^2) per line, FP64
+// accumulation, FFTW's conventions (unnormalised, r2c keeps N/2+1 terms, c2r
+// ignores the imaginary parts of the DC and Nyquist terms).
+
+// divergence (as div_ffty_kernel) of one (i, k) line into shared memory, then
+// its r2c transform along y
+template <class T, class Z>
+__global__ void div_dfty_kernel(Geo g, Coefs cf, Poisson ps, const T * __restrict__ ux, const T * __restrict__ uy,
+                                const T * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
+  extern __shared__ double line[];
+  const int ny = g.ny, nz = g.nz, nyh = ps.nyh;
+  const int i = blockIdx.x + 1, k = blockIdx.y + 1;
+  const double prefactor = 1. / (rk_gamma(rkstep) * (*dtp)) / (1. * ny * nz);
+  const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
+  const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i), ijd = __ldg(cf.c_invjdxc + i);
+  for (int j = threadIdx.x + 1; j <= ny; j += blockDim.x) {
+    const double div = ijd * (
+        -jxm * (double)ux[sidx_f<T>(g, i, j, k)] + jxp * (double)ux[sidx_f<T>(g, i + 1, j, k)]
+        - jy * (double)uy[sidx_c<T>(g, i, j, k)] + jy * (double)uy[sidx_c<T>(g, i, j + 1, k)]
+        - jz * (double)uz[sidx_c<T>(g, i, j, k)] + jz * (double)uz[sidx_c<T>(g, i, j, k + 1)]);
+    line[j - 1] = prefactor * div;
+  }
+  __syncthreads();
+  Z * out = static_cast<Z *>(ps.spec) + ((size_t)(i - 1) * nz + (k - 1)) * nyh;
+  for (int m = threadIdx.x; m < nyh; m += blockDim.x) {
+    double re = 0., im = 0.;
+    int q = 0;   // j m mod ny
+    for (int j = 0; j < ny; j++) {
+      const double2 w = ps.tw_y[q];
+      re += line[j] * w.x;
+      im += line[j] * w.y;
+      q += m;
+      if (q >= ny) q -= ny;
+    }
+    zput(out + m, make_double2(re, im));
+  }
+}
+
+// complex transform along z of the columns (i, ky), in place; SIGN -1 forward
+template <int SIGN, class Z>
+__global__ void dftz_kernel(Geo g, Poisson ps) {
+  extern __shared__ double2 col[];
+  const int nz = g.nz, nyh = ps.nyh;
+  const int ky = blockIdx.x, i = blockIdx.y + 1;
+  Z * base = static_cast<Z *>(ps.spec) + (size_t)(i - 1) * nz * nyh + ky;
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) col[k] = zget(base + (size_t)k * nyh);
+  __syncthreads();
+  for (int m = threadIdx.x; m < nz; m += blockDim.x) {
+    double re = 0., im = 0.;
+    int q = 0;   // k m mod nz
+    for (int k = 0; k < nz; k++) {
+      const double2 w = ps.tw_z[q];
+      const double wy = SIGN < 0 ? w.y : -w.y;
+      re += col[k].x * w.x - col[k].y * wy;
+      im += col[k].x * wy + col[k].y * w.x;
+      q += m;
+      if (q >= nz) q -= nz;
+    }
+    zput(base + (size_t)m * nyh, make_double2(re, im));
+  }
+}
+
+// c2r transform along y of one (i, k) line into psi with its Neumann x ghosts
+// and periodic images (as iffty_kernel)
+template <class Z>
+__global__ void idfty_kernel(Geo g, Poisson ps, double * __restrict__ psi) {
+  extern __shared__ double2 spec_line[];
+  const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh, half = ny / 2;
+  const int i = blockIdx.x + 1, k = blockIdx.y + 1;
+  const Z * in = static_cast<const Z *>(ps.spec) + ((size_t)(i - 1) * nz + (k - 1)) * nyh;
+  for (int m = threadIdx.x; m < nyh; m += blockDim.x) {
+    double2 x = zget(in + m);
+    if (m == 0 || m == half) x.y = 0.;
+    spec_line[m] = x;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < ny; j += blockDim.x) {
+    // X_0 + (-1)^j X_{N/2} + 2 Re sum_{0 < m < N/2} X_m exp(+2 pi i j m / N)
+    double acc = 0.;
+    int q = j;   // j m mod ny for m = 1
+    for (int m = 1; m < half; m++) {
+      const double2 w = ps.tw_y[q];     // exp(-2 pi i q / N): conjugated below
+      acc += spec_line[m].x * w.x + spec_line[m].y * w.y;
+      q += j;
+      if (q >= ny) q -= ny;
+    }
+    const double val = spec_line[0].x + ((j & 1) ? -spec_line[half].x : spec_line[half].x) + 2. * acc;
+    auto put = [&](int jj, int kk) {
+      psi[cidx(g, i, jj, kk)] = val;
+      if (i == 1) psi[cidx(g, 0, jj, kk)] = val;
+      if (i == nx) psi[cidx(g, nx + 1, jj, kk)] = val;
+    };
+    put(j + 1, k);
+    for_images(j + 1, k, ny, nz, put);
+  }
+}
+
 // --------------------------------------------------------------- launchers
+static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
 static int ilog2(int n) {
   int l = 0;
   while ((1 << l) < n) l++;
@@ -924,12 +1027,15 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
                              const double * tab_y, const double * tab_z, const double * base,
                              const double * dtp, int rkstep, cudaStream_t st, const PoissonMarks & pm) {
   auto mark = [&](int kk) { if (pm.mark) pm.mark(kk, 1); };
+  const bool fy = pow2(g.ny), fz = pow2(g.nz);   // FFTs; otherwise the direct transforms
   const int lgy = ilog2(g.ny), lgz = ilog2(g.nz);
   const int Py = lines_per_cta(g.ny, (g.nx + 1) / 2, EPTY, TC_FFTY_THREADS);
   const int tply = g.ny / EPTY;
   const size_t smy = sizeof(double2) * (size_t)Py * padded_len(g.ny);
   dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
-  div_ffty_kernel<EPTY, T, Z><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
+  const dim3 gl(g.nx, g.nz);   // one CTA per (i, k) line of the direct transforms in y
+  if (fy) div_ffty_kernel<EPTY, T, Z><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
+  else div_dfty_kernel<T, Z><<<gl, 128, sizeof(double) * g.ny, st>>>(g, cf, ps, f.ux, f.uy, f.uz, dtp, rkstep);
   mark(pm.k_div);
   const int Pz = lines_per_cta(g.nz, ps.nyh, EPTZ, TC_FFTZ_THREADS);
   const int tplz = g.nz / EPTZ;
@@ -939,16 +1045,20 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
 #else
   dim3 gz(g.nx, (ps.nyh + Pz - 1) / Pz);
 #endif
-  fftz_kernel<EPTZ, -1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  const dim3 gc(ps.nyh, g.nx);   // one CTA per (ky, i) column of the direct transforms in z
+  if (fz) fftz_kernel<EPTZ, -1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  else dftz_kernel<-1, Z><<<gc, 128, sizeof(double2) * g.nz, st>>>(g, ps);
   mark(pm.k_fwd);
   if (!launch_tdm_lines<Z>(g, ps, st)) {
     const long long nl = (long long)ps.nyh * g.nz;
     tdm_kernel<Z><<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, ps, tab_y, tab_z, base);
   }
   mark(pm.k_tdm);
-  fftz_kernel<EPTZ, +1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  if (fz) fftz_kernel<EPTZ, +1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
+  else dftz_kernel<+1, Z><<<gc, 128, sizeof(double2) * g.nz, st>>>(g, ps);
   mark(pm.k_inv);
-  iffty_kernel<EPTY, Z><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
+  if (fy) iffty_kernel<EPTY, Z><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
+  else idfty_kernel<Z><<<gl, 128, sizeof(double2) * ps.nyh, st>>>(g, ps, f.psi);
   mark(pm.k_ify);
 }
 

@@ -39,6 +39,10 @@ CASES = {
     # 8 radial indices has idle ones
     "tc_lines_y1024": ic.taylor_couette(12, 1024, 8, 3400.0),
     "tc_lines_y512": ic.taylor_couette(12, 512, 16, 3400.0),
+    # lengths that are not powers of two: direct transforms in y and z, plane
+    # chunks that divide nz (96 = 3 x 32 points in y, 48 and 36 in z)
+    "tc_y96_z48": ic.taylor_couette(16, 96, 48, 3400.0),
+    "planar_y48_z36": ic.plane_couette(12, 48, 36, 2000.0),
 }
 
 # Tolerance multipliers. With 512 and 1024 azimuthal points the spacing is

@@ -74,7 +74,9 @@ def test_oracle_tdm_bit_exact_with_reference(key):
 
 @pytest.mark.skipif(not have_ref("tc"), reason="reference build oracle/_ref absent")
 @pytest.mark.parametrize("build,nx,ny,nz", [("tc", 10, 16, 8), ("tc", 12, 64, 16), ("tcexp", 12, 16, 8),
-                                             ("planar", 10, 8, 16)])
+                                             ("planar", 10, 8, 16),
+                                             # lengths that are not powers of two (the shim's direct DFT)
+                                             ("tc", 10, 24, 12), ("planar", 10, 12, 20)])
 def test_oracle_matches_reference_fresh_case(build, nx, ny, nz, tmp_path):
     if build == "planar":
         case = ic.plane_couette(nx, ny, nz, 2000.0, seed=7)
