@@ -325,6 +325,13 @@ def kernel_table(kms_total, kdev, klaunch, ncell, bytes_map, peak):
     return per_kernel
 
 
+def gpu_config(nx, ny, nz, world):
+    """The workload's config, the same for both arms."""
+    return {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz], "Re": 1.0e4,
+            "coef_dt_adv": 0.4, "implicit": "x", "parallelism": f"replicas{world}",
+            "l2": "no flush: every field (1.09 GB at 256x1024x512) exceeds the 126 MB L2"}
+
+
 def gpu_arm(args, rank, world, local):
     import ctypes as C
     from simpletcsolver_b200 import abi, build, ic
@@ -421,9 +428,7 @@ def gpu_arm(args, rank, world, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": elapsed * 1e3 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field generated on the device (no dataset involved)",
-            "config": {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz], "Re": 1.0e4,
-                       "coef_dt_adv": case.coef_dt_adv, "implicit": "x", "parallelism": f"replicas{world}",
-                       "l2": "no flush: every field (1.09 GB at 256x1024x512) exceeds the 126 MB L2"},
+            "config": gpu_config(nx, ny, nz, world),
             "roofline": roofline,
             "step_model": {"bytes_per_cell_step": MODEL_BYTES_PER_CELL_STEP, "achieved_gbs": step_model,
                            "frac": step_model / peak},
@@ -716,11 +721,14 @@ def reference_arm(args, rank, world):
         return 0
     cpu = cpu_reference_run(args.steps, args.warmup)
     nx, ny, nz = parse_grid(args.grid)
+    # milliseconds per step of the whole workload at the measured throughput
+    ms_per_step = nx * ny * nz / (cpu["value"] * 1e6) * 1e3
     out = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic: seeded noisy circular-Couette field",
-           "config": {"workload": f"taylor-couette {nx}x{ny}x{nz} Re=1e4 fp64", "grid": [nx, ny, nz],
-                      "sample_grid": list(SAMPLE_GRID)},
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic: seeded noisy circular-Couette field",
+           "config": gpu_config(nx, ny, nz, world),
+           "sample": {"grid": list(SAMPLE_GRID), "note": cpu["sample"]},
            "cpu_baseline": cpu,
            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))

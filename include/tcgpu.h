@@ -217,7 +217,8 @@ typedef enum {
   TCGPU_K_PREDICT,       /* fused predict: right-hand sides, RK increment,
                             radial implicit solve, update, boundaries */
   TCGPU_K_APPLY,         /* update after the y / z solves (planar case) */
-  TCGPU_K_YZSOLVE,       /* periodic implicit solves in y and z */
+  TCGPU_K_YZSOLVE,       /* implicit line solves outside the predict: periodic y
+                            and z, and x when nx > 256 */
   TCGPU_K_DIV_FFTY,      /* divergence + forward y transform */
   TCGPU_K_FFTZ_FWD,      /* forward z transform */
   TCGPU_K_TDM,           /* radial Poisson solve per wavenumber pair */

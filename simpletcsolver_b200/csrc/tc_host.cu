@@ -533,7 +533,7 @@ static int check_domain(const domain_t * d) {
                   dim, d->mysizes[dim], d->glsizes[dim], d->offsets[dim]);
   }
   const size_t nx = d->glsizes[0], ny = d->glsizes[1], nz = d->glsizes[2];
-  if (nx < 2 || nx > 256) return fail("nx = %zu outside the supported range [2, 256]", nx);
+  if (nx < 2 || nx > 1024) return fail("nx = %zu outside the supported range [2, 1024]", nx);
   // any even ny and any nz that is a multiple of 4 (powers of two take the
   // FFT kernels, other lengths direct transforms)
   if (ny < 4 || ny > 2048 || ny % 2 || nz < 4 || nz > 2048 || nz % 4)
@@ -591,7 +591,9 @@ static Ctx * create_ctx(const domain_t * d, const fluid_t * fl) {
     if (!c->stage) return bad("cudaMalloc of the staging buffer failed");
   }
   const size_t nin = (size_t)c->nx * c->ny * c->nz;
-  const bool need_delta = c->bc.implicit[1] || c->bc.implicit[2];
+  // increments between the predict and separate line solves: implicit y or z,
+  // or radial lines longer than the predict kernel's 256 field threads
+  const bool need_delta = c->bc.implicit[1] || c->bc.implicit[2] || c->nx > 256;
   for (int v = 0; v < 4; v++) {
     const size_t n = (v == VUX) ? (size_t)(c->nx - 1) * c->ny * c->nz : nin;
     const size_t ns = f32 ? (size_t)spitch32(c->nx) * c->ny * c->nz : n;
@@ -689,17 +691,18 @@ static void enqueue_predict(Ctx & c, int rk) {
   }
   const FieldBufs in = c.fb[c.cur];
   const FieldBufs out = c.fb[c.cur ^ 1];
-  const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2];
+  const bool iy = c.bc.implicit[1], iz = c.bc.implicit[2], tiles = c.nx > 256;
   c.have_prev = true;
   auto predict = [&](int mode) {
     launch_predict_march(c.g, c.bc, c.cf, c.xf, c.nu, c.kappa, in, out, ss, c.ds, c.dtp, rk, mode, c.status, c.st);
   };
-  if (!iy && !iz) {
+  if (!iy && !iz && !tiles) {
     predict(PREDICT_APPLY);
     mark(TCGPU_K_PREDICT);
   } else {
     predict(PREDICT_DELTA);
     mark(TCGPU_K_PREDICT);
+    if (tiles && c.bc.implicit[0]) { launch_xsolve(c.g, c.xf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE); }
     if (iy) { launch_ysolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
     if (iz) { launch_zsolve(c.g, c.yf, rk, c.ds, c.st); mark(TCGPU_K_YZSOLVE, 4); }
     launch_apply(c.g, c.bc, in, out, c.ds, c.st);

@@ -40,7 +40,7 @@ struct FieldBufs {
 // All tables live in one allocation laid out [table][CSTRIDE] so that a
 // thread's coefficients are reached from one base pointer with compile-time
 // offsets (tab + table * CSTRIDE + i); nx + 2 <= CSTRIDE.
-constexpr int CSTRIDE = 264;
+constexpr int CSTRIDE = 1032;
 enum CoefTable {
   F_INVJD, F_A1, F_A2, F_A3, F_B1, F_B2, F_C1, F_C2, F_HD1, F_HD2, F_LXL, F_LXC, F_LXU, F_LYL, F_LYC, F_LYU,
   F_E1, F_E2, C_LYX1F, C_WM, C_WP, C_INVHXXF, C_INVHYXC, C_INVHYXF, C_LYY1, C_INVJDXC, C_A1, C_A2, C_B, C_CZ,
@@ -220,6 +220,9 @@ void launch_predict_march(const Geo & g, const Bc & bc, const Coefs & cf, const 
                           const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
                           cudaStream_t st);
 void march_smem_limits();
+// radial implicit solves of the delta buffers, lines of up to 1024 points
+// (after the predict's tile mode, nx > 256)
+void launch_xsolve(const Geo & g, const XFactors & xf, int rkstep, const DeltaSet & ds, cudaStream_t st);
 // one CTA whose mbarrier wait can never complete: sets ST_TIMEOUT in *status
 void launch_wait_selftest(unsigned * status, cudaStream_t st);
 void launch_xfactors(const XFactors & xf, const double * dtp, double nu, double kappa, cudaStream_t st);

@@ -482,26 +482,35 @@ __device__ __forceinline__ int slot_of(int kp, int k0, int nslot) { return (kp -
 __device__ __forceinline__ unsigned fill_parity(int kp, int k0, int nslot) { return ((kp - k0 + 1) / nslot) & 1u; }
 
 // The field warps: one thread per radial index i of the CTA's JT lines.
-template <int NW, int JT, int IMPL, class T>
+// TILE: radial lines longer than the field warps (nx > 32 NW). The CTA then
+// covers the radial indices ib + 1 .. ib + NRT of its lines (ib = tile x NRT),
+// its rows hold i = ib .. ib + NRT + 1 (ux faces ib .. ib + NRT + 1), the old
+// source terms are read from global memory, and the increments go to the
+// delta buffers before any radial solve (a separate line solve follows).
+template <int NW, int JT, int IMPL, class T, bool TILE = false>
 __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring, double * stage, T * olds,
                                              unsigned long long * bar, volatile int * abort_flag,
                                              int * release_cnt, volatile int * issued_p, int j0, int k0, int k1,
-                                             double dt) {
+                                             double dt, int ib = 0) {
   using L = MarchLayout<NW, JT, T>;
   constexpr int E = L::E, RL = L::RL, SL = L::SL, NS = L::NSLOT, OL = L::OL;
   const Geo & g = A.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int tx = threadIdx.x;
-  const int i = tx + 1;
+  const int i = ib + tx + 1;
   const bool act = i <= nx;
   unsigned long long * full = bar + NS;
   unsigned long long * done = bar + NS + 2;
   unsigned long long * obar = bar + NS + 4;
-  // element offsets of odd rows in their widened copies: ux / centre fields
-  // (none in the FP32 layout, whose rows start on 16-byte boundaries) and p
+  // element offsets in the widened copies of even and odd rows: ux (fe, of),
+  // centre fields (0, oc) and p (0, op); none in the FP32 layout, whose rows
+  // and tiles start on 16-byte boundaries. A tile's rows start at centre
+  // index ib (even) and ux face ib (element ib - 1).
   constexpr bool D64 = sizeof(T) == 8;
-  const int of = D64 ? (nx + 1) & 1 : 0, oc = D64 ? (nx + 2) & 1 : 0, op = (nx + 2) & 1;
-  constexpr int FSH = D64 ? 1 : 0;   // ux face i at element i - FSH of its row
+  const int e0f = (D64 && ib > 0) ? ib - 1 : ib;   // first ux element of the tile's rows
+  const int fe = D64 ? e0f & 1 : 0;
+  const int of = D64 ? ((nx + 1) & 1) ^ (e0f & 1) : 0, oc = D64 ? (nx + 2) & 1 : 0, op = (nx + 2) & 1;
+  const int fsh = (D64 && ib == 0) ? 1 : 0;   // ux face i at smem element i - ib - fsh of its row
   const size_t sjc = (size_t)ny + 2;
   auto frow = [&](char * slot, int f, int r) { return reinterpret_cast<T *>(slot) + (size_t)(f * (JT + 2) + r) * RL; };
   auto prow = [&](char * slot, int r) { return reinterpret_cast<double *>(slot + L::POFF) + (size_t)r * RL; };
@@ -517,9 +526,13 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
     auto all = [&](bool go, unsigned & total) {
       for (int f = 0; f < 5; f++) {
         const size_t es = f == SF_P ? sizeof(double) : sizeof(T), al = 16 / es;
-        const size_t n = (f == SF_P || (D64 && f != SF_UX)) ? (size_t)nx + 2 : D64 ? (size_t)nx + 1 : (size_t)pitch32(nx);
+        const size_t len = (f == SF_P || (D64 && f != SF_UX)) ? (size_t)nx + 2 : D64 ? (size_t)nx + 1 : (size_t)pitch32(nx);
+        // the part of the row the tile reads (the whole row without tiles)
+        const size_t e0 = f == SF_UX ? (size_t)e0f : (size_t)ib;
+        const size_t want = (f == SF_UX && D64) ? (size_t)L::NRT + 1 + (ib > 0 ? 1 : 0) : (size_t)L::NRT + 2;
+        const size_t n = TILE ? (len - e0 < want ? len - e0 : want) : len;
         for (int r = 0; r < (f == SF_P ? JT + 1 : JT + 2); r++) {
-          const size_t s0 = n * ((size_t)(j0 - 1 + r) + sjc * kp);
+          const size_t s0 = len * ((size_t)(j0 - 1 + r) + sjc * kp) + (TILE ? e0 : 0);
           const size_t a = s0 & ~(al - 1), b = (s0 + n + al - 1) & ~(al - 1);
           const unsigned by = (unsigned)((b - a) * es);
           const size_t off = (D64 || f != SF_P) ? (size_t)(f * (JT + 2) + r) * RL * sizeof(T)
@@ -562,7 +575,8 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
                (unsigned)((size_t)JT * li * sizeof(T)), &obar[buf]);
     }
   };
-  if (tx == 0 && use_old) {
+  const bool olds_smem = use_old && !TILE;   // tiles read the old terms from global memory
+  if (tx == 0 && olds_smem) {
     fetch_olds(k0, 0);
     if (k0 + 1 < k1) fetch_olds(k0 + 1, 1);
   }
@@ -647,12 +661,13 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
     store(k, x, u0);
   };
 
-  const bool solve_x = IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0;
+  // tiles leave the radial solve to the line kernel that follows
+  const bool solve_x = !TILE && (IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0);
   double up[JT][4];   // values of the previous plane's cells, until its solutions arrive
   for (int k = k0; k < k1; k++) {
     const int step = k - k0;
     wait(&bar[slot_of(k + 1, k0, NS)], fill_parity(k + 1, k0, NS));
-    if (use_old) wait(&obar[step & 1], (unsigned)(step >> 1) & 1u);
+    if (olds_smem) wait(&obar[step & 1], (unsigned)(step >> 1) & 1u);
     double dl[JT][4], u0[JT][4];   // indexed by Var
 #pragma unroll
     for (int jl = 0; jl < JT; jl++)
@@ -663,27 +678,28 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
       char * cs = ring + (size_t)slot_of(k, k0, NS) * L::SLOT;
       char * ns = ring + (size_t)slot_of(k + 1, k0, NS) * L::SLOT;
       SlotView<T> V;
-      V.cb = reinterpret_cast<const T *>(cs) + i;
+      const int is = i - ib;   // the cell's element in the tile's rows
+      V.cb = reinterpret_cast<const T *>(cs) + is;
       V.cbo = V.cb + oc;
-      V.fb = V.cb - FSH;
-      V.fbo = V.fb + of;
-      V.nb = reinterpret_cast<const T *>(ns) + i;
+      V.fb = V.cb - fsh + fe;
+      V.fbo = V.cb - fsh + of;
+      V.nb = reinterpret_cast<const T *>(ns) + is;
       V.nbo = V.nb + oc;
-      V.nf = V.nb - FSH;
-      V.nfo = V.nf + of;
-      V.mb = reinterpret_cast<const T *>(ms) + i;
+      V.nf = V.nb - fsh + fe;
+      V.nfo = V.nb - fsh + of;
+      V.mb = reinterpret_cast<const T *>(ms) + is;
       V.mbo = V.mb + oc;
-      V.mf = V.mb - FSH;
-      V.mfo = V.mf + of;
+      V.mf = V.mb - fsh + fe;
+      V.mfo = V.mb - fsh + of;
       if constexpr (D64) {   // p rows follow the field rows: same base registers, constant offsets
         V.pb = reinterpret_cast<const double *>(V.cb) + L::NFROW * RL;
         V.pbo = reinterpret_cast<const double *>(V.cbo) + L::NFROW * RL;
         V.mp = reinterpret_cast<const double *>(V.mb) + L::NFROW * RL;
         V.mpo = reinterpret_cast<const double *>(V.mbo) + L::NFROW * RL;
       } else {
-        V.pb = prow(cs, 0) + i;
+        V.pb = prow(cs, 0) + is;
         V.pbo = V.pb + op;
-        V.mp = prow(ms, 0) + i;
+        V.mp = prow(ms, 0) + is;
         V.mpo = V.mp + op;
       }
       const size_t qf = pidx(lf, ny, i - 2, j0, k), qc = pidx(lc, ny, i - 1, j0, k);
@@ -692,7 +708,14 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
         constexpr int JL = decltype(jlc)::value;
         double d2[2], w2[2];
         auto old = [&](int v) {
-          return use_old ? (double)ob[(size_t)v * JT * OL + JL * (v == VUX ? lf : lc) + (v == VUX ? i - 2 : i - 1)] : 0.;
+          if (!use_old) return 0.;
+          if constexpr (TILE) {   // from global memory (ux at i = 1 has none)
+            if (v == VUX && i < 2) return 0.;
+            const int li = v == VUX ? lf : lc;
+            return (double)A.ss.old_[v][pidx(li, ny, v == VUX ? i - 2 : i - 1, j0 + JL, k)];
+          } else {
+            return (double)ob[(size_t)v * JT * OL + JL * (v == VUX ? lf : lc) + (v == VUX ? i - 2 : i - 1)];
+          }
         };
         // old(VUX) at i = 1 reads the shared-memory word before the line (discarded)
         cell_a<JT, RL, JL, IMPL>(qa, qb, V, A.bc, A.cf, A.nu, A.kappa, rpr, i, qf + (size_t)JL * lf,
@@ -721,7 +744,7 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
             issue(k + 3, slot_of(k + 3, k0, NS));
             *issued_p = k + 3;
           }
-          if (use_old && k + 2 < k1) fetch_olds(k + 2, step & 1);
+          if (olds_smem && k + 2 < k1) fetch_olds(k + 2, step & 1);
         }
       }
     }
@@ -753,7 +776,7 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
     const int issued = *issued_p;
     for (int kp = (issued - NS + 1 > k0 - 1 ? issued - NS + 1 : k0 - 1); kp <= issued; kp++)
       mbar_wait(&bar[slot_of(kp, k0, NS)], fill_parity(kp, k0, NS));
-    if (use_old) {
+    if (olds_smem) {
       for (int kp = k1 - 2 > k0 ? k1 - 2 : k0; kp < k1; kp++)
         mbar_wait(&obar[(kp - k0) & 1], (unsigned)((kp - k0) >> 1) & 1u);
     }
@@ -791,7 +814,7 @@ __device__ __forceinline__ void regs_dec() { asm volatile("setmaxnreg.dec.sync.a
 
 // CTA = JT lines (j0 .. j0+JT-1) x KC planes; field warps and the solve
 // warpgroup as above.
-template <int NW, int JT, int IMPL, class T>
+template <int NW, int JT, int IMPL, class T, bool TILE = false>
 __global__ void __launch_bounds__(MarchLayout<NW, JT, T>::THREADS, 1)
 march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
   using L = MarchLayout<NW, JT, T>;
@@ -805,8 +828,11 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
   int * release_cnt = const_cast<int *>(abort_flag + 2);
   const int tx = threadIdx.x;
   const int njg = A.g.ny / JT;
-  const int j0 = (int)(blockIdx.x % njg) * JT + 1;   // odd
-  const int k0 = (int)(blockIdx.x / njg) * A.KC + 1;
+  const int ntile = TILE ? (A.g.nx + L::NRT - 1) / L::NRT : 1;
+  const int tile = TILE ? (int)(blockIdx.x % ntile) : 0;
+  const unsigned bl = TILE ? blockIdx.x / ntile : blockIdx.x;
+  const int j0 = (int)(bl % njg) * JT + 1;   // odd
+  const int k0 = (int)(bl / njg) * A.KC + 1;
   const int k1 = k0 + A.KC;   // planes k0 .. k1-1 are computed; k0-1 .. k1 are read
   if (tx == 0) {
     for (int s = 0; s < L::NSLOT; s++) mbar_init(&bar[s], 1);
@@ -826,10 +852,11 @@ march_predict_kernel(MarchArgs<T> A, const double * __restrict__ dtp) {
   const double dt = *dtp;
   if (tx < L::NRT) {
     if constexpr (L::REGS > 0) regs_inc<L::REGS_FIELD>();
-    march_fields<NW, JT, IMPL, T>(A, ring, stage, olds, bar, abort_flag, release_cnt, issued_p, j0, k0, k1, dt);
+    march_fields<NW, JT, IMPL, T, TILE>(A, ring, stage, olds, bar, abort_flag, release_cnt, issued_p, j0, k0, k1,
+                                        dt, tile * L::NRT);
   } else {
     if constexpr (L::REGS > 0) regs_dec<L::REGS_SOLVE>();
-    const bool solve_x = IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0;
+    const bool solve_x = !TILE && (IMPL >= 0 ? (IMPL & 1) != 0 : A.bc.implicit[0] != 0);
     if (solve_x) march_solves<NW, JT, T>(A, stage, bar, abort_flag, A.KC);
   }
   __syncthreads();
@@ -927,6 +954,57 @@ void allow_march_smem() {
   cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if constexpr (sizeof(T) == 8)
     cudaFuncSetAttribute(march_predict_kernel<NW, JT, -2, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if constexpr (NW == 8) {
+    cudaFuncSetAttribute(march_predict_kernel<NW, JT, -1, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if constexpr (sizeof(T) == 8)
+      cudaFuncSetAttribute(march_predict_kernel<NW, JT, -2, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes);
+  }
+}
+
+// radial lines longer than one CTA's field threads: tiles of 256 radial
+// indices, increments to the delta buffers (the radial solve is launched
+// separately), implicit flags and the closure forcing read at run time
+template <class T>
+void launch_march_tiles(MarchArgs<T> A, const double * dtp, cudaStream_t st) {
+  constexpr int NW = 8, JT = TC_MARCH_JT;
+  using L = MarchLayout<NW, JT, T>;
+  A.KC = march_planes<NW, T>(A.g);
+  A.mode = PREDICT_DELTA;
+  const int ntile = (A.g.nx + L::NRT - 1) / L::NRT;
+  const long long nblk = (long long)ntile * (A.g.ny / JT) * (A.g.nz / A.KC);
+  if constexpr (sizeof(T) == 8) {
+    if (A.ss.frc[0]) {
+      march_predict_kernel<NW, JT, -2, T, true><<<(unsigned)nblk, L::THREADS, L::BYTES, st>>>(A, dtp);
+      return;
+    }
+  }
+  march_predict_kernel<NW, JT, -1, T, true><<<(unsigned)nblk, L::THREADS, L::BYTES, st>>>(A, dtp);
+}
+
+// Radial implicit solves of lines longer than one CTA's field threads (the
+// tile mode above leaves its increments unsolved): one warp per (variable,
+// j, k) line of the delta buffers, staged in shared memory, with the factor
+// rows and scans of the march kernel (solve_line).
+template <int E>
+__global__ void __launch_bounds__(256) xsolve_kernel(Geo g, XFactors xf, int rk, DeltaSet ds) {
+  extern __shared__ double xs_stage[];
+  constexpr int SL = 32 * E + 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long lines = (long long)g.ny * g.nz;
+  const long long q = (long long)blockIdx.x * 8 + w;   // (variable, line)
+  if (q >= 4 * lines) return;                          // whole warps
+  const int v = (int)(q / lines);
+  const long long line = q % lines;
+  const int n = xf.n[v];
+  double * sb = xs_stage + (size_t)w * SL;
+  double * d = ds.d[v] + (size_t)line * n;   // packed layout: line (j, k) holds n values
+  for (int e = lane; e < 32 * E; e += 32) sb[spad<E>(e)] = e < n ? d[e] : 0.;
+  __syncwarp();
+  const size_t fo = (size_t)(rk * 4 + v) * xf.stride;
+  solve_line<E>(sb, xf.lo + fo, xf.w + fo, xf.v + fo, lane);
+  __syncwarp();
+  for (int e = lane; e < n; e += 32) d[e] = sb[spad<E>(e)];
 }
 
 template <class T>
@@ -935,6 +1013,10 @@ void launch_march_t(const Geo & g, const Bc & bc, const Coefs & cf, const XFacto
                     const DeltaSet & ds, const double * dtp, int rkstep, int mode, unsigned * status,
                     cudaStream_t st) {
   MarchArgs<T> A{g, bc, cf, xf, nu, kappa, in.as<T>(), out.as<T>(), ss.as<T>(), ds, rkstep, mode, 0, status};
+  if (g.nx > MarchLayout<8, TC_MARCH_JT, T>::NRT) {
+    launch_march_tiles<T>(A, dtp, st);
+    return;
+  }
   switch (predict_warps(g.nx)) {
     case 1: launch_march_nw<1>(A, dtp, st); break;
     case 2: launch_march_nw<2>(A, dtp, st); break;
@@ -971,7 +1053,15 @@ __global__ void wait_selftest_kernel(unsigned * status) {
 
 void launch_wait_selftest(unsigned * status, cudaStream_t st) { wait_selftest_kernel<<<1, 64, 0, st>>>(status); }
 
+void launch_xsolve(const Geo & g, const XFactors & xf, int rkstep, const DeltaSet & ds, cudaStream_t st) {
+  const long long lines = 4LL * g.ny * g.nz;
+  const unsigned blocks = (unsigned)((lines + 7) / 8);
+  if (xf.ne <= 16) xsolve_kernel<16><<<blocks, 256, 8 * (32 * 16 + 32) * sizeof(double), st>>>(g, xf, rkstep, ds);
+  else xsolve_kernel<32><<<blocks, 256, 8 * (32 * 32 + 32) * sizeof(double), st>>>(g, xf, rkstep, ds);
+}
+
 void march_smem_limits() {
+  cudaFuncSetAttribute(xsolve_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * (32 * 32 + 32) * 8);
   allow_march_smem<1, double>();
   allow_march_smem<2, double>();
   allow_march_smem<4, double>();

@@ -57,14 +57,16 @@ def test_push_pull_round_trip_is_fp32_rounding(lib, tmp_path):
         s.release()
 
 
-@pytest.mark.parametrize("name", ["tc", "tcexp", "planar"])
+@pytest.mark.parametrize("name", ["tc", "tcexp", "planar", "tc_radial320"])
 def test_short_runs_track_fp64(lib, name, tmp_path):
-    """Five steps of each boundary/implicitness family: velocity and scalar
+    """Five steps of each boundary/implicitness family (and of a radial line
+    longer than the predict kernel's 256 field threads): velocity and scalar
     within 1e-5 relative L2 of the FP64 path, p within 1e-4, the same time
     steps to 1e-5 and divergence at the FP32 storage floor (below 1e-4)."""
     case = {"tc": ic.taylor_couette(32, 32, 16, 3400.0),
             "tcexp": ic.taylor_couette(20, 16, 8, 3400.0, implicit=(False, False, False)),
-            "planar": ic.plane_couette(24, 16, 16, 2000.0)}[name]
+            "planar": ic.plane_couette(24, 16, 16, 2000.0),
+            "tc_radial320": ic.taylor_couette(320, 16, 8, 1.0e4)}[name]
     d0 = ic.write_ic(case, str(tmp_path / "ic"))
     a = _run(lib, d0, case, 8, 5)
     b = _run(lib, d0, case, 4, 5)

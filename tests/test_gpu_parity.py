@@ -42,6 +42,11 @@ CASES = {
     # lengths that are not powers of two: direct transforms in y and z, plane
     # chunks that divide nz (96 = 3 x 32 points in y, 48 and 36 in z)
     "tc_y96_z48": ic.taylor_couette(16, 96, 48, 3400.0),
+    # radial lines longer than the predict kernel's 256 field threads: tiles of
+    # 256 radial indices, then the line solves (x; and y, z in the planar case)
+    "tc_radial384": ic.taylor_couette(384, 16, 8, 1.0e4),
+    "tc_radial512": ic.taylor_couette(512, 16, 8, 1.0e4),
+    "planar_radial320": ic.plane_couette(320, 16, 8, 2000.0),
     "planar_y48_z36": ic.plane_couette(12, 48, 36, 2000.0),
 }
 
