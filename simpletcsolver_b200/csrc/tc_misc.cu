@@ -706,7 +706,7 @@ __global__ void initial_field_kernel(Geo g, FieldsT<T> f, const double * __restr
   f.uy[sidx_c<T>(g, i, j, k)] = (T)(uy_prof[i] + noise(seed, 1, q, amp_u));
   f.uz[sidx_c<T>(g, i, j, k)] = (T)noise(seed, 2, q, amp_u);
   f.t[sidx_c<T>(g, i, j, k)] = (T)(t_prof[i] + (amp_t > 0. ? noise(seed, 3, q, amp_t) : 0.));
-  f.p[sidx_c<T>(g, i, j, k)] = 0.;
+  f.p[sidx_c<double>(g, i, j, k)] = 0.;   // p is FP64 in the reference layout in every storage mode
   if (i >= 1) f.ux[sidx_f<T>(g, i, j, k)] = (T)((i == 1 || i == nx + 1) ? 0. : noise(seed, 0, q, amp_u));
 }
 

@@ -822,23 +822,31 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   const int LS = padded_len(ny);
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
-  // Hermitian extension of the two packed real lines
+  // Hermitian extension of the two packed real lines: each stored wavenumber
+  // mr < ny/2 is loaded once and gives the line's values at m = mr and
+  // m = ny - mr; the Nyquist terms follow (imaginary parts of DC and Nyquist
+  // ignored, as FFTW's c2r does)
+  const int half = ny >> 1;
+  const Z * sp = static_cast<const Z *>(ps.spec);
 #pragma unroll kIfftyUnroll
-  for (int r = 0; r < EPT; r++) {
-    const int idx = threadIdx.x + r * blockDim.x;
-    const int m = idx & (ny - 1);
-    const int pp = idx >> lg;
+  for (int r = 0; r < EPT / 2; r++) {     // P half = blockDim EPT / 2 items
+    const int u = threadIdx.x + r * blockDim.x;
+    const int mr = u & (half - 1);
+    const int pp = u >> (lg - 1);
     const int ia = i0 + 2 * pp, ib = ia + 1;
-    const int mr = (m <= ny / 2) ? m : ny - m;
     double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
-    const Z * sp = static_cast<const Z *>(ps.spec);
     if (ia <= nx) xa = zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr);
     if (ib <= nx) xb = zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr);
-    if (mr == 0 || 2 * mr == ny) { xa.y = 0.; xb.y = 0.; }
-    double2 z;
-    if (m <= ny / 2) z = make_double2(xa.x - xb.y, xa.y + xb.x);
-    else z = make_double2(xa.x + xb.y, -xa.y + xb.x);
-    smem[(size_t)pp * LS + pad(m)] = z;
+    if (mr == 0) { xa.y = 0.; xb.y = 0.; }
+    double2 * line = smem + (size_t)pp * LS;
+    line[pad(mr)] = make_double2(xa.x - xb.y, xa.y + xb.x);
+    if (mr != 0) line[pad(ny - mr)] = make_double2(xa.x + xb.y, -xa.y + xb.x);
+  }
+  for (int pp = threadIdx.x; pp < P; pp += blockDim.x) {
+    const int ia = i0 + 2 * pp, ib = ia + 1;
+    const double xa = ia <= nx ? zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + half).x : 0.;
+    const double xb = ib <= nx ? zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + half).x : 0.;
+    smem[(size_t)pp * LS + pad(half)] = make_double2(xa, xb);
   }
   __syncthreads();
   {

@@ -92,9 +92,13 @@ def test_reference_main_runs_on_the_library(lib, reference_run, tmp_path):
             x = np.load(os.path.join(cpu, "save", d, n + ".npy"))
             y = np.load(os.path.join(gpu, "save", d, n + ".npy"))
             assert rel_l2(y, x) < 1e-10, (d, n)
-        for n in ("step", "time", "glsizes", "xf", "xc"):
+        for n in ("step", "glsizes", "xf", "xc"):
             np.testing.assert_array_equal(np.load(os.path.join(cpu, "save", d, n + ".npy")),
                                           np.load(os.path.join(gpu, "save", d, n + ".npy")), err_msg=n)
+        # dt is the minimum of h / |u| over fields equal to round-off, so the
+        # summed time may differ in its last bits
+        assert float(np.load(os.path.join(gpu, "save", d, "time.npy"))) == pytest.approx(
+            float(np.load(os.path.join(cpu, "save", d, "time.npy"))), rel=1e-13)
     # statistics collected by the reference's statistics.c from the library's host arrays
     sc, sg = latest(cpu, "stat"), latest(gpu, "stat")
     assert os.path.basename(sc) == os.path.basename(sg)

@@ -72,6 +72,25 @@ def test_generated_field_follows_its_definition(lib, tmp_path, curved):
         s.release()
 
 
+def test_generated_field_in_fp32_storage(lib, tmp_path):
+    """The same field with 4-byte storage: one FP32 rounding of the FP64 field
+    (p stays FP64 and zero)."""
+    case = ic.taylor_couette(24, 32, 16, 3400.0, seed=11)
+    a = Solver.from_case(case, str(tmp_path / "a"), lib=lib)
+    b = Solver.from_case(case, str(tmp_path / "b"), lib=lib, storage=4)
+    try:
+        assert b.storage == 4
+        fa, fb = fields(a), fields(b)
+        for n in ("ux", "uy", "uz", "t"):
+            np.testing.assert_array_equal(fb[n], fa[n].astype(np.float32).astype(np.float64), err_msg=n)
+        assert not fb["p"].any()
+        b.integrate()
+        assert b.diagnostics()["divmax"] < 1e-4
+    finally:
+        a.release()
+        b.release()
+
+
 def test_generated_field_at_the_headline_grid(lib, tmp_path):
     """256x1024x512 without any field file: generated, stepped resident, and
     divergence-free to round-off after the first step."""
