@@ -9,7 +9,7 @@ network (autograd gives the reference gradients).
 Conventions shared with the CUDA side: activations [k][j][i][c] over the
 interior cells of the coarse grid; weights w[t][co][ci] with
 t = 9 (dz+1) + 3 (dy+1) + (dx+1); convolution = cross-correlation, zero padding
-in x (radial), periodic in y and z; GELU in its erf form.
+in x (radial), periodic in y and z; GELU in its tanh form.
 """
 from __future__ import annotations
 
@@ -73,15 +73,15 @@ def conv(x, w, b=None):
 
 
 def network(x, params):
-    """params: [(w, b)] of the four layers (torch tensors); GELU after the
-    first three."""
+    """params: [(w, b)] of the four layers (torch tensors); GELU (tanh form)
+    after the first three."""
     import torch
     F = torch.nn.functional
     h = x
     for li, (w, b) in enumerate(params):
         h = conv(h, w, b)
         if li < len(params) - 1:
-            h = F.gelu(h)
+            h = F.gelu(h, approximate="tanh")
     return h
 
 

@@ -139,38 +139,89 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
 }
 
-// GELU, erf form: 0.5 z (1 + erf(z / sqrt 2)), and its derivative
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float (&v)[8]) {
+  unsigned r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 8; q++) v[q] = __uint_as_float(r[q]);
+}
+template <int N>
+__device__ __forceinline__ void tmem_ld(unsigned taddr, float (&v)[N]) {
+  static_assert(N == 8 || N == 16, "8 or 16 columns");
+  if constexpr (N == 16) tmem_ld16(taddr, v);
+  else tmem_ld8(taddr, v);
 }
 
+// GELU in its tanh form (Hendrycks and Gimpel 2016),
+//   gelu(z) = 0.5 z (1 + tanh(u)), u = sqrt(2/pi) (z + 0.044715 z^3),
+// with the hardware tanh approximation (tanh.approx.f32, about 2^-11
+// relative), and its derivative
+//   0.5 (1 + t) + 0.5 z (1 - t^2) sqrt(2/pi) (1 + 3 0.044715 z^2), t = tanh(u).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+constexpr float kGeluS = 0.79788456080286536f, kGeluC = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+  const float t = tanh_hw(kGeluS * z * fmaf(kGeluC * z, z, 1.f));
+  const float h = 0.5f * z;
+  return fmaf(h, t, h);
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float z2 = z * z;
+  const float t = tanh_hw(kGeluS * z * fmaf(kGeluC, z2, 1.f));
+  return fmaf(0.5f, 1.f + t, 0.5f * z * (1.f - t * t) * kGeluS * fmaf(3.f * kGeluC, z2, 1.f));
+}
 
 // ---- convolution: forward and input gradient ------------------------------
 constexpr int TX = 8, TY = 16;             // output tile: 8 x, 16 y, one z plane (M = 128)
 constexpr int HX = TX + 2, HY = TY + 2;    // halo of one plane
-constexpr int NN_THREADS = 128;            // 4 warps: one TMEM lane quarter each
-constexpr int NSLOT_NN = 4;                // halo planes z-1, z, z+1 and the one streaming in
+constexpr int NN_THREADS = 128;            // weight gradient: 4 warps, one TMEM lane quarter each
+constexpr int NEPI = 8;                    // epilogue warps: two per TMEM lane quarter
+constexpr int NLD = 2;                     // halo loader warps
+constexpr int CONV_THREADS = 32 * (NEPI + 1 + NLD);   // + the MMA warp and the loaders
 
 enum ConvEpilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
 
+// The three z taps are stacked along N: one MMA multiplies the halo of input
+// plane p, shifted by (dy, dx), with the weights of taps dz = -1, 0, +1 side
+// by side (N = 3 COUT) and adds into the accumulators of output planes p + 1,
+// p and p - 1, which sit side by side in tensor memory. Output plane number g
+// of the CTA (counted over all its work items) owns accumulator columns
+// [c(g) COUT, (c(g) + 1) COUT) with c(g) = S - 1 - g mod S: the planes
+// p + 1, p, p - 1 are at consecutive c except where c wraps from S - 1 to 0,
+// where the MMA is split in two. Accumulators start at zero and are zeroed
+// again by the epilogue that drains them, so every MMA accumulates.
 template <int CIN, int COUT>
 struct ConvLayout {
   static_assert(CIN == 16 || CIN == 32, "input channels: 16 or 32");
   static_assert(COUT == 16 || COUT == 32, "output channels: 16 or 32");
+  static constexpr int CC = CIN / 8;                     // 16-byte channel chunks per cell
   static constexpr int CHB = HX * 16;                    // bytes between channel chunks of a halo row
-  static constexpr int ROWB = (CIN / 8) * CHB;           // bytes between halo rows (y)
+  static constexpr int ROWB = CC * CHB;                  // bytes between halo rows (y)
   static constexpr int SLOTB = HY * ROWB;                // one halo plane
   static constexpr int WB = 27 * CIN * COUT * 2;         // packed BF16 weights
+  static constexpr int WSH = 3 * COUT * 16;              // bytes per (dy, dx, channel chunk): 3 COUT rows of 8
   static constexpr int HALO = WB;                        // halo slots after the weights
-  static constexpr int BAR = HALO + NSLOT_NN * SLOTB;    // two mbarriers, then the TMEM address
-  static constexpr int BYTES = BAR + 32;
+  static constexpr int NSL = 5;                          // halo planes in the ring
+  static constexpr int LAG = NSL - 2;                    // planes a loader thread keeps in flight
+  static constexpr int S = 8;                            // output-plane accumulators in tensor memory
+  static constexpr int TCOLS = S * COUT;
+  static constexpr int BAR = HALO + NSL * SLOTB;         // mbarriers, TMEM address, abort flag
+  static constexpr int NBAR = 2 * NSL + 2 * S + 1;
+  static constexpr int BYTES = BAR + NBAR * 8 + 16;
+  static_assert(TCOLS == 128 || TCOLS == 256, "tensor-memory allocation: a power of two");
 };
 
 struct ConvArgs {
-  int nx, ny, nz, zc;             // coarse interior, z planes per CTA
+  int nx, ny, nz, zc;             // coarse interior, z planes per work item
+  int nitems;                     // work items: (column tile, z chunk), tile fastest
   const __nv_bfloat16 * in;       // [cell][CIN]
-  const __nv_bfloat16 * w;        // packed [27][CIN/8][COUT][8]
+  const __nv_bfloat16 * w;        // packed [dy+1][dx+1][CIN/8][3 COUT][8], rows (dz+1) COUT + co
   const float * bias;             // [COUT] (forward epilogues)
   const __nv_bfloat16 * zsave;    // [cell][COUT] pre-activations (EPI_DGELU)
   __nv_bfloat16 * out;            // [cell][COUT] (EPI_GELU, EPI_DGELU)
@@ -182,13 +233,18 @@ struct ConvArgs {
 
 __device__ __forceinline__ int wrapi(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
-// 16-byte units of one halo plane (global plane kp) into a slot: coalesced
-// over the channel chunks of consecutive cells, written to [y][chunk][x]
+__device__ __forceinline__ void nn_arrive(unsigned long long * bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(bar)) : "memory");
+}
+// The loader threads' share (thread lt of 32 NLD) of one halo plane (global
+// plane kp) into a slot: 16-byte units, coalesced over the channel chunks of
+// consecutive cells, written to [y][chunk][x]; cells outside 0 <= x < nx are
+// zero-filled (the walls), y wraps around.
 template <int CIN>
-__device__ __forceinline__ void load_halo(char * slot, const __nv_bfloat16 * in, int nx, int ny, int x0, int y0,
-                                          int kp) {
+__device__ __forceinline__ void load_halo_part(char * slot, const __nv_bfloat16 * in, int nx, int ny, int x0, int y0,
+                                               int kp, int lt) {
   constexpr int CC = CIN / 8;
-  for (int u = threadIdx.x; u < HY * HX * CC; u += NN_THREADS) {
+  for (int u = lt; u < HY * HX * CC; u += 32 * NLD) {
     const int cc = u % CC, xh = (u / CC) % HX, yh = u / (CC * HX);
     const int i = x0 - 1 + xh, j = wrapi(y0 - 1 + yh, ny);
     const bool valid = i >= 0 && i < nx;
@@ -196,163 +252,274 @@ __device__ __forceinline__ void load_halo(char * slot, const __nv_bfloat16 * in,
     cp16(slot + ((yh * CC + cc) * HX + xh) * 16, src, valid);
   }
 }
-
-// Two-stage pipeline over the planes of the chunk: the MMAs of plane z (into
-// accumulator z & 1) run while the warps drain the accumulator of plane z - 1
-// and the halo of plane z + 2 streams in (into the slot of plane z - 2, free
-// once the MMAs of z - 1 completed).
-#ifndef TC_CONV_NPART
-#define TC_CONV_NPART 1
-#endif
-// partial accumulators per plane: the taps alternate between them, so
-// consecutive MMAs do not accumulate into the same tensor-memory columns
-constexpr int NPART = TC_CONV_NPART;
-
-template <int CIN, int COUT, int EPI>
-__device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tacc, int warp, size_t cell) {
-#pragma unroll
-  for (int h = 0; h < COUT / 16; h++) {
-    float v[16];
-    tmem_ld16(tacc + ((unsigned)(warp * 32) << 16) + h * 16, v);
-#pragma unroll
-    for (int pp = 1; pp < NPART; pp++) {
-      float w2[16];
-      tmem_ld16(tacc + ((unsigned)(warp * 32) << 16) + pp * 32 + h * 16, w2);
-#pragma unroll
-      for (int q = 0; q < 16; q++) v[q] += w2[q];
-    }
-    if constexpr (EPI == EPI_LINEAR) {
-#pragma unroll
-      for (int q = 0; q < 16; q++)
-        if (h * 16 + q < A.nout) A.outf[cell * A.nout + h * 16 + q] = v[q] + A.bias[h * 16 + q];
-    } else {
-      alignas(16) __nv_bfloat16 o[16];
-      if constexpr (EPI == EPI_GELU) {
-        alignas(16) __nv_bfloat16 zp[16];
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-          const float zv = v[q] + A.bias[h * 16 + q];
-          zp[q] = __float2bfloat16_rn(zv);
-          o[q] = __float2bfloat16_rn(gelu(zv));
-        }
-        if (A.pre) {
-          uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + h * 16);
-          dp[0] = reinterpret_cast<const uint4 *>(zp)[0];
-          dp[1] = reinterpret_cast<const uint4 *>(zp)[1];
-        }
-      } else {
-        alignas(16) __nv_bfloat16 zs[16];
-        const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + h * 16);
-        reinterpret_cast<uint4 *>(zs)[0] = sp[0];
-        reinterpret_cast<uint4 *>(zs)[1] = sp[1];
-#pragma unroll
-        for (int q = 0; q < 16; q++) o[q] = __float2bfloat16_rn(v[q] * gelu_grad(__bfloat162float(zs[q])));
-      }
-      uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + h * 16);
-      op[0] = reinterpret_cast<const uint4 *>(o)[0];
-      op[1] = reinterpret_cast<const uint4 *>(o)[1];
+// zeros into 32 lanes x N consecutive columns (one lane per thread of the warp)
+template <int N>
+__device__ __forceinline__ void tmem_zero(unsigned taddr) {
+  static_assert(N == 8 || N == 16, "8 or 16 columns");
+  const unsigned z = 0u;
+  if constexpr (N == 16)
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+        "%1};" ::"r"(taddr), "r"(z)
+        : "memory");
+  else
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr), "r"(z)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// bounded wait that also gives up once another role of the CTA has given up
+__device__ __forceinline__ bool conv_wait(unsigned long long * bar, unsigned parity, volatile int * abort_flag) {
+  if (nn_mbar_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!nn_mbar_try(bar, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kNnWaitCycles) {
+      *abort_flag = 1;
+      return false;
     }
   }
+  return true;
 }
 
+// work item k of the CTA: its column tile and z range
+struct ConvItem { int x0, y0, z0, z1; };
+__device__ __forceinline__ ConvItem conv_item(const ConvArgs & A, int item) {
+  const int nbx = A.nx / TX, ntile = nbx * (A.ny / TY);
+  const int tile = item % ntile, zch = item / ntile;
+  ConvItem c;
+  c.x0 = (tile % nbx) * TX;
+  c.y0 = (tile / nbx) * TY;
+  c.z0 = zch * A.zc;
+  c.z1 = min(c.z0 + A.zc, A.nz);
+  return c;
+}
+
+// Accumulator rows = TMEM lanes: warp w drains lane quarter w % 4, warps w and
+// w + 4 the lower and upper half of the columns (bias values bv of those
+// columns), and zeroes what it read; the zeros land while it computes.
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(NN_THREADS) conv3_kernel(ConvArgs A) {
+__device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tacc, int warp, size_t cell,
+                                              unsigned long long * empty, int lane, const float (&bv)[COUT / 2]) {
+  constexpr int CW = COUT / 2;
+  const int c0 = (warp >> 2) * CW;
+  const unsigned ta = tacc + ((unsigned)((warp & 3) * 32) << 16) + c0;
+  float v[CW];
+  tmem_ld<CW>(ta, v);
+  tmem_zero<CW>(ta);
+  if constexpr (EPI == EPI_LINEAR) {
+#pragma unroll
+    for (int q = 0; q < CW; q++)
+      if (c0 + q < A.nout) A.outf[cell * A.nout + c0 + q] = v[q] + bv[q];
+  } else {
+    alignas(16) __nv_bfloat162 o[CW / 2];
+    if constexpr (EPI == EPI_GELU) {
+      alignas(16) __nv_bfloat162 zp[CW / 2];
+#pragma unroll
+      for (int q = 0; q < CW; q += 2) {
+        const float za = v[q] + bv[q], zb = v[q + 1] + bv[q + 1];
+        zp[q / 2] = __floats2bfloat162_rn(za, zb);
+        o[q / 2] = __floats2bfloat162_rn(gelu(za), gelu(zb));
+      }
+      if (A.pre) {
+        uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + c0);
+#pragma unroll
+        for (int u = 0; u < CW / 8; u++) dp[u] = reinterpret_cast<const uint4 *>(zp)[u];
+      }
+    } else {
+      alignas(16) __nv_bfloat162 zs[CW / 2];
+      const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + c0);
+#pragma unroll
+      for (int u = 0; u < CW / 8; u++) reinterpret_cast<uint4 *>(zs)[u] = sp[u];
+#pragma unroll
+      for (int q = 0; q < CW; q += 2) {
+        const float2 zf = __bfloat1622float2(zs[q / 2]);
+        o[q / 2] = __floats2bfloat162_rn(v[q] * gelu_grad(zf.x), v[q + 1] * gelu_grad(zf.y));
+      }
+    }
+    uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + c0);
+#pragma unroll
+    for (int u = 0; u < CW / 8; u++) op[u] = reinterpret_cast<const uint4 *>(o)[u];
+  }
+  // the accumulator may be written again once every warp has read and zeroed its part
+  tmem_wait_st();
+  tc_fence_before();
+  __syncwarp();
+  if (lane == 0) nn_arrive(empty);
+}
+
+// Persistent CTAs over work items k = blockIdx.x, blockIdx.x + gridDim.x, ...
+// Loader warps (NLD): the input planes of the items, in order, into a ring of
+// NSL slots (16-byte asynchronous copies; each thread arrives on full once its
+// copies of a plane landed). MMA warp (warp NEPI, one thread): per input plane
+// the MMAs of its 9 shifts into the accumulators of the output planes it
+// feeds; tcgen05.commit then releases the slot (slot_free) and, when an output
+// plane got its last contribution, hands it to the epilogue (acc_full). Before
+// an output plane's first contribution its accumulator must have been drained
+// and zeroed (acc_empty). Epilogue warps 0 .. NEPI-1: per output plane, wait
+// acc_full, read and zero the accumulator, release it, apply the epilogue and
+// store. Every wait is bounded; a CTA whose wait gave up stops issuing and
+// storing, waits (bounded) for the copies and MMAs it started, and reports
+// ST_TIMEOUT.
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
   using L = ConvLayout<CIN, COUT>;
+  constexpr int NS = L::NSL, S = L::S;
   extern __shared__ __align__(128) char smc[];
   char * wsm = smc;
   char * halo = smc + L::HALO;
-  unsigned long long * bar = reinterpret_cast<unsigned long long *>(smc + L::BAR);   // two
-  unsigned * tslot = reinterpret_cast<unsigned *>(smc + L::BAR + 16);
+  unsigned long long * full = reinterpret_cast<unsigned long long *>(smc + L::BAR);
+  unsigned long long * sfree = full + NS;
+  unsigned long long * accf = sfree + NS;
+  unsigned long long * acce = accf + S;
+  unsigned long long * fin = acce + S;
+  unsigned * tslot = reinterpret_cast<unsigned *>(fin + 1);
+  volatile int * abort_flag = reinterpret_cast<volatile int *>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nbx = A.nx / TX;
-  const int x0 = (blockIdx.x % nbx) * TX, y0 = (blockIdx.x / nbx) * TY;
-  const int z0 = blockIdx.y * A.zc, z1 = min(z0 + A.zc, A.nz);
-
-  // two planes x NPART accumulators of 32 columns, rounded up to the power of
-  // two an allocation takes
-  constexpr unsigned TCOLS = 64 * NPART <= 64 ? 64 : 64 * NPART <= 128 ? 128 : 256;
-  static_assert(NPART >= 1 && NPART <= 4, "1 to 4 partial accumulators");
-  if (warp == 0) tmem_alloc(tslot, TCOLS);
+  if (warp == NEPI) tmem_alloc(tslot, L::TCOLS);
   if (tid == 0) {
-    nn_mbar_init(&bar[0], 1);
-    nn_mbar_init(&bar[1], 1);
+    for (int s = 0; s < NS; s++) {
+      nn_mbar_init(&full[s], 32 * NLD);
+      nn_mbar_init(&sfree[s], 1);
+    }
+    for (int a = 0; a < S; a++) {
+      nn_mbar_init(&accf[a], 1);
+      nn_mbar_init(&acce[a], NEPI);
+    }
+    nn_mbar_init(fin, 1);
+    *abort_flag = 0;
     fence_barrier_init();
   }
-  // weights (exact shared-memory image) and the first three halo planes
-  for (int u = tid; u < L::WB / 16; u += NN_THREADS) cp16(wsm + u * 16, reinterpret_cast<const char *>(A.w) + u * 16, true);
-  load_halo<CIN>(halo + 0 * L::SLOTB, A.in, A.nx, A.ny, x0, y0, wrapi(z0 - 1, A.nz));
+  // weights: the exact shared-memory image, read by the tensor cores
+  for (int u = tid; u < L::WB / 16; u += CONV_THREADS) cp16(wsm + u * 16, reinterpret_cast<const char *>(A.w) + u * 16, true);
   cp_commit();
-  load_halo<CIN>(halo + 1 * L::SLOTB, A.in, A.nx, A.ny, x0, y0, z0);
-  cp_commit();
-  load_halo<CIN>(halo + 2 * L::SLOTB, A.in, A.nx, A.ny, x0, y0, wrapi(z0 + 1, A.nz));
-  cp_commit();
+  cp_wait<0>();
+  fence_proxy_async();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tslot;
-  constexpr uint32_t IDESC = instr_desc_bf16(128, COUT, 0, 0);
-  const int m = warp * 32 + lane;                // accumulator row = TMEM lane of this thread
-  const int xi = x0 + (m & 7), yj = y0 + (m >> 3);
-  unsigned phase[2] = {0u, 0u};
-  bool bad = false;
-
-  for (int z = z0, it = 0; z <= z1 && !bad; z++, it++) {
-    const int r = z - z0 + 1;                    // plane z in slot r % 4
-    if (z < z1) {
-      // planes up to z + 1 have landed (plane z + 1 was the last group issued)
-      cp_wait<0>();
-      fence_proxy_async();                       // make them visible to the tensor cores
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        const unsigned hb = su32(halo), wb = su32(wsm);
-        const unsigned dacc = tmem + (it & 1) * 32 * NPART;
-        // slot base of each of the three planes, then every tap's descriptors
-        // from compile-time offsets
-        const unsigned sb[3] = {hb + ((r - 1) % NSLOT_NN) * L::SLOTB, hb + (r % NSLOT_NN) * L::SLOTB,
-                                hb + ((r + 1) % NSLOT_NN) * L::SLOTB};
-#pragma unroll
-        for (int t = 0; t < 27; t++) {
-          const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-          const unsigned a0 = sb[dz + 1] + (1 + dy) * L::ROWB + (1 + dx) * 16;
-          const int pp = t % NPART;
-#pragma unroll
-          for (int kk = 0; kk < CIN / 16; kk++) {
-            const uint64_t ad = smem_desc(a0 + kk * 2 * L::CHB, L::CHB, L::ROWB);
-            const uint64_t bd = smem_desc(wb + (t * (CIN / 8) + 2 * kk) * COUT * 16, COUT * 16, 128);
-            mma_bf16(dacc + pp * 32, ad, bd, IDESC, t >= NPART || kk > 0);
-          }
-        }
-        mma_commit(&bar[it & 1]);
-      }
-    }
-    if (it > 0) {
-      // plane z - 1: its MMAs done, so the slot of plane z - 2 is free for z + 2
-      const int pb = (it - 1) & 1;
-      const bool ok = nn_mbar_wait(&bar[pb], phase[pb]);
-      phase[pb] ^= 1u;
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) atomicOr(A.status, ST_TIMEOUT);
-        bad = true;
-        break;
-      }
-      tc_fence_after();
-    }
-    if (z < z1 && z + 2 <= z1)
-      load_halo<CIN>(halo + ((r + 2) % NSLOT_NN) * L::SLOTB, A.in, A.nx, A.ny, x0, y0, wrapi(z + 2, A.nz));
-    cp_commit();
-    if (it > 0) {
-      const size_t cell = ((size_t)(z - 1) * A.ny + yj) * A.nx + xi;
-      conv_epilogue<CIN, COUT, EPI>(A, tmem + ((it - 1) & 1) * 32 * NPART, warp, cell);
-    }
-    tc_fence_before();
-    __syncthreads();                             // the drained accumulator may be written again
+  constexpr int CW = COUT / 2;
+  if (warp < NEPI) {   // every accumulator starts at zero
+    const unsigned tl = tmem + ((unsigned)((warp & 3) * 32) << 16) + (warp >> 2) * CW;
+    for (int c = 0; c < S; c++) tmem_zero<CW>(tl + c * COUT);
+    tmem_wait_st();
   }
-  cp_wait<0>();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_free(tmem, TCOLS);
+
+  auto colslot = [&](int g) { return S - 1 - (g % S); };
+  if (warp == NEPI) {
+    if (lane == 0) {
+      // K-major weights: channel chunks (K) at WSH, groups of 8 rows (N) at 128 bytes
+      const uint64_t bdesc0 = smem_desc(su32(wsm), L::WSH, 128);
+      const unsigned hb = su32(halo);
+      bool ok = true;
+      int hc = 0, gb = 0;   // input planes consumed; output planes of the items before this one
+      for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
+        const ConvItem it = conv_item(A, k);
+        for (int p = it.z0 - 1; p <= it.z1 && ok; p++, hc++) {
+          ok = conv_wait(&full[hc % NS], (unsigned)(hc / NS) & 1u, abort_flag);
+          // first contribution to output plane p + 1: its accumulator drained
+          const int gn = gb + (p + 1 - it.z0);
+          if (ok && p + 1 < it.z1 && gn >= S) ok = conv_wait(&acce[gn % S], (unsigned)(gn / S - 1) & 1u, abort_flag);
+          if (!ok) break;
+          tc_fence_after();
+          // outputs ohi .. olo (descending, so ascending accumulator columns),
+          // taps dz = p - o; at most two runs of consecutive columns
+          const int ohi = min(p + 1, it.z1 - 1), olo = max(p - 1, it.z0);
+          const uint64_t adesc = smem_desc(hb + (unsigned)((hc % NS) * L::SLOTB), L::CHB, L::ROWB);
+          int o = ohi;
+          while (o >= olo) {
+            const int c = colslot(gb + (o - it.z0));
+            int n = 1;   // run length: columns c .. c + n - 1
+            while (o - n >= olo && c + n < S) n++;
+            const unsigned d = tmem + (unsigned)(c * COUT);
+            const uint32_t idesc = n == 1 ? instr_desc_bf16(128, COUT, 0, 0)
+                                 : n == 2 ? instr_desc_bf16(128, 2 * COUT, 0, 0)
+                                          : instr_desc_bf16(128, 3 * COUT, 0, 0);
+            const uint64_t bd0 = bdesc0 + (uint64_t)(((p - o + 1) * COUT * 16) >> 4);   // rows of tap dz = p - o
+#pragma unroll
+            for (int sh = 0; sh < 9; sh++) {
+              const int dy = sh / 3, dx = sh % 3;   // offsets + 1
+#pragma unroll
+              for (int kk = 0; kk < CIN / 16; kk++) {
+                // start addresses advance in 16-byte units in the low bits of the descriptors
+                const uint64_t a = adesc + (uint64_t)((dy * L::ROWB + dx * 16 + kk * 2 * L::CHB) >> 4);
+                const uint64_t b = bd0 + (uint64_t)(((sh * L::CC + 2 * kk) * L::WSH) >> 4);
+                mma_bf16(d, a, b, idesc, true);
+              }
+            }
+            o -= n;
+          }
+          mma_commit(&sfree[hc % NS]);
+          if (p - 1 >= it.z0) mma_commit(&accf[(gb + p - 1 - it.z0) % S]);   // output plane p - 1 complete
+        }
+        gb += it.z1 - it.z0;
+      }
+      if (!ok) atomicOr(A.status, ST_TIMEOUT);
+      // drain: the MMAs issued and the arrivals of their last slot releases
+      mma_commit(fin);
+      nn_mbar_wait(fin, 0);
+      for (int h = hc - 1; h >= 0 && h >= hc - NS; h--) nn_mbar_wait(&sfree[h % NS], (unsigned)(h / NS) & 1u);
+    }
+    __syncwarp();
+  } else if (warp > NEPI) {
+    // loaders: plane h into slot h % NS once the MMAs of plane h - NS are done;
+    // plane h - LAG is announced (each thread: its copies landed, made visible
+    // to the tensor cores, one arrival) after plane h's copies were issued, so
+    // LAG + 1 planes of copies are in flight
+    constexpr int LAG = L::LAG;
+    const int lt = tid - 32 * (NEPI + 1);
+    int h = 0;
+    bool ok = true;
+    for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
+      const ConvItem it = conv_item(A, k);
+      for (int p = it.z0 - 1; p <= it.z1; p++, h++) {
+        if (h >= NS && !conv_wait(&sfree[h % NS], (unsigned)((h - NS) / NS) & 1u, abort_flag)) {
+          ok = false;
+          break;
+        }
+        load_halo_part<CIN>(halo + (h % NS) * L::SLOTB, A.in, A.nx, A.ny, it.x0, it.y0, wrapi(p, A.nz), lt);
+        cp_commit();
+        if (h >= LAG) {
+          cp_wait<LAG>();
+          fence_proxy_async();
+          nn_arrive(&full[(h - LAG) % NS]);
+        }
+      }
+    }
+    cp_wait<0>();
+    fence_proxy_async();
+    if (ok)
+      for (int q = h - LAG < 0 ? 0 : h - LAG; q < h; q++) nn_arrive(&full[q % NS]);
+    if (!ok && lane == 0) atomicOr(A.status, ST_TIMEOUT);
+  } else {
+    const int m = (warp & 3) * 32 + lane;   // accumulator row = TMEM lane of this thread
+    float bv[CW];
+#pragma unroll
+    for (int q = 0; q < CW; q++) bv[q] = (EPI != EPI_DGELU) ? A.bias[(warp >> 2) * CW + q] : 0.f;
+    int g = 0;
+    bool ok = true;
+    for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
+      const ConvItem it = conv_item(A, k);
+      const int xi = it.x0 + (m & 7), yj = it.y0 + (m >> 3);
+      for (int z = it.z0; z < it.z1; z++, g++) {
+        if (!conv_wait(&accf[g % S], (unsigned)(g / S) & 1u, abort_flag)) {
+          if (lane == 0) atomicOr(A.status, ST_TIMEOUT);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const size_t cell = ((size_t)z * A.ny + yj) * A.nx + xi;
+        conv_epilogue<CIN, COUT, EPI>(A, tmem + (unsigned)(colslot(g) * COUT), warp, cell, &acce[g % S], lane, bv);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == NEPI) tmem_free(tmem, L::TCOLS);
 }
 
 // ---- convolution: weight gradient -----------------------------------------
@@ -635,29 +802,98 @@ __global__ void adam_kernel(float * __restrict__ p, const float * __restrict__ g
 // ---- weights ---------------------------------------------------------------
 // Master weights (FP32) w[t][co][ci], t = 9 (dz+1) + 3 (dy+1) + (dx+1), real
 // channel counts cin x cout, into the BF16 shared-memory images of the forward
-// convolution, [t][ci/8][co][ci%8] over padded counts CINP x COUTP, and of the
+// convolution, [dy+1][dx+1][ci/8][(dz+1) COUTP + co][ci%8] over padded counts
+// CINP x COUTP (the three z taps of a shift side by side along N), and of the
 // input-gradient convolution (taps mirrored, channels swapped),
-// [26-t][co/8][ci][co%8] over COUTP x CINP. Padding channels are zero.
+// [1-dy][1-dx][co/8][(1-dz) CINP + ci][co%8]. Padding channels are zero.
 __global__ void pack_weights_kernel(const float * __restrict__ w, int cin, int cout, int cinp, int coutp,
                                     __nv_bfloat16 * __restrict__ fwd, __nv_bfloat16 * __restrict__ bwd) {
   const int n = 27 * cinp * coutp;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const int ci = q % cinp, co = (q / cinp) % coutp, t = q / (cinp * coutp);
+    const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;   // offsets + 1
     const float v = (ci < cin && co < cout) ? w[((size_t)t * cout + co) * cin + ci] : 0.f;
     const __nv_bfloat16 b = __float2bfloat16_rn(v);
-    fwd[((size_t)(t * (cinp / 8) + ci / 8) * coutp + co) * 8 + ci % 8] = b;
-    if (bwd) bwd[((size_t)((26 - t) * (coutp / 8) + co / 8) * cinp + ci) * 8 + co % 8] = b;
+    fwd[((size_t)((dy * 3 + dx) * (cinp / 8) + ci / 8) * 3 * coutp + dz * coutp + co) * 8 + ci % 8] = b;
+    if (bwd)
+      bwd[((size_t)(((2 - dy) * 3 + (2 - dx)) * (coutp / 8) + co / 8) * 3 * cinp + (2 - dz) * cinp + ci) * 8 + co % 8] =
+          b;
   }
 }
 
+// SMs of the current device
+static int device_sms() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  return n;
+}
+
+// CTAs of a kernel that fit on one SM: registers (allocated per warp in units
+// of 256), shared memory (plus the per-block reservation), threads, and at
+// most 512 tensor-memory columns, so that no allocation has to wait
+static int conv_ctas_per_sm(const void * kern, int threads, int smem, int tcols) {
+  int dev = 0, regs_sm = 0, smem_sm = 0, resv = 0, thr_sm = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaFuncGetAttributes(&fa, kern) != cudaSuccess ||
+      cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+    return 0;
+  const int warps = (threads + 31) / 32;
+  const int regs_cta = warps * ((fa.numRegs * 32 + 255) / 256 * 256);
+  int n = 512 / tcols;
+  if (regs_cta > 0 && regs_sm / regs_cta < n) n = regs_sm / regs_cta;
+  if (smem_sm / (smem + resv) < n) n = smem_sm / (smem + resv);
+  if (thr_sm / (32 * warps) < n) n = thr_sm / (32 * warps);
+  return n;
+}
+
+// z planes per work item. Work items go round-robin to the g = per_sm x nsm
+// persistent CTAs; CTAs b and b + nsm share an SM, and CTA b gets
+// items / g items, one more when b < items mod g. The chunk minimises the
+// input planes (z planes + 2 per item) of the busiest SM.
+static int conv_chunk(int ntile, int nz, int nsm, int per_sm) {
+  const long g = (long)nsm * per_sm;
+  long best = -1;
+  int zc = nz;
+  for (int c = 1; c <= nz; c++) {
+    const long items = (long)ntile * ((nz + c - 1) / c);
+    long load = 0;
+    for (int j = 0; j < per_sm; j++) {
+      const long b = (long)j * nsm;
+      load += items / g + (b < items % g ? 1 : 0);
+    }
+    load *= c + 2;
+    if (best < 0 || load < best) { best = load; zc = c; }
+  }
+  return zc;
+}
+
 template <int CIN, int COUT, int EPI>
-int launch_conv3(const ConvArgs & a, cudaStream_t st) {
+int launch_conv3(ConvArgs a, cudaStream_t st) {
   using L = ConvLayout<CIN, COUT>;
-  if (cudaFuncSetAttribute(conv3_kernel<CIN, COUT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES) !=
-      cudaSuccess)
-    return 1;
-  const dim3 grid((a.nx / TX) * (a.ny / TY), (a.nz + a.zc - 1) / a.zc);
-  conv3_kernel<CIN, COUT, EPI><<<grid, NN_THREADS, L::BYTES, st>>>(a);
+  auto kern = conv3_kernel<CIN, COUT, EPI>;
+  // once per instantiation: the whole unified L1 as shared memory, so that two
+  // CTAs fit per SM, and the resident CTAs per SM from the kernel's registers,
+  // shared memory and tensor-memory columns (the occupancy query reports one
+  // CTA here, which leaves half of every SM idle)
+  static const int per_sm = [&] {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES) != cudaSuccess ||
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+            cudaSuccess)
+      return 0;
+    return conv_ctas_per_sm(reinterpret_cast<const void *>(kern), CONV_THREADS, L::BYTES, L::TCOLS);
+  }();
+  if (per_sm < 1) return 1;
+  const int ntile = (a.nx / TX) * (a.ny / TY), nsm = device_sms();
+  const int g = per_sm * nsm;
+  if (g < 1) return 1;
+  a.zc = conv_chunk(ntile, a.nz, nsm, per_sm);
+  a.nitems = ntile * ((a.nz + a.zc - 1) / a.zc);
+  const int grid = a.nitems < g ? a.nitems : g;
+  kern<<<grid, CONV_THREADS, L::BYTES, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -677,15 +913,6 @@ void wgrad_split(int nx, int ny, int nz, int & zc, int & nitems, int & nblk) {
   while (zc > 4 && (long)ncol * ((nz + zc - 1) / zc) < 148L * 2) zc = (zc + 1) / 2;
   nitems = ncol * ((nz + zc - 1) / zc);
   nblk = nitems < 148 ? nitems : 148;
-}
-
-// z planes per CTA: about four CTAs' worth of work per SM pair
-int conv_zchunk(int nx, int ny, int nz) {
-  const long cols = (long)(nx / TX) * (ny / TY);
-  long zc = cols * nz / (148L * 8);
-  if (zc < 1) zc = 1;
-  if (zc > nz) zc = nz;
-  return (int)zc;
 }
 
 }  // namespace
@@ -849,7 +1076,7 @@ int tcgpu_nn_conv3(int mode, int cin, int cout, int nx, int ny, int nz, const vo
     return nn_fail("nn_conv3: nx must be a multiple of 8 and ny of 16");
   if (!in || !wpacked || !aligned16(in) || !aligned16(wpacked)) return nn_fail("nn_conv3: inputs not 16-byte aligned");
   ConvArgs a{};
-  a.nx = nx; a.ny = ny; a.nz = nz; a.zc = conv_zchunk(nx, ny, nz);
+  a.nx = nx; a.ny = ny; a.nz = nz;
   a.in = static_cast<const __nv_bfloat16 *>(in);
   a.w = static_cast<const __nv_bfloat16 *>(wpacked);
   a.bias = bias;
