@@ -139,22 +139,6 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
 }
 
-__device__ __forceinline__ void tmem_ld8(unsigned taddr, float (&v)[8]) {
-  unsigned r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int q = 0; q < 8; q++) v[q] = __uint_as_float(r[q]);
-}
-template <int N>
-__device__ __forceinline__ void tmem_ld(unsigned taddr, float (&v)[N]) {
-  static_assert(N == 8 || N == 16, "8 or 16 columns");
-  if constexpr (N == 16) tmem_ld16(taddr, v);
-  else tmem_ld8(taddr, v);
-}
-
 // GELU in its tanh form (Hendrycks and Gimpel 2016),
 //   gelu(z) = 0.5 z (1 + tanh(u)), u = sqrt(2/pi) (z + 0.044715 z^3),
 // with the hardware tanh approximation (tanh.approx.f32, about 2^-11
@@ -191,10 +175,12 @@ enum ConvEpilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
 // plane p, shifted by (dy, dx), with the weights of taps dz = -1, 0, +1 side
 // by side (N = 3 COUT) and adds into the accumulators of output planes p + 1,
 // p and p - 1, which sit side by side in tensor memory. Output plane number g
-// of the CTA (counted over all its work items) owns accumulator columns
-// [c(g) COUT, (c(g) + 1) COUT) with c(g) = S - 1 - g mod S: the planes
-// p + 1, p, p - 1 are at consecutive c except where c wraps from S - 1 to 0,
-// where the MMA is split in two. Accumulators start at zero and are zeroed
+// of the CTA (counted over all its segments) owns the accumulator at column
+// block c(g) = S - 1 - g mod S of a ring of S blocks of COUT columns; the
+// window of step p starts at c(g(p + 1)) and runs on into two overflow blocks
+// S and S + 1 past the ring instead of wrapping, so every step is one MMA per
+// shift. A plane whose block is 0 or 1 therefore also collects in block S or
+// S + 1, which the epilogue adds. Accumulators start at zero and are zeroed
 // again by the epilogue that drains them, so every MMA accumulates.
 template <int CIN, int COUT>
 struct ConvLayout {
@@ -208,18 +194,18 @@ struct ConvLayout {
   static constexpr int WSH = 3 * COUT * 16;              // bytes per (dy, dx, channel chunk): 3 COUT rows of 8
   static constexpr int HALO = WB;                        // halo slots after the weights
   static constexpr int NSL = 5;                          // halo planes in the ring
-  static constexpr int LAG = NSL - 2;                    // planes a loader thread keeps in flight
-  static constexpr int S = 8;                            // output-plane accumulators in tensor memory
-  static constexpr int TCOLS = S * COUT;
+  static constexpr int LAG = 2;                          // planes between a plane's copies and its announcement
+  static constexpr int S = 6;                            // output-plane accumulators in the ring
+  static constexpr int TCOLS = (S + 2) * COUT;           // + two overflow blocks
   static constexpr int BAR = HALO + NSL * SLOTB;         // mbarriers, TMEM address, abort flag
   static constexpr int NBAR = 2 * NSL + 2 * S + 1;
-  static constexpr int BYTES = BAR + NBAR * 8 + 16;
+  static constexpr int BIAS = BAR + NBAR * 8 + 16;       // COUT floats
+  static constexpr int BYTES = BIAS + COUT * 4;
   static_assert(TCOLS == 128 || TCOLS == 256, "tensor-memory allocation: a power of two");
 };
 
 struct ConvArgs {
-  int nx, ny, nz, zc;             // coarse interior, z planes per work item
-  int nitems;                     // work items: (column tile, z chunk), tile fastest
+  int nx, ny, nz;                 // coarse interior
   const __nv_bfloat16 * in;       // [cell][CIN]
   const __nv_bfloat16 * w;        // packed [dy+1][dx+1][CIN/8][3 COUT][8], rows (dz+1) COUT + co
   const float * bias;             // [COUT] (forward epilogues)
@@ -281,75 +267,102 @@ __device__ __forceinline__ bool conv_wait(unsigned long long * bar, unsigned par
   return true;
 }
 
-// work item k of the CTA: its column tile and z range
-struct ConvItem { int x0, y0, z0, z1; };
-__device__ __forceinline__ ConvItem conv_item(const ConvArgs & A, int item) {
-  const int nbx = A.nx / TX, ntile = nbx * (A.ny / TY);
-  const int tile = item % ntile, zch = item / ntile;
-  ConvItem c;
-  c.x0 = (tile % nbx) * TX;
-  c.y0 = (tile / nbx) * TY;
-  c.z0 = zch * A.zc;
-  c.z1 = min(c.z0 + A.zc, A.nz);
-  return c;
-}
-
-// Accumulator rows = TMEM lanes: warp w drains lane quarter w % 4, warps w and
-// w + 4 the lower and upper half of the columns (bias values bv of those
-// columns), and zeroes what it read; the zeros land while it computes.
-template <int CIN, int COUT, int EPI>
-__device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tacc, int warp, size_t cell,
-                                              unsigned long long * empty, int lane, const float (&bv)[COUT / 2]) {
-  constexpr int CW = COUT / 2;
-  const int c0 = (warp >> 2) * CW;
-  const unsigned ta = tacc + ((unsigned)((warp & 3) * 32) << 16) + c0;
-  float v[CW];
-  tmem_ld<CW>(ta, v);
-  tmem_zero<CW>(ta);
-  if constexpr (EPI == EPI_LINEAR) {
-#pragma unroll
-    for (int q = 0; q < CW; q++)
-      if (c0 + q < A.nout) A.outf[cell * A.nout + c0 + q] = v[q] + bv[q];
-  } else {
-    alignas(16) __nv_bfloat162 o[CW / 2];
-    if constexpr (EPI == EPI_GELU) {
-      alignas(16) __nv_bfloat162 zp[CW / 2];
-#pragma unroll
-      for (int q = 0; q < CW; q += 2) {
-        const float za = v[q] + bv[q], zb = v[q + 1] + bv[q + 1];
-        zp[q / 2] = __floats2bfloat162_rn(za, zb);
-        o[q / 2] = __floats2bfloat162_rn(gelu(za), gelu(zb));
-      }
-      if (A.pre) {
-        uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + c0);
-#pragma unroll
-        for (int u = 0; u < CW / 8; u++) dp[u] = reinterpret_cast<const uint4 *>(zp)[u];
-      }
-    } else {
-      alignas(16) __nv_bfloat162 zs[CW / 2];
-      const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + c0);
-#pragma unroll
-      for (int u = 0; u < CW / 8; u++) reinterpret_cast<uint4 *>(zs)[u] = sp[u];
-#pragma unroll
-      for (int q = 0; q < CW; q += 2) {
-        const float2 zf = __bfloat1622float2(zs[q / 2]);
-        o[q / 2] = __floats2bfloat162_rn(v[q] * gelu_grad(zf.x), v[q + 1] * gelu_grad(zf.y));
-      }
-    }
-    uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + c0);
-#pragma unroll
-    for (int u = 0; u < CW / 8; u++) op[u] = reinterpret_cast<const uint4 *>(o)[u];
+// The CTA's output planes: q0 <= q < q1 in the order q = tile nz + z (the
+// 128-cell column tiles, x fastest), an equal share of all of them, walked as
+// segments of one tile each (a z range that the CTA marches through).
+struct ConvSeg { int x0, y0, z0, z1; };
+struct ConvCursor {
+  long long q, q1;
+  __device__ __forceinline__ ConvCursor(const ConvArgs & A) {
+    const long long total = (long long)(A.nx / TX) * (A.ny / TY) * A.nz;
+    q = total * blockIdx.x / gridDim.x;
+    q1 = total * (blockIdx.x + 1) / gridDim.x;
   }
-  // the accumulator may be written again once every warp has read and zeroed its part
+  __device__ __forceinline__ bool next(const ConvArgs & A, ConvSeg & s) {
+    if (q >= q1) return false;
+    const int nbx = A.nx / TX;
+    const int tile = (int)(q / A.nz), z0 = (int)(q % A.nz);
+    const long long rest = q1 - q;
+    const int z1 = rest < (long long)(A.nz - z0) ? z0 + (int)rest : A.nz;
+    s.x0 = (tile % nbx) * TX;
+    s.y0 = (tile / nbx) * TY;
+    s.z0 = z0;
+    s.z1 = z1;
+    q += z1 - z0;
+    return true;
+  }
+};
+
+// Accumulator rows = TMEM lanes: warp w drains lane quarter w % 4 of block blk
+// (and of its overflow block), all COUT columns in chunks of 16 (bias bias[]
+// in shared memory), and zeroes what it read; the zeros land while it
+// computes. The epilogue warps form two groups of four that take alternate
+// output planes, so that two planes are drained at a time.
+template <int CIN, int COUT, int EPI>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tmem, int blk, int warp, size_t cell,
+                                              unsigned long long * empty, int lane, const float * bias) {
+  constexpr int S = ConvLayout<CIN, COUT>::S;
+  const unsigned tq = tmem + ((unsigned)((warp & 3) * 32) << 16) + (unsigned)(blk * COUT);
+#pragma unroll
+  for (int c0 = 0; c0 < COUT; c0 += 16) {
+    const unsigned ta = tq + c0;
+    float v[16];
+    tmem_ld16(ta, v);
+    tmem_zero<16>(ta);
+    if (blk < 2) {   // the part collected in the overflow block
+      const unsigned tb = ta + (unsigned)(S * COUT);
+      float w[16];
+      tmem_ld16(tb, w);
+      tmem_zero<16>(tb);
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] += w[q];
+    }
+    if constexpr (EPI == EPI_LINEAR) {
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (c0 + q < A.nout) A.outf[cell * A.nout + c0 + q] = v[q] + bias[c0 + q];
+    } else {
+      alignas(16) __nv_bfloat162 o[8];
+      if constexpr (EPI == EPI_GELU) {
+        alignas(16) __nv_bfloat162 zp[8];
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          const float za = v[q] + bias[c0 + q], zb = v[q + 1] + bias[c0 + q + 1];
+          zp[q / 2] = __floats2bfloat162_rn(za, zb);
+          o[q / 2] = __floats2bfloat162_rn(gelu(za), gelu(zb));
+        }
+        if (A.pre) {
+          uint4 * dp = reinterpret_cast<uint4 *>(A.pre + cell * COUT + c0);
+          dp[0] = reinterpret_cast<const uint4 *>(zp)[0];
+          dp[1] = reinterpret_cast<const uint4 *>(zp)[1];
+        }
+      } else {
+        alignas(16) __nv_bfloat162 zs[8];
+        const uint4 * sp = reinterpret_cast<const uint4 *>(A.zsave + cell * COUT + c0);
+        reinterpret_cast<uint4 *>(zs)[0] = sp[0];
+        reinterpret_cast<uint4 *>(zs)[1] = sp[1];
+#pragma unroll
+        for (int q = 0; q < 16; q += 2) {
+          const float2 zf = __bfloat1622float2(zs[q / 2]);
+          o[q / 2] = __floats2bfloat162_rn(v[q] * gelu_grad(zf.x), v[q + 1] * gelu_grad(zf.y));
+        }
+      }
+      uint4 * op = reinterpret_cast<uint4 *>(A.out + cell * COUT + c0);
+      op[0] = reinterpret_cast<const uint4 *>(o)[0];
+      op[1] = reinterpret_cast<const uint4 *>(o)[1];
+    }
+  }
+  // the accumulator may be written again once every warp of the group has
+  // read and zeroed its part
   tmem_wait_st();
   tc_fence_before();
   __syncwarp();
   if (lane == 0) nn_arrive(empty);
 }
 
-// Persistent CTAs over work items k = blockIdx.x, blockIdx.x + gridDim.x, ...
-// Loader warps (NLD): the input planes of the items, in order, into a ring of
-// NSL slots (16-byte asynchronous copies; each thread arrives on full once its
+// Persistent CTAs, each over its share of the output planes (ConvCursor).
+// Loader warps (NLD): the input planes of its segments, in order, into a ring
+// of NSL slots (16-byte asynchronous copies; each thread arrives on full once its
 // copies of a plane landed). MMA warp (warp NEPI, one thread): per input plane
 // the MMAs of its 9 shifts into the accumulators of the output planes it
 // feeds; tcgen05.commit then releases the slot (slot_free) and, when an output
@@ -383,12 +396,14 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     }
     for (int a = 0; a < S; a++) {
       nn_mbar_init(&accf[a], 1);
-      nn_mbar_init(&acce[a], NEPI);
+      nn_mbar_init(&acce[a], NEPI / 2);
     }
     nn_mbar_init(fin, 1);
     *abort_flag = 0;
     fence_barrier_init();
   }
+  float * bias_s = reinterpret_cast<float *>(smc + L::BIAS);
+  if (tid < COUT) bias_s[tid] = (EPI != EPI_DGELU) ? A.bias[tid] : 0.f;
   // weights: the exact shared-memory image, read by the tensor cores
   for (int u = tid; u < L::WB / 16; u += CONV_THREADS) cp16(wsm + u * 16, reinterpret_cast<const char *>(A.w) + u * 16, true);
   cp_commit();
@@ -398,10 +413,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tslot;
-  constexpr int CW = COUT / 2;
   if (warp < NEPI) {   // every accumulator starts at zero
-    const unsigned tl = tmem + ((unsigned)((warp & 3) * 32) << 16) + (warp >> 2) * CW;
-    for (int c = 0; c < S; c++) tmem_zero<CW>(tl + c * COUT);
+    const unsigned tl = tmem + ((unsigned)((warp & 3) * 32) << 16);
+    for (int c = warp >> 2; c < S + 2; c += 2)
+      for (int c0 = 0; c0 < COUT; c0 += 16) tmem_zero<16>(tl + c * COUT + c0);
     tmem_wait_st();
   }
   tc_fence_before();
@@ -415,9 +430,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
       const uint64_t bdesc0 = smem_desc(su32(wsm), L::WSH, 128);
       const unsigned hb = su32(halo);
       bool ok = true;
-      int hc = 0, gb = 0;   // input planes consumed; output planes of the items before this one
-      for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
-        const ConvItem it = conv_item(A, k);
+      int hc = 0, gb = 0;   // input planes consumed; output planes of the segments before this one
+      ConvCursor cur(A);
+      ConvSeg it;
+      while (ok && cur.next(A, it)) {
         for (int p = it.z0 - 1; p <= it.z1 && ok; p++, hc++) {
           ok = conv_wait(&full[hc % NS], (unsigned)(hc / NS) & 1u, abort_flag);
           // first contribution to output plane p + 1: its accumulator drained
@@ -425,32 +441,27 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
           if (ok && p + 1 < it.z1 && gn >= S) ok = conv_wait(&acce[gn % S], (unsigned)(gn / S - 1) & 1u, abort_flag);
           if (!ok) break;
           tc_fence_after();
-          // outputs ohi .. olo (descending, so ascending accumulator columns),
-          // taps dz = p - o; at most two runs of consecutive columns
+          // outputs ohi .. olo (descending: ascending accumulator blocks), taps
+          // dz = p - o; the window starts at block c(g(p + 1))
           const int ohi = min(p + 1, it.z1 - 1), olo = max(p - 1, it.z0);
+          const int n = ohi - olo + 1;
+          const int blk = colslot(gb + (p + 1 - it.z0)) + (p + 1 - ohi);
           const uint64_t adesc = smem_desc(hb + (unsigned)((hc % NS) * L::SLOTB), L::CHB, L::ROWB);
-          int o = ohi;
-          while (o >= olo) {
-            const int c = colslot(gb + (o - it.z0));
-            int n = 1;   // run length: columns c .. c + n - 1
-            while (o - n >= olo && c + n < S) n++;
-            const unsigned d = tmem + (unsigned)(c * COUT);
-            const uint32_t idesc = n == 1 ? instr_desc_bf16(128, COUT, 0, 0)
-                                 : n == 2 ? instr_desc_bf16(128, 2 * COUT, 0, 0)
-                                          : instr_desc_bf16(128, 3 * COUT, 0, 0);
-            const uint64_t bd0 = bdesc0 + (uint64_t)(((p - o + 1) * COUT * 16) >> 4);   // rows of tap dz = p - o
+          const unsigned d = tmem + (unsigned)(blk * COUT);
+          const uint32_t idesc = n == 1 ? instr_desc_bf16(128, COUT, 0, 0)
+                               : n == 2 ? instr_desc_bf16(128, 2 * COUT, 0, 0)
+                                        : instr_desc_bf16(128, 3 * COUT, 0, 0);
+          const uint64_t bd0 = bdesc0 + (uint64_t)(((p - ohi + 1) * COUT * 16) >> 4);   // rows of tap dz = p - ohi
 #pragma unroll
-            for (int sh = 0; sh < 9; sh++) {
-              const int dy = sh / 3, dx = sh % 3;   // offsets + 1
+          for (int sh = 0; sh < 9; sh++) {
+            const int dy = sh / 3, dx = sh % 3;   // offsets + 1
 #pragma unroll
-              for (int kk = 0; kk < CIN / 16; kk++) {
-                // start addresses advance in 16-byte units in the low bits of the descriptors
-                const uint64_t a = adesc + (uint64_t)((dy * L::ROWB + dx * 16 + kk * 2 * L::CHB) >> 4);
-                const uint64_t b = bd0 + (uint64_t)(((sh * L::CC + 2 * kk) * L::WSH) >> 4);
-                mma_bf16(d, a, b, idesc, true);
-              }
+            for (int kk = 0; kk < CIN / 16; kk++) {
+              // start addresses advance in 16-byte units in the low bits of the descriptors
+              const uint64_t a = adesc + (uint64_t)((dy * L::ROWB + dx * 16 + kk * 2 * L::CHB) >> 4);
+              const uint64_t b = bd0 + (uint64_t)(((sh * L::CC + 2 * kk) * L::WSH) >> 4);
+              mma_bf16(d, a, b, idesc, true);
             }
-            o -= n;
           }
           mma_commit(&sfree[hc % NS]);
           if (p - 1 >= it.z0) mma_commit(&accf[(gb + p - 1 - it.z0) % S]);   // output plane p - 1 complete
@@ -465,28 +476,30 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     }
     __syncwarp();
   } else if (warp > NEPI) {
-    // loaders: plane h into slot h % NS once the MMAs of plane h - NS are done;
-    // plane h - LAG is announced (each thread: its copies landed, made visible
-    // to the tensor cores, one arrival) after plane h's copies were issued, so
-    // LAG + 1 planes of copies are in flight
+    // loaders: plane h into slot h % NS once the MMAs of plane h - NS are done.
+    // Plane h - LAG is announced (each thread: its copies landed, made visible
+    // to the tensor cores, one arrival) before that wait, so the announcement
+    // never waits on recent MMAs: while the loaders wait for a slot, the MMA
+    // warp has the planes up to h - LAG
     constexpr int LAG = L::LAG;
     const int lt = tid - 32 * (NEPI + 1);
     int h = 0;
     bool ok = true;
-    for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
-      const ConvItem it = conv_item(A, k);
+    ConvCursor cur(A);
+    ConvSeg it;
+    while (ok && cur.next(A, it)) {
       for (int p = it.z0 - 1; p <= it.z1; p++, h++) {
+        if (h >= LAG) {
+          cp_wait<LAG - 1>();
+          fence_proxy_async();
+          nn_arrive(&full[(h - LAG) % NS]);
+        }
         if (h >= NS && !conv_wait(&sfree[h % NS], (unsigned)((h - NS) / NS) & 1u, abort_flag)) {
           ok = false;
           break;
         }
         load_halo_part<CIN>(halo + (h % NS) * L::SLOTB, A.in, A.nx, A.ny, it.x0, it.y0, wrapi(p, A.nz), lt);
         cp_commit();
-        if (h >= LAG) {
-          cp_wait<LAG>();
-          fence_proxy_async();
-          nn_arrive(&full[(h - LAG) % NS]);
-        }
       }
     }
     cp_wait<0>();
@@ -496,15 +509,15 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     if (!ok && lane == 0) atomicOr(A.status, ST_TIMEOUT);
   } else {
     const int m = (warp & 3) * 32 + lane;   // accumulator row = TMEM lane of this thread
-    float bv[CW];
-#pragma unroll
-    for (int q = 0; q < CW; q++) bv[q] = (EPI != EPI_DGELU) ? A.bias[(warp >> 2) * CW + q] : 0.f;
+    const int grp = warp >> 2;              // this warp's group takes planes g with g % 2 == grp
     int g = 0;
     bool ok = true;
-    for (int k = blockIdx.x; k < A.nitems && ok; k += gridDim.x) {
-      const ConvItem it = conv_item(A, k);
+    ConvCursor cur(A);
+    ConvSeg it;
+    while (ok && cur.next(A, it)) {
       const int xi = it.x0 + (m & 7), yj = it.y0 + (m >> 3);
       for (int z = it.z0; z < it.z1; z++, g++) {
+        if ((g & 1) != grp) continue;
         if (!conv_wait(&accf[g % S], (unsigned)(g / S) & 1u, abort_flag)) {
           if (lane == 0) atomicOr(A.status, ST_TIMEOUT);
           ok = false;
@@ -512,7 +525,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
         }
         tc_fence_after();
         const size_t cell = ((size_t)z * A.ny + yj) * A.nx + xi;
-        conv_epilogue<CIN, COUT, EPI>(A, tmem + (unsigned)(colslot(g) * COUT), warp, cell, &acce[g % S], lane, bv);
+        conv_epilogue<CIN, COUT, EPI>(A, tmem, colslot(g), warp, cell, &acce[g % S], lane, bias_s);
       }
     }
   }
@@ -850,27 +863,6 @@ static int conv_ctas_per_sm(const void * kern, int threads, int smem, int tcols)
   return n;
 }
 
-// z planes per work item. Work items go round-robin to the g = per_sm x nsm
-// persistent CTAs; CTAs b and b + nsm share an SM, and CTA b gets
-// items / g items, one more when b < items mod g. The chunk minimises the
-// input planes (z planes + 2 per item) of the busiest SM.
-static int conv_chunk(int ntile, int nz, int nsm, int per_sm) {
-  const long g = (long)nsm * per_sm;
-  long best = -1;
-  int zc = nz;
-  for (int c = 1; c <= nz; c++) {
-    const long items = (long)ntile * ((nz + c - 1) / c);
-    long load = 0;
-    for (int j = 0; j < per_sm; j++) {
-      const long b = (long)j * nsm;
-      load += items / g + (b < items % g ? 1 : 0);
-    }
-    load *= c + 2;
-    if (best < 0 || load < best) { best = load; zc = c; }
-  }
-  return zc;
-}
-
 template <int CIN, int COUT, int EPI>
 int launch_conv3(ConvArgs a, cudaStream_t st) {
   using L = ConvLayout<CIN, COUT>;
@@ -887,12 +879,10 @@ int launch_conv3(ConvArgs a, cudaStream_t st) {
     return conv_ctas_per_sm(reinterpret_cast<const void *>(kern), CONV_THREADS, L::BYTES, L::TCOLS);
   }();
   if (per_sm < 1) return 1;
-  const int ntile = (a.nx / TX) * (a.ny / TY), nsm = device_sms();
-  const int g = per_sm * nsm;
+  const long long total = (long long)(a.nx / TX) * (a.ny / TY) * a.nz;   // output planes of all tiles
+  const int g = per_sm * device_sms();
   if (g < 1) return 1;
-  a.zc = conv_chunk(ntile, a.nz, nsm, per_sm);
-  a.nitems = ntile * ((a.nz + a.zc - 1) / a.zc);
-  const int grid = a.nitems < g ? a.nitems : g;
+  const int grid = total < g ? (int)total : g;
   kern<<<grid, CONV_THREADS, L::BYTES, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
