@@ -330,21 +330,25 @@ def block_mean(a, coarse):
 
 
 def train(net: ClosureNet, data: Dataset, idx, epochs: int, batch: int = 8, lr: float = 1e-3, seed: int = 0,
-          log=None):
+          log=None, lr_final: float | None = None):
     """Adam over the samples idx (a batch accumulates its samples'
-    gradients); returns the mean loss of each epoch."""
+    gradients), the learning rate decaying from lr to lr_final (default
+    lr / 10) along a half cosine over the epochs, so that the last epochs take
+    small steps; returns the mean loss of each epoch."""
     torch = _torch()
     rng = np.random.default_rng(seed)
+    lo = lr / 10 if lr_final is None else lr_final
     hist = []
     for ep in range(epochs):
         order = rng.permutation(np.asarray(idx))
         net.loss.zero_()
+        lr_ep = lo + (lr - lo) * 0.5 * (1.0 + math.cos(math.pi * ep / max(epochs, 1)))
         for b0 in range(0, len(order), batch):
             chunk = order[b0:b0 + batch]
             for q, s in enumerate(chunk):
                 net.forward(data.X[s])
                 net.backward(data.T[s], x=data.X[s], accumulate=q > 0)
-            net.adam(lr)
+            net.adam(lr_ep)
         torch.cuda.synchronize()
         hist.append(net.loss.item() / len(order))
         if log:

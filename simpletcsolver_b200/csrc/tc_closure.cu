@@ -165,8 +165,17 @@ __device__ __forceinline__ float gelu_grad(float z) {
 constexpr int TX = 8, TY = 16;             // output tile: 8 x, 16 y, one z plane (M = 128)
 constexpr int HX = TX + 2, HY = TY + 2;    // halo of one plane
 constexpr int NN_THREADS = 128;            // weight gradient: 4 warps, one TMEM lane quarter each
-constexpr int NEPI = 8;                    // epilogue warps: two per TMEM lane quarter
-constexpr int NLD = 2;                     // halo loader warps
+// epilogue warps: groups of four (one per TMEM lane quarter), each group
+// draining every NGRP-th output plane; halo loader warps
+#ifndef TC_CONV_EPI_GROUPS
+#define TC_CONV_EPI_GROUPS 2
+#endif
+#ifndef TC_CONV_LOADERS
+#define TC_CONV_LOADERS 2
+#endif
+constexpr int NGRP = TC_CONV_EPI_GROUPS;
+constexpr int NEPI = 4 * NGRP;
+constexpr int NLD = TC_CONV_LOADERS;
 constexpr int CONV_THREADS = 32 * (NEPI + 1 + NLD);   // + the MMA warp and the loaders
 
 enum ConvEpilogue { EPI_GELU = 0, EPI_LINEAR = 1, EPI_DGELU = 2 };
@@ -202,6 +211,7 @@ struct ConvLayout {
   static constexpr int BIAS = BAR + NBAR * 8 + 16;       // COUT floats
   static constexpr int BYTES = BIAS + COUT * 4;
   static_assert(TCOLS == 128 || TCOLS == 256, "tensor-memory allocation: a power of two");
+  static_assert(S % NGRP == 0, "each accumulator belongs to one epilogue group");
 };
 
 struct ConvArgs {
@@ -296,8 +306,8 @@ struct ConvCursor {
 // Accumulator rows = TMEM lanes: warp w drains lane quarter w % 4 of block blk
 // (and of its overflow block), all COUT columns in chunks of 16 (bias bias[]
 // in shared memory), and zeroes what it read; the zeros land while it
-// computes. The epilogue warps form two groups of four that take alternate
-// output planes, so that two planes are drained at a time.
+// computes. The epilogue warps form NGRP groups of four that take the output
+// planes in turn, so that NGRP planes are drained at a time.
 template <int CIN, int COUT, int EPI>
 __device__ __forceinline__ void conv_epilogue(const ConvArgs & A, unsigned tmem, int blk, int warp, size_t cell,
                                               unsigned long long * empty, int lane, const float * bias) {
@@ -396,7 +406,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     }
     for (int a = 0; a < S; a++) {
       nn_mbar_init(&accf[a], 1);
-      nn_mbar_init(&acce[a], NEPI / 2);
+      nn_mbar_init(&acce[a], 4);
     }
     nn_mbar_init(fin, 1);
     *abort_flag = 0;
@@ -415,7 +425,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
   const unsigned tmem = *tslot;
   if (warp < NEPI) {   // every accumulator starts at zero
     const unsigned tl = tmem + ((unsigned)((warp & 3) * 32) << 16);
-    for (int c = warp >> 2; c < S + 2; c += 2)
+    for (int c = warp >> 2; c < S + 2; c += NGRP)
       for (int c0 = 0; c0 < COUT; c0 += 16) tmem_zero<16>(tl + c * COUT + c0);
     tmem_wait_st();
   }
@@ -509,7 +519,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     if (!ok && lane == 0) atomicOr(A.status, ST_TIMEOUT);
   } else {
     const int m = (warp & 3) * 32 + lane;   // accumulator row = TMEM lane of this thread
-    const int grp = warp >> 2;              // this warp's group takes planes g with g % 2 == grp
+    const int grp = warp >> 2;              // this warp's group takes planes g with g % NGRP == grp
     int g = 0;
     bool ok = true;
     ConvCursor cur(A);
@@ -517,7 +527,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 2) conv3_kernel(ConvArgs A) {
     while (ok && cur.next(A, it)) {
       const int xi = it.x0 + (m & 7), yj = it.y0 + (m >> 3);
       for (int z = it.z0; z < it.z1; z++, g++) {
-        if ((g & 1) != grp) continue;
+        if (g % NGRP != grp) continue;
         if (!conv_wait(&accf[g % S], (unsigned)(g / S) & 1u, abort_flag)) {
           if (lane == 0) atomicOr(A.status, ST_TIMEOUT);
           ok = false;

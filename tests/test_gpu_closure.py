@@ -34,13 +34,17 @@ def _rel_max(a, b):
     return float((a - b).abs().max() / b.abs().max())
 
 
+@pytest.mark.parametrize("grid", [(16, 32, 6), (64, 256, 32)])
 @pytest.mark.parametrize("cinp,coutp,cin,cout", [(16, 32, 4, 32), (32, 32, 32, 32), (32, 16, 32, 3)])
-def test_convolution_passes_match_cpu_oracle(lib, cinp, coutp, cin, cout):
+def test_convolution_passes_match_cpu_oracle(lib, cinp, coutp, cin, cout, grid):
     """forward (linear and GELU epilogues), input and weight gradients of one
-    layer on a 16 x 32 x 6 grid, tensor-core kernels vs torch FP64 on the CPU"""
+    layer, tensor-core kernels vs torch FP64 on the CPU. 16 x 32 x 6: one
+    output plane per CTA; 64 x 256 x 32: about 14 planes per CTA, so the
+    accumulator ring wraps, planes collect in the overflow blocks and CTA
+    ranges cross column tiles."""
     torch = _torch()
     F = torch.nn.functional
-    nx, ny, nz = 16, 32, 6
+    nx, ny, nz = grid
     g = torch.Generator().manual_seed(7)
     bf = lambda t: t.to(torch.bfloat16).to(torch.float64)
     x = torch.zeros(nz, ny, nx, cinp, dtype=torch.float64)
@@ -96,15 +100,18 @@ def test_convolution_passes_match_cpu_oracle(lib, cinp, coutp, cin, cout):
     assert _rel_max(db.cpu().double(), dy[..., :cout].sum(dim=(0, 1, 2))) < 1e-5
 
 
-def test_network_gradients_match_cpu_oracle(lib):
-    """loss and the gradients of all four layers through BF16 activations"""
+@pytest.mark.parametrize("grid", [(8, 16, 4), (64, 128, 64)])
+def test_network_gradients_match_cpu_oracle(lib, grid):
+    """loss and the gradients of all four layers through BF16 activations; at
+    64 x 128 x 64 every convolution runs about 14 output planes per CTA"""
     torch = _torch()
-    net = closure.ClosureNet(lib, (8, 16, 4), seed=3, last_scale=1.0)
+    nx, ny, nz = grid
+    net = closure.ClosureNet(lib, grid, seed=3, last_scale=1.0)
     g = torch.Generator().manual_seed(0)
-    x = torch.zeros(4, 16, 8, 16, dtype=torch.float64)
-    x[..., :4] = torch.randn(4, 16, 8, 4, generator=g, dtype=torch.float64)
+    x = torch.zeros(nz, ny, nx, 16, dtype=torch.float64)
+    x[..., :4] = torch.randn(nz, ny, nx, 4, generator=g, dtype=torch.float64)
     x = x.to(torch.bfloat16).to(torch.float64)
-    tgt = torch.randn(4, 16, 8, 3, generator=g, dtype=torch.float64)
+    tgt = torch.randn(nz, ny, nx, 3, generator=g, dtype=torch.float64)
     xd = x.to(torch.bfloat16).cuda().reshape(-1)
     net.loss.zero_()
     net.forward(xd)
