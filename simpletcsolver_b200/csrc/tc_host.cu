@@ -462,6 +462,7 @@ static int build_tables(Ctx & c, const domain_t * d) {
   // Poisson tables (compute_potential.c:173-211, 311-349)
   const int nyh = ny / 2 + 1;
   c.ps.nyh = nyh;
+  c.ps.status = c.status;
   std::vector<double> tl(nx), tu(nx), base(nx), tz(nz), ty((size_t)nx * nyh);
   for (int i = 1; i <= nx; i++) {
     tl[i - 1] = 1. / JDXC(i) * JDXF(i) / HXXF(i) / HXXF(i);

@@ -178,6 +178,7 @@ struct Poisson {
   const double * hyxc;      // HYXC(i), length nx (index i-1)
   const double * eval_y;    // -4 sin^2(pi m / ny), m < nyh
   const double * eval_z;    // -4 sin^2(pi m / nz), m < nz
+  unsigned * status;        // the context's error word (ST_TIMEOUT from a bounded wait)
 };
 
 // RK source terms of one substep: old_ (srcA of the previous substep) and new_,

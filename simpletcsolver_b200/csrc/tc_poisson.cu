@@ -28,9 +28,16 @@
 #include "tc_kernels.h"
 
 // resident CTAs per SM requested from the register allocator (measured best
-// at 256 x 1024 x 512: 2 for the divergence + y transform, 3 for the inverse y
-// transform; the divergence at 3 spills 296 bytes and takes 2.36 ms against
-// 1.25, with 8 rows of loads in flight 1.30)
+// at 256 x 1024 x 512: 2 for the divergence + y transform, whose version at 3
+// spills 296 bytes and takes 2.36 ms against 1.25 (with 8 rows of loads in
+// flight 1.30); 2 for the inverse y transform with its spectrum rows staged by
+// bulk copies (FP64), 0.68 ms against 0.74 at 3, which spills; the staged rows
+// against per-thread loads at 3: 0.74 against 0.84 ms; 3 for the inverse
+// transform of FP32 spectra (per-thread loads), 0.77 against 0.83 at 2; a persistent,
+// double-buffered version over tiles of two lines at 3 CTAs per SM: 1.00 ms;
+// the divergence with its field rows staged in chunks of 512 cells by
+// 16-byte asynchronous copies, two chunks in flight: 1.94 ms against 1.25,
+// since the per-thread loads already keep more bytes in flight)
 // y transforms (divergence + forward, inverse): elements per thread and
 // threads per CTA. Measured at 256 x 1024 x 512 (ms, divergence + forward /
 // inverse): 16 / 256 1.32 / 0.96; 8 / 512 1.59-1.68 / 1.02; 8 / 256 1.68 / 0.97.
@@ -79,6 +86,9 @@
 #endif
 #ifndef TC_IFFTY_MIN_BLOCKS
 #define TC_IFFTY_MIN_BLOCKS 3
+#endif
+#ifndef TC_IFFTY_BULK_MIN_BLOCKS
+#define TC_IFFTY_BULK_MIN_BLOCKS 2
 #endif
 #ifndef TC_DIVFFT_MIN_BLOCKS
 #define TC_DIVFFT_MIN_BLOCKS 2
@@ -812,9 +822,16 @@ static bool launch_tdm_lines(const Geo & g, const Poisson & ps, cudaStream_t st)
 }
 
 // --------------------------------------------------------------- inverse y
-template <int EPT, class Z>
-__global__ void __launch_bounds__(TC_FFTY_THREADS, TC_IFFTY_MIN_BLOCKS)
+// BULK (FP64 spectra): one thread copies the two spectrum rows of each line
+// pair (nyh values each, 16-byte aligned) straight into the pair's line buffer
+// with bulk asynchronous copies, all rows of the CTA in flight at once; every
+// thread then reads the values its extension needs from shared memory, and
+// after a barrier writes the extended lines over the staged rows. Otherwise
+// each thread loads its values from global memory.
+template <int EPT, class Z, bool BULK>
+__global__ void __launch_bounds__(TC_FFTY_THREADS, BULK ? TC_IFFTY_BULK_MIN_BLOCKS : TC_IFFTY_MIN_BLOCKS)
 iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
+  static_assert(!BULK || sizeof(Z) == 16, "bulk rows: FP64 spectra (16-byte values)");
   extern __shared__ double2 smem[];
   const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh;
   const int TI = 2 * P;
@@ -823,30 +840,82 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   const int i0 = blockIdx.x * TI + 1;
   const int k = blockIdx.y + 1;
   // Hermitian extension of the two packed real lines: each stored wavenumber
-  // mr < ny/2 is loaded once and gives the line's values at m = mr and
-  // m = ny - mr; the Nyquist terms follow (imaginary parts of DC and Nyquist
-  // ignored, as FFTW's c2r does)
+  // mr < ny/2 gives the line's values at m = mr and m = ny - mr; the Nyquist
+  // terms follow (imaginary parts of DC and Nyquist ignored, as FFTW's c2r
+  // does)
   const int half = ny >> 1;
   const Z * sp = static_cast<const Z *>(ps.spec);
+  if constexpr (BULK) {
+    unsigned long long * bar = reinterpret_cast<unsigned long long *>(smem + (size_t)P * LS);
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned row = (unsigned)(nyh * sizeof(double2));
+      unsigned total = 0;
+      for (int q = 0; q < TI; q++)
+        if (i0 + q <= nx) total += row;
+      mbar_expect_tx(bar, total);
+      for (int q = 0; q < TI; q++)
+        if (i0 + q <= nx)
+          bulk_g2s(smem + (size_t)(q >> 1) * LS + (q & 1) * nyh, sp + ((size_t)(i0 + q - 1) * nz + (k - 1)) * nyh, row,
+                   bar);
+    }
+    if (!mbar_wait(bar, 0)) {   // the copies did not land: report, store nothing
+      if (threadIdx.x == 0) atomicOr(ps.status, ST_TIMEOUT);
+      return;
+    }
+    double2 xa[EPT / 2], xb[EPT / 2];
+#pragma unroll
+    for (int r = 0; r < EPT / 2; r++) {
+      const int u = threadIdx.x + r * blockDim.x;
+      const int mr = u & (half - 1), pp = u >> (lg - 1);
+      const double2 * rows = smem + (size_t)pp * LS;
+      xa[r] = i0 + 2 * pp <= nx ? rows[mr] : make_double2(0., 0.);
+      xb[r] = i0 + 2 * pp + 1 <= nx ? rows[nyh + mr] : make_double2(0., 0.);
+    }
+    double qa = 0., qb = 0.;
+    const int pq = threadIdx.x;
+    if (pq < P) {
+      const double2 * rows = smem + (size_t)pq * LS;
+      if (i0 + 2 * pq <= nx) qa = rows[half].x;
+      if (i0 + 2 * pq + 1 <= nx) qb = rows[nyh + half].x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < EPT / 2; r++) {
+      const int u = threadIdx.x + r * blockDim.x;
+      const int mr = u & (half - 1), pp = u >> (lg - 1);
+      double2 a = xa[r], b = xb[r];
+      if (mr == 0) { a.y = 0.; b.y = 0.; }
+      double2 * line = smem + (size_t)pp * LS;
+      line[pad(mr)] = make_double2(a.x - b.y, a.y + b.x);
+      if (mr != 0) line[pad(ny - mr)] = make_double2(a.x + b.y, -a.y + b.x);
+    }
+    if (pq < P) smem[(size_t)pq * LS + pad(half)] = make_double2(qa, qb);
+  } else {
 #pragma unroll kIfftyUnroll
-  for (int r = 0; r < EPT / 2; r++) {     // P half = blockDim EPT / 2 items
-    const int u = threadIdx.x + r * blockDim.x;
-    const int mr = u & (half - 1);
-    const int pp = u >> (lg - 1);
-    const int ia = i0 + 2 * pp, ib = ia + 1;
-    double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
-    if (ia <= nx) xa = zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr);
-    if (ib <= nx) xb = zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr);
-    if (mr == 0) { xa.y = 0.; xb.y = 0.; }
-    double2 * line = smem + (size_t)pp * LS;
-    line[pad(mr)] = make_double2(xa.x - xb.y, xa.y + xb.x);
-    if (mr != 0) line[pad(ny - mr)] = make_double2(xa.x + xb.y, -xa.y + xb.x);
-  }
-  for (int pp = threadIdx.x; pp < P; pp += blockDim.x) {
-    const int ia = i0 + 2 * pp, ib = ia + 1;
-    const double xa = ia <= nx ? zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + half).x : 0.;
-    const double xb = ib <= nx ? zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + half).x : 0.;
-    smem[(size_t)pp * LS + pad(half)] = make_double2(xa, xb);
+    for (int r = 0; r < EPT / 2; r++) {     // P half = blockDim EPT / 2 items
+      const int u = threadIdx.x + r * blockDim.x;
+      const int mr = u & (half - 1);
+      const int pp = u >> (lg - 1);
+      const int ia = i0 + 2 * pp, ib = ia + 1;
+      double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
+      if (ia <= nx) xa = zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr);
+      if (ib <= nx) xb = zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr);
+      if (mr == 0) { xa.y = 0.; xb.y = 0.; }
+      double2 * line = smem + (size_t)pp * LS;
+      line[pad(mr)] = make_double2(xa.x - xb.y, xa.y + xb.x);
+      if (mr != 0) line[pad(ny - mr)] = make_double2(xa.x + xb.y, -xa.y + xb.x);
+    }
+    for (int pp = threadIdx.x; pp < P; pp += blockDim.x) {
+      const int ia = i0 + 2 * pp, ib = ia + 1;
+      const double xa = ia <= nx ? zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + half).x : 0.;
+      const double xb = ib <= nx ? zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + half).x : 0.;
+      smem[(size_t)pp * LS + pad(half)] = make_double2(xa, xb);
+    }
   }
   __syncthreads();
   {
@@ -1065,7 +1134,11 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   if (fz) fftz_kernel<EPTZ, +1, Z><<<gz, Pz * tplz, smz, st>>>(g, ps, Pz, lgz);
   else dftz_kernel<+1, Z><<<gc, 128, sizeof(double2) * g.nz, st>>>(g, ps);
   mark(pm.k_inv);
-  if (fy) iffty_kernel<EPTY, Z><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
+  constexpr bool bulk = sizeof(Z) == 16;   // staged spectrum rows need 16-byte values
+  if (fy && bulk && g.ny >= 16)   // two rows of nyh values fit a padded line buffer from ny = 16 on
+    iffty_kernel<EPTY, Z, bulk><<<gy, Py * tply, smy + 16, st>>>(g, ps, Py, lgy, f.psi);
+  else if (fy)
+    iffty_kernel<EPTY, Z, false><<<gy, Py * tply, smy, st>>>(g, ps, Py, lgy, f.psi);
   else idfty_kernel<Z><<<gl, 128, sizeof(double2) * ps.nyh, st>>>(g, ps, f.psi);
   mark(pm.k_ify);
 }
@@ -1111,9 +1184,12 @@ static void poisson_smem_limits_s() {
   allow_dyn_smem(div_ffty_kernel<16, T, Z>);
   allow_dyn_smem(div_ffty_kernel<8, T, Z>);
   allow_dyn_smem(div_ffty_kernel<4, T, Z>);
-  allow_dyn_smem(iffty_kernel<16, Z>);
-  allow_dyn_smem(iffty_kernel<8, Z>);
-  allow_dyn_smem(iffty_kernel<4, Z>);
+  allow_dyn_smem(iffty_kernel<16, Z, false>);
+  allow_dyn_smem(iffty_kernel<8, Z, false>);
+  allow_dyn_smem(iffty_kernel<4, Z, false>);
+  allow_dyn_smem(iffty_kernel<16, Z, sizeof(Z) == 16>);
+  allow_dyn_smem(iffty_kernel<8, Z, sizeof(Z) == 16>);
+  allow_dyn_smem(iffty_kernel<4, Z, sizeof(Z) == 16>);
   allow_dyn_smem(fftz_kernel<16, -1, Z>);
   allow_dyn_smem(fftz_kernel<16, +1, Z>);
   allow_dyn_smem(fftz_kernel<8, -1, Z>);
