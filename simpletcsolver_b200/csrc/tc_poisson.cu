@@ -37,7 +37,10 @@
 // double-buffered version over tiles of two lines at 3 CTAs per SM: 1.00 ms;
 // the divergence with its field rows staged in chunks of 512 cells by
 // 16-byte asynchronous copies, two chunks in flight: 1.94 ms against 1.25,
-// since the per-thread loads already keep more bytes in flight)
+// since the per-thread loads already keep more bytes in flight; a persistent
+// divergence transform with two roles (256 threads forming the divergence of
+// the next tile into one of two line buffers while 256 transform the current
+// one, at named barriers, one CTA per SM): 1.31 ms)
 // y transforms (divergence + forward, inverse): elements per thread and
 // threads per CTA. Measured at 256 x 1024 x 512 (ms, divergence + forward /
 // inverse): 16 / 256 1.32 / 0.96; 8 / 512 1.59-1.68 / 1.02; 8 / 256 1.68 / 0.97.
