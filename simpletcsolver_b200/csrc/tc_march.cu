@@ -34,6 +34,11 @@
 #include "tc_common.cuh"
 #include "tc_kernels.h"
 
+// FP32-storage mode: right-hand sides in float arithmetic (1), or double (0)
+#ifndef TC_MARCH_FP32_ARITH
+#define TC_MARCH_FP32_ARITH 1
+#endif
+
 namespace tcgpu {
 namespace {
 
@@ -47,26 +52,37 @@ enum SlotField { SF_UX = 0, SF_UY = 1, SF_UZ = 2, SF_T = 3, SF_P = 4 };
 // variables in registers, loaded once (they depend on i only). The
 // coefficients are products of the metric tables taken once on the host
 // (P_* tables); each is spelled out below where it is used.
+// C is the arithmetic type of the right-hand sides: double, or float in the
+// FP32-storage mode (the increments, the radial solves and the update stay
+// double).
+template <class C>
 struct CoefA {
-  double xa1, xa2, xa3, yb1, yb2, zc1, zc2, h1, h2;   // ux advection
-  double lxl, lxu, ly;                                // ux Laplacian, x and y (carry 2 nu, nu)
-  double cy1, cy2, ca1, ca2, cz1, px;                 // ux cross diffusion, pressure gradient
-  double tx0, tx1, ty, tz;                            // t advection
+  C xa1, xa2, xa3, yb1, yb2, zc1, zc2, h1, h2;        // ux advection
+  C lxl, lxu, ly;                                     // ux Laplacian, x and y (carry 2 nu, nu)
+  C cy1, cy2, ca1, ca2, cz1, px;                      // ux cross diffusion, pressure gradient
+  C tx0, tx1, ty, tz;                                 // t advection
 };
+template <class C>
 struct CoefB {
-  double a1, a2, b, c, h;                             // uy / uz advection
-  double lxl, lxu, ly;                                // centred Laplacian, x and y (carry nu; t: x kappa/nu)
-  double p1, p2, qm, q0, qp, yk, yz, py;              // uy cross diffusion, pressure gradient
-  double zx0, zx1, zy;                                // uz cross diffusion
+  C a1, a2, b, c, h;                                  // uy / uz advection
+  C lxl, lxu, ly;                                     // centred Laplacian, x and y (carry nu; t: x kappa/nu)
+  C p1, p2, qm, q0, qp, yk, yz, py;                   // uy cross diffusion, pressure gradient
+  C zx0, zx1, zy;                                     // uz cross diffusion
+};
+// the z Laplacian's coefficients and 1/hz, shared by every cell
+template <class C>
+struct CoefZ {
+  C l, c, u, ihz;
 };
 // The Laplacians in x and y are applied as differences from the centre value:
 // the centre coefficients of the tables are the negated sums of the others
 // (F_LXC = -F_LXL - F_LXU, F_LYC = -2 F_LYL = -2 F_LYU, likewise for C_*), so
 // l a + c b + u d = l (a - b) + u (d - b) and only l and u are held.
 
-__device__ __forceinline__ void load_coefs(CoefA & q, const Coefs & cf, int i) {
+template <class C>
+__device__ __forceinline__ void load_coefs(CoefA<C> & q, const Coefs & cf, int i) {
   const double * __restrict__ b = cf.tab + i;
-#define CF(T) LD(b + (T) * CSTRIDE)
+#define CF(T) (C)LD(b + (T) * CSTRIDE)
   q.xa1 = CF(P_XA1); q.xa2 = CF(P_XA2); q.xa3 = CF(P_XA3); q.yb1 = CF(P_YB1); q.yb2 = CF(P_YB2);
   q.zc1 = CF(P_ZC1); q.zc2 = CF(P_ZC2); q.h1 = CF(P_H1); q.h2 = CF(P_H2);
   q.lxl = CF(F_LXL); q.lxu = CF(F_LXU); q.ly = CF(F_LYL);
@@ -75,9 +91,10 @@ __device__ __forceinline__ void load_coefs(CoefA & q, const Coefs & cf, int i) {
   q.tx0 = CF(P_TX0); q.tx1 = CF(P_TX1); q.ty = CF(P_TY); q.tz = CF(P_TZ);
 #undef CF
 }
-__device__ __forceinline__ void load_coefs(CoefB & q, const Coefs & cf, int i) {
+template <class C>
+__device__ __forceinline__ void load_coefs(CoefB<C> & q, const Coefs & cf, int i) {
   const double * __restrict__ b = cf.tab + i;
-#define CF(T) LD(b + (T) * CSTRIDE)
+#define CF(T) (C)LD(b + (T) * CSTRIDE)
   q.a1 = CF(P_UA1); q.a2 = CF(P_UA2); q.b = CF(P_UB); q.c = CF(P_UC); q.h = CF(P_UH);
   q.lxl = CF(C_LXL); q.lxu = CF(C_LXU); q.ly = CF(C_LYL);
   q.p1 = CF(P_P1); q.p2 = CF(P_P2); q.qm = CF(P_QM); q.q0 = CF(P_Q0); q.qp = CF(P_QP);
@@ -133,63 +150,71 @@ struct SlotView {
 // diffusion in direction D goes to the implicit part when D is implicit
 #define ROUTE(D, V_) do { if (D) gi += (V_); else e += (V_); } while (0)
 
+// the z Laplacian's coefficients and 1/hz: kernel parameters in double
+// arithmetic, per-thread float copies in float arithmetic
+#define ZL (std::is_same<C, double>::value ? (C)cf.lz_l : lz.l)
+#define ZC (std::is_same<C, double>::value ? (C)cf.lz_c : lz.c)
+#define ZU (std::is_same<C, double>::value ? (C)cf.lz_u : lz.u)
+#define ZIH (std::is_same<C, double>::value ? (C)cf.inv_hz : lz.ihz)
 // Group A: right-hand sides of ux at face i (src/fluid/predict/ux.c) and t at
 // centre i (t.c) of cell (i, j, k); new source terms to ss.new_, increments
 // dl[0] (ux, 0 at i = 1 where ux has no unknown) and dl[1] (t), current
 // values u0[0] (ux) and u0[1] (t).
-template <int JT, int RL, int JL, int IMPL, class T>
-__device__ __forceinline__ void cell_a(const CoefA & q, const CoefB & qc_, const SlotView<T> & V, const Bc & bc, const Coefs & cf, double nu, double kappa, double rpr, int i,
-                                       size_t qf, size_t qc, const SrcSetT<T> & ss, double ca, double cb, double cg,
-                                       double old_x, double old_t, double dl[2], double u0[2]) {
+template <int JT, int RL, int JL, int IMPL, class T, class C>
+__device__ __forceinline__ void cell_a(const CoefA<C> & q, const CoefB<C> & qc_, const SlotView<T> & V, const Bc & bc,
+                                       const Coefs & cf, const CoefZ<C> & lz, C nu, C kappa, C rpr, int i, size_t qf,
+                                       size_t qc,
+                                       const SrcSetT<T> & ss, C ca, C cb, C cg, C old_x, C old_t, double dl[2],
+                                       double u0[2]) {
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
   const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
   const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
-  const double ux_0 = UX(0, 0), ux_p = UX(1, 0);
-  const double uy_00 = UY(0, 0), uy_01 = UY(0, 1);
-  const double uz_00 = UZ(0, 0), uz_01 = NUZ(0, 0);
+  const C ux_0 = UX(0, 0), ux_p = UX(1, 0);
+  const C uy_00 = UY(0, 0), uy_01 = UY(0, 1);
+  const C uz_00 = UZ(0, 0), uz_01 = NUZ(0, 0);
   // ux has no unknown at i = 1 (face 1 is the wall): its value there is
   // formed from in-bounds shared-memory neighbours and discarded, so the
   // whole cell stays one branch-free block the scheduler can interleave
   {
-    const double ux_m = UX(-1, 0);
-    const double ux_jm = UX(0, -1), ux_jp = UX(0, 1);
-    const double ux_km = MUX(0), ux_kp = NUX(0);
-    const double uy_m0 = UY(-1, 0), uy_m1 = UY(-1, 1);
-    const double uz_m0 = UZ(-1, 0), uz_m1 = NUZ(-1, 0);
-    double e, gi;
+    const C ux_m = UX(-1, 0);
+    const C ux_jm = UX(0, -1), ux_jp = UX(0, 1);
+    const C ux_km = MUX(0), ux_kp = NUX(0);
+    const C uy_m0 = UY(-1, 0), uy_m1 = UY(-1, 1);
+    const C uz_m0 = UZ(-1, 0), uz_m1 = NUZ(-1, 0);
+    C e, gi;
     // advection (ux.c:92-186): invj (l q_m + c q_0 + u q_p) with c = -l - u,
     // l = -0.5 (a q_m' + a' q_0'), u = 0.5 (...), as differences from q_0
     e = (q.xa1 * ux_m + q.xa2 * ux_0) * (ux_m - ux_0) - (q.xa2 * ux_0 + q.xa3 * ux_p) * (ux_p - ux_0);
     e += (q.yb1 * uy_m0 + q.yb2 * uy_00) * (ux_jm - ux_0) - (q.yb1 * uy_m1 + q.yb2 * uy_01) * (ux_jp - ux_0);
     e += (q.zc1 * uz_m0 + q.zc2 * uz_00) * (ux_km - ux_0) - (q.zc1 * uz_m1 + q.zc2 * uz_01) * (ux_kp - ux_0);
     // centrifugal term (:194-226): invj hd (uy averaged to the face)^2
-    const double sm = uy_m0 + uy_m1, sp = uy_00 + uy_01;
+    const C sm = uy_m0 + uy_m1, sp = uy_00 + uy_01;
     e += q.h1 * sm * sm + q.h2 * sp * sp;
     // cross diffusion (:266-375): diffusion_y1 and the uy part of diffusion_a
     // as differences of uy across j, the ux part of diffusion_a, diffusion_z1
     e += q.cy1 * (uy_m1 - uy_m0) + q.cy2 * (uy_01 - uy_00) + q.ca1 * (ux_m + ux_0) +
          q.ca2 * (ux_0 + ux_p) + q.cz1 * ((uz_01 - uz_m1) - (uz_00 - uz_m0));   // coefficients carry nu
     // pressure gradient (:377-394)
-    gi = -q.px * (PP(0, 0) - PP(-1, 0));
+    gi = -q.px * (C)(PP(0, 0) - PP(-1, 0));
     ROUTE(ix, q.lxl * (ux_m - ux_0) + q.lxu * (ux_p - ux_0));        // carries 2 nu
     ROUTE(iy, q.ly * ((ux_jm - ux_0) + (ux_jp - ux_0)));             // carries nu
-    ROUTE(iz, nu * (cf.lz_l * ux_km + cf.lz_c * ux_0 + cf.lz_u * ux_kp));
-    if constexpr (IMPL == -2) e += (i >= 2) ? ss.frc[VUX][qf] : 0.;   // closure forcing
+    ROUTE(iz, nu * (ZL * ux_km + ZC * ux_0 + ZU * ux_kp));
+    if constexpr (IMPL == -2) e += (i >= 2) ? (C)ss.frc[VUX][qf] : C(0);   // closure forcing
     if (i >= 2) ss.new_[VUX][qf] = (T)e;
-    dl[0] = (i >= 2) ? ca * e + cb * old_x + cg * gi : 0.;
+    dl[0] = (i >= 2) ? (double)(ca * e + cb * old_x + cg * gi) : 0.;
   }
   {
-    const double t_0 = TT(0, 0);
-    const double tim = TT(-1, 0), tip = TT(1, 0), tjm = TT(0, -1), tjp = TT(0, 1);
-    const double tkm = MTT(), tkp = NTT(0);
-    double e, gi = 0.;
+    const C t_0 = TT(0, 0);
+    const C tim = TT(-1, 0), tip = TT(1, 0), tjm = TT(0, -1), tjp = TT(0, 1);
+    const C tkm = MTT(), tkp = NTT(0);
+    C e, gi = 0;
     // advection (t.c:88-116) with face velocities ux_0, ux_p, uy_00, uy_01, uz_00, uz_01
     e = q.tx0 * ux_0 * (tim - t_0) - q.tx1 * ux_p * (tip - t_0);
     e += q.ty * uy_00 * (tjm - t_0) - q.ty * uy_01 * (tjp - t_0);
     e += q.tz * uz_00 * (tkm - t_0) - q.tz * uz_01 * (tkp - t_0);
     ROUTE(ix, rpr * (qc_.lxl * (tim - t_0) + qc_.lxu * (tip - t_0)));   // nu kappa/nu
     ROUTE(iy, rpr * (qc_.ly * ((tjm - t_0) + (tjp - t_0))));
-    ROUTE(iz, kappa * (cf.lz_l * tkm + cf.lz_c * t_0 + cf.lz_u * tkp));
+    ROUTE(iz, kappa * (ZL * tkm + ZC * t_0 + ZU * tkp));
     ss.new_[VT][qc] = (T)e;
     dl[1] = ca * e + cb * old_t + cg * gi;
     u0[1] = t_0;
@@ -200,24 +225,24 @@ __device__ __forceinline__ void cell_a(const CoefA & q, const CoefB & qc_, const
 // Group B: right-hand sides of uy (src/fluid/predict/uy.c) and uz (uz.c) at
 // centre i of cell (i, j, k); increments dl[0] (uy), dl[1] (uz), current
 // values u0[0], u0[1].
-template <int JT, int RL, int JL, int IMPL, class T>
-__device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, const Bc & bc,
-                                       const Coefs & cf, double nu, int i, size_t qc, const SrcSetT<T> & ss,
-                                       double ca, double cb, double cg, double old_y, double old_z, double dl[2],
-                                       double u0[2]) {
+template <int JT, int RL, int JL, int IMPL, class T, class C>
+__device__ __forceinline__ void cell_b(const CoefB<C> & q, const SlotView<T> & V, const Bc & bc,
+                                       const Coefs & cf, const CoefZ<C> & lz, C nu, int i, size_t qc,
+                                       const SrcSetT<T> & ss,
+                                       C ca, C cb, C cg, C old_y, C old_z, double dl[2], double u0[2]) {
   const bool ix = IMPL >= 0 ? (IMPL & 1) != 0 : bc.implicit[0] != 0;
   const bool iy = IMPL >= 0 ? (IMPL & 2) != 0 : bc.implicit[1] != 0;
   const bool iz = IMPL >= 0 ? (IMPL & 4) != 0 : bc.implicit[2] != 0;
-  const double ux_0 = UX(0, 0), ux_1 = UX(1, 0);
-  const double uy_0 = UY(0, 0), uy_jp = UY(0, 1);
-  const double uz_0 = UZ(0, 0), uz_kp = NUZ(0, 0);
-  const double p_0 = PP(0, 0);
+  const C ux_0 = UX(0, 0), ux_1 = UX(1, 0);
+  const C uy_0 = UY(0, 0), uy_jp = UY(0, 1);
+  const C uz_0 = UZ(0, 0), uz_kp = NUZ(0, 0);
+  const double p_0 = PP(0, 0);   // p is double in both modes
   {  // uy
-    const double uy_im = UY(-1, 0), uy_ip = UY(1, 0), uy_jm = UY(0, -1);
-    const double uy_km = MUY(0), uy_kp = NUY(0);
-    const double ux_0m = UX(0, -1), ux_1m = UX(1, -1);
-    const double uz_jm = UZ(0, -1), uz_jmkp = NUZ(0, -1);
-    double e, gi;
+    const C uy_im = UY(-1, 0), uy_ip = UY(1, 0), uy_jm = UY(0, -1);
+    const C uy_km = MUY(0), uy_kp = NUY(0);
+    const C ux_0m = UX(0, -1), ux_1m = UX(1, -1);
+    const C uz_jm = UZ(0, -1), uz_jmkp = NUZ(0, -1);
+    C e, gi;
     // advection (uy.c:93-180), as differences from uy_0
     e = q.a1 * (ux_0m + ux_0) * (uy_im - uy_0) - q.a2 * (ux_1m + ux_1) * (uy_ip - uy_0);
     e += q.b * (uy_jm + uy_0) * (uy_jm - uy_0) - q.b * (uy_0 + uy_jp) * (uy_jp - uy_0);
@@ -228,37 +253,41 @@ __device__ __forceinline__ void cell_b(const CoefB & q, const SlotView<T> & V, c
     // (lyy1 at j-1, j), diffusion_z1 (lyz at k, k+1)
     e += q.p1 * (ux_0 - ux_0m) + q.p2 * (ux_1 - ux_1m) + q.qm * uy_im + q.q0 * uy_0 + q.qp * uy_ip +
          q.yk * ((ux_0 + ux_1) - (ux_0m + ux_1m)) + q.yz * ((uz_kp - uz_jmkp) - (uz_0 - uz_jm));   // carry nu
-    gi = -q.py * (p_0 - PP(0, -1));
+    gi = -q.py * (C)(p_0 - PP(0, -1));
     ROUTE(ix, q.lxl * (uy_im - uy_0) + q.lxu * (uy_ip - uy_0));      // carry nu
-    ROUTE(iy, 2. * (q.ly * ((uy_jm - uy_0) + (uy_jp - uy_0))));
-    ROUTE(iz, nu * (cf.lz_l * uy_km + cf.lz_c * uy_0 + cf.lz_u * uy_kp));
-    if constexpr (IMPL == -2) e += ss.frc[VUY][qc];
+    ROUTE(iy, C(2) * (q.ly * ((uy_jm - uy_0) + (uy_jp - uy_0))));
+    ROUTE(iz, nu * (ZL * uy_km + ZC * uy_0 + ZU * uy_kp));
+    if constexpr (IMPL == -2) e += (C)ss.frc[VUY][qc];
     ss.new_[VUY][qc] = (T)e;
     dl[0] = ca * e + cb * old_y + cg * gi;
   }
   {  // uz
-    const double uz_im = UZ(-1, 0), uz_ip = UZ(1, 0), uz_jm = UZ(0, -1), uz_jp = UZ(0, 1);
-    const double uz_km = MUZ();
-    const double uy_km = MUY(0), uy_jpkm = MUY(1);
-    const double ux_0k = MUX(0), ux_1k = MUX(1);
-    double e, gi;
+    const C uz_im = UZ(-1, 0), uz_ip = UZ(1, 0), uz_jm = UZ(0, -1), uz_jp = UZ(0, 1);
+    const C uz_km = MUZ();
+    const C uy_km = MUY(0), uy_jpkm = MUY(1);
+    const C ux_0k = MUX(0), ux_1k = MUX(1);
+    C e, gi;
     // advection (uz.c:88-180), as differences from uz_0
     e = q.a1 * (ux_0k + ux_0) * (uz_im - uz_0) - q.a2 * (ux_1k + ux_1) * (uz_ip - uz_0);
     e += q.b * (uy_km + uy_0) * (uz_jm - uz_0) - q.b * (uy_jpkm + uy_jp) * (uz_jp - uz_0);
     e += q.c * (uz_km + uz_0) * (uz_km - uz_0) - q.c * (uz_0 + uz_kp) * (uz_kp - uz_0);
     // diffusion_x1 (lzx at faces i, i+1), diffusion_y1 (lzy at j, j+1)
     e += q.zx1 * (ux_1 - ux_1k) - q.zx0 * (ux_0 - ux_0k) + q.zy * ((uy_jp - uy_jpkm) - (uy_0 - uy_km));   // carry nu
-    gi = -cf.inv_hz * (p_0 - MPP());
+    gi = -ZIH * (C)(p_0 - MPP());
     ROUTE(ix, q.lxl * (uz_im - uz_0) + q.lxu * (uz_ip - uz_0));
     ROUTE(iy, q.ly * ((uz_jm - uz_0) + (uz_jp - uz_0)));
-    ROUTE(iz, 2. * nu * (cf.lz_l * uz_km + cf.lz_c * uz_0 + cf.lz_u * uz_kp));
-    if constexpr (IMPL == -2) e += ss.frc[VUZ][qc];
+    ROUTE(iz, C(2) * nu * (ZL * uz_km + ZC * uz_0 + ZU * uz_kp));
+    if constexpr (IMPL == -2) e += (C)ss.frc[VUZ][qc];
     ss.new_[VUZ][qc] = (T)e;
     dl[1] = ca * e + cb * old_z + cg * gi;
   }
   u0[0] = uy_0;
   u0[1] = uz_0;
 }
+#undef ZL
+#undef ZC
+#undef ZU
+#undef ZIH
 #undef ROW_
 #undef ODD_
 #undef UX
@@ -533,24 +562,28 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
     if (k0 + 1 < k1) fetch_olds(k0 + 1, 1);
   }
 
-  CoefA qa;
-  CoefB qb;
+  // arithmetic type of the right-hand sides
+  using C = typename std::conditional<sizeof(T) == 4 && TC_MARCH_FP32_ARITH, float, double>::type;
+  CoefA<C> qa;
+  CoefB<C> qb;
   load_coefs(qa, A.cf, act ? i : 1);
   load_coefs(qb, A.cf, act ? i : 1);
+  const CoefZ<C> qz{(C)A.cf.lz_l, (C)A.cf.lz_c, (C)A.cf.lz_u, (C)A.cf.inv_hz};
   // the diffusivities folded into the per-thread coefficients once, so the
   // cell updates multiply by them no more (the z Laplacian, a shared scalar
   // set, keeps its factor)
   {
-    const double nu = A.nu, n2 = 2. * A.nu;
+    const C nu = (C)A.nu, n2 = (C)(2. * A.nu);
     qa.lxl *= n2; qa.lxu *= n2; qa.ly *= nu;
     qa.cy1 *= nu; qa.cy2 *= nu; qa.ca1 *= nu; qa.ca2 *= nu; qa.cz1 *= nu;
     qb.lxl *= nu; qb.lxu *= nu; qb.ly *= nu;
     qb.p1 *= nu; qb.p2 *= nu; qb.qm *= nu; qb.q0 *= nu; qb.qp *= nu; qb.yk *= nu; qb.yz *= nu;
     qb.zx0 *= nu; qb.zx1 *= nu; qb.zy *= nu;
   }
-  const double rpr = A.kappa / A.nu;   // the scalar's Laplacians use the centred tables with kappa
+  const C rpr = (C)(A.kappa / A.nu);   // the scalar's Laplacians use the centred tables with kappa
   const int rk = A.rkstep;
-  const double ca = rk_alpha(rk) * dt, cb = rk_beta(rk) * dt, cg = rk_gamma(rk) * dt;
+  const C ca = (C)(rk_alpha(rk) * dt), cb = (C)(rk_beta(rk) * dt), cg = (C)(rk_gamma(rk) * dt);
+  const C nu_c = (C)A.nu, kappa_c = (C)A.kappa;
 
   // planes k0 - 1 and k0
   wait(&bar[0], 0);
@@ -670,11 +703,11 @@ __device__ __forceinline__ void march_fields(const MarchArgs<T> & A, char * ring
           }
         };
         // old(VUX) at i = 1 reads the shared-memory word before the line (discarded)
-        cell_a<JT, RL, JL, IMPL>(qa, qb, V, A.bc, A.cf, A.nu, A.kappa, rpr, i, qf + (size_t)JL * lf,
-                                 qc + (size_t)JL * lc, A.ss, ca, cb, cg, old(VUX), old(VT), d2, w2);
+        cell_a<JT, RL, JL, IMPL>(qa, qb, V, A.bc, A.cf, qz, nu_c, kappa_c, rpr, i, qf + (size_t)JL * lf,
+                                 qc + (size_t)JL * lc, A.ss, ca, cb, cg, (C)old(VUX), (C)old(VT), d2, w2);
         dl[JL][VUX] = d2[0]; dl[JL][VT] = d2[1]; u0[JL][VUX] = w2[0]; u0[JL][VT] = w2[1];
-        cell_b<JT, RL, JL, IMPL>(qb, V, A.bc, A.cf, A.nu, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
-                                 old(VUY), old(VUZ), d2, w2);
+        cell_b<JT, RL, JL, IMPL>(qb, V, A.bc, A.cf, qz, nu_c, i, qc + (size_t)JL * lc, A.ss, ca, cb, cg,
+                                 (C)old(VUY), (C)old(VUZ), d2, w2);
         dl[JL][VUY] = d2[0]; dl[JL][VUZ] = d2[1]; u0[JL][VUY] = w2[0]; u0[JL][VUZ] = w2[1];
       };
       cells(std::integral_constant<int, 0>());
