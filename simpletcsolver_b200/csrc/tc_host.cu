@@ -509,6 +509,23 @@ static int build_tables(Ctx & c, const domain_t * d) {
   };
   c.ps.tw_y = twiddles(ny);
   c.ps.tw_z = twiddles(nz);
+  // FP32-storage contexts transform in float: the same tables rounded once
+  auto twiddles32 = [&](int N) -> float2 * {
+    std::vector<float> tw(2 * (size_t)N);
+    for (int k = 0; k < N; k++) {
+      const double a = 2. * g_pi * k / N;
+      tw[2 * k] = (float)cos(a);
+      tw[2 * k + 1] = (float)-sin(a);
+    }
+    float * p = static_cast<float *>(valloc(c, 2 * (size_t)N * sizeof(float)));
+    if (p) cudaMemcpy(p, tw.data(), 2 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice);
+    return reinterpret_cast<float2 *>(p);
+  };
+  if (c.sb == 4) {
+    c.ps.tw_y32 = twiddles32(ny);
+    c.ps.tw_z32 = twiddles32(nz);
+    if (!c.ps.tw_y32 || !c.ps.tw_z32) return fail("cudaMalloc of Poisson buffers failed");
+  }
   const size_t nspec = (size_t)nx * nz * nyh;
   c.ps.spec_bytes = 2 * c.sb;
   c.ps.spec = valloc(c, nspec * c.ps.spec_bytes);

@@ -172,6 +172,8 @@ struct Poisson {
   double * fv;              // back-substitution factors
   const double2 * tw_y;     // exp(-2 pi i m / ny), m < ny
   const double2 * tw_z;     // exp(-2 pi i m / nz), m < nz
+  const float2 * tw_y32;    // the same rounded to float (FP32-storage contexts, whose transforms run in float)
+  const float2 * tw_z32;
   const double * tl;        // radial l_i (compute_potential.c:197-200), length nx
   const double * tu;        // radial u_i
   const double * ihy2;      // 1 / HYXC(i)^2 as (1/HYXC)/HYXC, length nx (index i-1)

@@ -96,6 +96,16 @@
 #ifndef TC_DIVFFT_MIN_BLOCKS
 #define TC_DIVFFT_MIN_BLOCKS 2
 #endif
+// the same for the float transforms of the FP32-storage mode
+#ifndef TC_DIVFFT_MIN_BLOCKS32
+#define TC_DIVFFT_MIN_BLOCKS32 3
+#endif
+#ifndef TC_FFTZ_MIN_BLOCKS32
+#define TC_FFTZ_MIN_BLOCKS32 4
+#endif
+#ifndef TC_IFFTY_MIN_BLOCKS32
+#define TC_IFFTY_MIN_BLOCKS32 3
+#endif
 
 namespace tcgpu {
 
@@ -111,9 +121,31 @@ __device__ __forceinline__ double2 zget(const float2 * p) {
 __device__ __forceinline__ void zput(double2 * p, double2 v) { *p = v; }
 __device__ __forceinline__ void zput(float2 * p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
 
-__device__ inline double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// The power-of-two transforms compute in the stored precision: double2, or
+// float2 in the FP32-storage mode (the radial Poisson eliminations, the
+// divergence and the direct transforms stay double).
+template <class CX> struct CxT;
+template <> struct CxT<double2> {
+  using R = double;
+  __device__ static double2 mk(double x, double y) { return make_double2(x, y); }
+};
+template <> struct CxT<float2> {
+  using R = float;
+  __device__ static float2 mk(float x, float y) { return make_float2(x, y); }
+};
+template <class CX>
+__device__ __forceinline__ CX mkc(typename CxT<CX>::R x, typename CxT<CX>::R y) { return CxT<CX>::mk(x, y); }
+template <class CX>
+__device__ __forceinline__ CX cmul(CX a, CX b) {
+  return mkc<CX>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// twiddle tables in the transforms' precision
+template <class CX> __device__ __forceinline__ const CX * tw_y_of(const Poisson & ps);
+template <> __device__ __forceinline__ const double2 * tw_y_of<double2>(const Poisson & ps) { return ps.tw_y; }
+template <> __device__ __forceinline__ const float2 * tw_y_of<float2>(const Poisson & ps) { return ps.tw_y32; }
+template <class CX> __device__ __forceinline__ const CX * tw_z_of(const Poisson & ps);
+template <> __device__ __forceinline__ const double2 * tw_z_of<double2>(const Poisson & ps) { return ps.tw_z; }
+template <> __device__ __forceinline__ const float2 * tw_z_of<float2>(const Poisson & ps) { return ps.tw_z32; }
 
 // Shared-memory lines are padded by one slot per 16 complex values so that the
 // strided stores of the first pass and the unit-stride accesses of the others
@@ -121,17 +153,17 @@ __device__ inline double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 __host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4) + 1; }
 
-template <int SIGN>
-__device__ __forceinline__ double2 twid(const double2 * __restrict__ tw, int m) {
-  double2 w = __ldg(tw + m);
+template <int SIGN, class CX>
+__device__ __forceinline__ CX twid(const CX * __restrict__ tw, int m) {
+  CX w = __ldg(tw + m);
   if (SIGN > 0) w.y = -w.y;
   return w;
 }
 
 // multiply by exp(SIGN i pi / 2) = SIGN i
-template <int SIGN>
-__device__ __forceinline__ double2 quarter(double2 z) {
-  return SIGN < 0 ? make_double2(z.y, -z.x) : make_double2(-z.y, z.x);
+template <int SIGN, class CX>
+__device__ __forceinline__ CX quarter(CX z) {
+  return SIGN < 0 ? mkc<CX>(z.y, -z.x) : mkc<CX>(-z.y, z.x);
 }
 
 template <int R>
@@ -145,25 +177,26 @@ __host__ __device__ constexpr int brev(int a) {
 // cos and sin of multiples of pi/8 (sqrt(2 + sqrt 2)/2, sqrt(2)/2,
 // sqrt(2 - sqrt 2)/2), correctly rounded
 __device__ constexpr double kC1 = 0.92387953251128674, kC2 = 0.70710678118654752, kC3 = 0.38268343236508977;
-template <int SIGN>
-__device__ __forceinline__ double2 twid16(int m) {
+template <int SIGN, class CX>
+__device__ __forceinline__ CX twid16(int m) {
+  using R = typename CxT<CX>::R;
   const double c = m == 0 ? 1. : m == 1 ? kC1 : m == 2 ? kC2 : m == 3 ? kC3 : m == 4 ? 0. : m == 5 ? -kC3
                  : m == 6 ? -kC2 : -kC1;
   const double sn = m == 0 ? 0. : m == 1 ? kC3 : m == 2 ? kC2 : m == 3 ? kC1 : m == 4 ? 1. : m == 5 ? kC1
                   : m == 6 ? kC2 : kC3;
-  return make_double2(c, SIGN < 0 ? -sn : sn);
+  return mkc<CX>((R)c, (R)(SIGN < 0 ? -sn : sn));
 }
 
 // In-register DFT of R points: v[s] <- sum_r v[r] exp(SIGN 2 pi i r s / R),
 // iterative radix-2 decimation in time; twiddles exp(SIGN 2 pi i k / len) are
 // compile-time constants (R <= 16).
-template <int R, int SIGN>
-__device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict__ tw, int N) {
+template <int R, int SIGN, class CX>
+__device__ __forceinline__ void dft_reg(CX * v, const CX * __restrict__ tw, int N) {
 #pragma unroll
   for (int a = 0; a < R; a++) {
     const int b = brev<R>(a);
     if (a < b) {
-      const double2 t = v[a];
+      const CX t = v[a];
       v[a] = v[b];
       v[b] = t;
     }
@@ -173,16 +206,16 @@ __device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict_
     const int half = len >> 1;
 #pragma unroll
     for (int k = 0; k < half; k++) {
-      double2 w = make_double2(1., 0.);
-      if (k != 0 && 4 * k != len) w = twid16<SIGN>(k * (16 / len));
+      CX w = mkc<CX>(1, 0);
+      if (k != 0 && 4 * k != len) w = twid16<SIGN, CX>(k * (16 / len));
 #pragma unroll
       for (int s = 0; s < R; s += len) {
-        const double2 a = v[s + k];
-        double2 b = v[s + k + half];
+        const CX a = v[s + k];
+        CX b = v[s + k + half];
         if (4 * k == len) b = quarter<SIGN>(b);
         else if (k != 0) b = cmul(b, w);
-        v[s + k] = make_double2(a.x + b.x, a.y + b.y);
-        v[s + k + half] = make_double2(a.x - b.x, a.y - b.y);
+        v[s + k] = mkc<CX>(a.x + b.x, a.y + b.y);
+        v[s + k + half] = mkc<CX>(a.x - b.x, a.y - b.y);
       }
     }
   }
@@ -201,14 +234,14 @@ __device__ __forceinline__ void dft_reg(double2 * v, const double2 * __restrict_
 #ifndef TC_FFT_TWIDDLE_PAIRED
 #define TC_FFT_TWIDDLE_PAIRED 1
 #endif
-template <int R, int SIGN>
-__device__ __forceinline__ void apply_twiddles(double2 * v, const double2 * __restrict__ tw, int step) {
+template <int R, int SIGN, class CX>
+__device__ __forceinline__ void apply_twiddles(CX * v, const CX * __restrict__ tw, int step) {
   if (TC_FFT_TWIDDLE_PRODUCTS) {
-    double2 p2[4];   // w^1, w^2, w^4, w^8
+    CX p2[4];   // w^1, w^2, w^4, w^8
 #pragma unroll
     for (int b = 0; (1 << b) < R; b++) p2[b] = twid<SIGN>(tw, (1 << b) * step);
-    double2 low[8];  // w^0 .. w^7 as products of p2
-    low[0] = make_double2(1., 0.);
+    CX low[8];  // w^0 .. w^7 as products of p2
+    low[0] = mkc<CX>(1, 0);
 #pragma unroll
     for (int r = 1; r < R && r < 8; r++) {
       const int hb = 31 - __clz(r);
@@ -257,10 +290,9 @@ __device__ __forceinline__ void line_barrier(int TPL) {
 // One in-place Stockham pass of radix R over a padded line x of length N: the
 // thread owns butterflies j = t + b TPL (b < B); Ns is the product of the
 // radices already applied. All inputs are read before anything is written.
-template <int R, int B, int SIGN, bool LB>
-__device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t, int TPL,
-                                              const double2 * __restrict__ tw) {
-  double2 v[B][R];
+template <int R, int B, int SIGN, bool LB, class CX>
+__device__ __forceinline__ void stockham_pass(CX * x, int N, int Ns, int t, int TPL, const CX * __restrict__ tw) {
+  CX v[B][R];
   const int NR = N / R;
 #pragma unroll
   for (int b = 0; b < B; b++) {
@@ -287,8 +319,8 @@ __device__ __forceinline__ void stockham_pass(double2 * x, int N, int Ns, int t,
 
 // Full transform of the CTA's lines (N = 2^lg): EPT elements per thread,
 // radix-16 passes then the remainder; natural-order output in place.
-template <int EPT, int SIGN, bool LB = false>
-__device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const double2 * __restrict__ tw) {
+template <int EPT, int SIGN, bool LB = false, class CX>
+__device__ void fft_inplace(CX * x, int N, int lg, int t, int TPL, const CX * __restrict__ tw) {
   int Ns = 1;
   int left = lg;
   while (left > 0) {
@@ -318,10 +350,10 @@ __device__ void fft_inplace(double2 * x, int N, int lg, int t, int TPL, const do
 // and last passes of a transform whose input or output lives elsewhere, so
 // the data crosses shared memory only between passes. A pass that reads and
 // writes the shared line synchronises like stockham_pass.
-template <int R, int B, int SIGN, bool IN, bool OUT, bool LB, class Ld, class St>
-__device__ __forceinline__ void stockham_pass_io(double2 * x, const Ld & ld, const St & st, int N, int Ns, int t,
-                                                 int TPL, const double2 * __restrict__ tw) {
-  double2 v[B][R];
+template <int R, int B, int SIGN, bool IN, bool OUT, bool LB, class CX, class Ld, class St>
+__device__ __forceinline__ void stockham_pass_io(CX * x, const Ld & ld, const St & st, int N, int Ns, int t,
+                                                 int TPL, const CX * __restrict__ tw) {
+  CX v[B][R];
   const int NR = N / R;
 #pragma unroll
   for (int b = 0; b < B; b++) {
@@ -352,9 +384,9 @@ __device__ __forceinline__ void stockham_pass_io(double2 * x, const Ld & ld, con
 // Full transform of one line (N = 2^lg) whose input comes from ld (IN_LD) or
 // the shared line x, and whose output goes to st (OUT_ST) or back to x; the
 // passes between go through x.
-template <int EPT, int SIGN, bool IN_LD, bool OUT_ST, bool LB = false, class Ld, class St>
-__device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg, int t, int TPL,
-                       const double2 * __restrict__ tw) {
+template <int EPT, int SIGN, bool IN_LD, bool OUT_ST, bool LB = false, class CX, class Ld, class St>
+__device__ void fft_io(CX * x, const Ld & ld, const St & st, int N, int lg, int t, int TPL,
+                       const CX * __restrict__ tw) {
   int Ns = 1;
   int left = lg;
   auto pass = [&](auto rc, auto bc) {
@@ -392,11 +424,13 @@ __device__ void fft_io(double2 * x, const Ld & ld, const St & st, int N, int lg,
 // CTA: P complex lines (radial indices i0 .. i0+2P-1) x all j at one k;
 // TPL = ny / EPT threads per line.
 template <int EPT, class T, class Z>
-__global__ void __launch_bounds__(TC_FFTY_THREADS, TC_DIVFFT_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTY_THREADS, sizeof(Z) == 8 ? TC_DIVFFT_MIN_BLOCKS32 : TC_DIVFFT_MIN_BLOCKS)
 div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
                 const T * __restrict__ ux, const T * __restrict__ uy,
                 const T * __restrict__ uz, const double * __restrict__ dtp, int rkstep) {
   extern __shared__ double2 smem[];
+  using R = typename CxT<Z>::R;   // the transform's precision
+  Z * const zsm = reinterpret_cast<Z *>(smem);
   const int ny = g.ny, nx = g.nx, nz = g.nz;
   const int TI = 2 * P;
   const int TPL = ny / EPT;
@@ -429,15 +463,15 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
             - jz * uz_zm + jz * uz_zp);
         val = prefactor * div;
       }
-      double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
-      line[2 * pad(j - 1) + (ii & 1)] = val;
+      R * line = reinterpret_cast<R *>(zsm + (size_t)(ii >> 1) * LS);
+      line[2 * pad(j - 1) + (ii & 1)] = (R)val;
     }
   } else {
     const int ii = threadIdx.x % TI;
     const int j0 = threadIdx.x / TI + 1;
     const int jstep = blockDim.x / TI;
     const int i = i0 + ii;
-    double * line = reinterpret_cast<double *>(smem + (size_t)(ii >> 1) * LS);
+    R * line = reinterpret_cast<R *>(zsm + (size_t)(ii >> 1) * LS);
     if (i <= nx) {
       const double jxm = __ldg(cf.c_jf + i), jxp = __ldg(cf.c_jf + i + 1);
       const double jy = __ldg(cf.c_e1 + i), jz = __ldg(cf.c_e2 + i);
@@ -460,7 +494,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
             -jxm * ux_xm + jxp * ux_xp
             - jy * uy_ym + jy * uy_yp
             - jz * uz_zm + jz * uz_zp);
-        line[2 * pad(j - 1) + (ii & 1)] = prefactor * div;
+        line[2 * pad(j - 1) + (ii & 1)] = (R)(prefactor * div);
       }
     } else {
 #pragma unroll 8
@@ -469,7 +503,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
   }
   __syncthreads();
   const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
-  fft_inplace<EPT, -1, true>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+  fft_inplace<EPT, -1, true>(zsm + (size_t)p * LS, ny, lg, t, TPL, tw_y_of<Z>(ps));
   if (TC_FFT_LINE_BARRIER) __syncthreads();
   // separate the two real transforms and store the ny/2+1 non-negative
   // wavenumbers: m < ny/2 for every radial index (power-of-two index
@@ -478,13 +512,13 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
   auto put = [&](int ii, int m) {
     const int i = i0 + ii;
     if (i > nx) return;
-    const double2 * z = smem + (size_t)(ii >> 1) * LS;
-    const double2 zm = z[pad(m)];
-    const double2 zn = z[pad((ny - m) & (ny - 1))];
-    double2 out;
-    if ((ii & 1) == 0) out = make_double2(0.5 * (zm.x + zn.x), 0.5 * (zm.y - zn.y));
-    else out = make_double2(0.5 * (zm.y + zn.y), -0.5 * (zm.x - zn.x));
-    zput(static_cast<Z *>(ps.spec) + ((size_t)(i - 1) * nz + (k - 1)) * nyh + m, out);
+    const Z * z = zsm + (size_t)(ii >> 1) * LS;
+    const Z zm = z[pad(m)];
+    const Z zn = z[pad((ny - m) & (ny - 1))];
+    Z out;
+    if ((ii & 1) == 0) out = mkc<Z>(R(0.5) * (zm.x + zn.x), R(0.5) * (zm.y - zn.y));
+    else out = mkc<Z>(R(0.5) * (zm.y + zn.y), R(-0.5) * (zm.x - zn.x));
+    static_cast<Z *>(ps.spec)[((size_t)(i - 1) * nz + (k - 1)) * nyh + m] = out;
   };
   for (int idx = threadIdx.x; idx < TI * half; idx += blockDim.x) put(idx >> (lg - 1), idx & (half - 1));
   for (int ii = threadIdx.x; ii < TI; ii += blockDim.x) put(ii, half);
@@ -496,7 +530,7 @@ div_ffty_kernel(Geo g, Coefs cf, Poisson ps, int P, int lg,
 // the first pass reads and the last pass writes rows of P values straight from
 // and to the spectral array.
 template <int EPT, int SIGN, class Z>
-__global__ void __launch_bounds__(TC_FFTZ_THREADS, TC_FFTZ_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTZ_THREADS, sizeof(Z) == 8 ? TC_FFTZ_MIN_BLOCKS32 : TC_FFTZ_MIN_BLOCKS)
 fftz_kernel(Geo g, Poisson ps, int P, int lg) {
   extern __shared__ double2 smem[];
   const int nz = g.nz, nyh = ps.nyh;
@@ -513,9 +547,9 @@ fftz_kernel(Geo g, Poisson ps, int P, int lg) {
 #endif
   Z * col = static_cast<Z *>(ps.spec) + (size_t)i * nz * nyh + m;
   const bool gv = m < nyh;
-  auto ld = [&](int e) { return gv ? zget(col + (size_t)e * nyh) : make_double2(0., 0.); };
-  auto st = [&](int e, double2 v) { if (gv) zput(col + (size_t)e * nyh, v); };
-  fft_io<EPT, SIGN, true, true>(smem + (size_t)p * LS, ld, st, nz, lg, t, TPL, ps.tw_z);
+  auto ld = [&](int e) { return gv ? col[(size_t)e * nyh] : mkc<Z>(0, 0); };
+  auto st = [&](int e, Z v) { if (gv) col[(size_t)e * nyh] = v; };
+  fft_io<EPT, SIGN, true, true>(reinterpret_cast<Z *>(smem) + (size_t)p * LS, ld, st, nz, lg, t, TPL, tw_z_of<Z>(ps));
 }
 
 // --------------------------------------------------------------- radial solve
@@ -832,10 +866,13 @@ static bool launch_tdm_lines(const Geo & g, const Poisson & ps, cudaStream_t st)
 // after a barrier writes the extended lines over the staged rows. Otherwise
 // each thread loads its values from global memory.
 template <int EPT, class Z, bool BULK>
-__global__ void __launch_bounds__(TC_FFTY_THREADS, BULK ? TC_IFFTY_BULK_MIN_BLOCKS : TC_IFFTY_MIN_BLOCKS)
+__global__ void __launch_bounds__(TC_FFTY_THREADS, BULK ? TC_IFFTY_BULK_MIN_BLOCKS
+                                                  : sizeof(Z) == 8 ? TC_IFFTY_MIN_BLOCKS32 : TC_IFFTY_MIN_BLOCKS)
 iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
   static_assert(!BULK || sizeof(Z) == 16, "bulk rows: FP64 spectra (16-byte values)");
   extern __shared__ double2 smem[];
+  using R = typename CxT<Z>::R;   // the transform's precision
+  Z * const zsm = reinterpret_cast<Z *>(smem);
   const int ny = g.ny, nx = g.nx, nz = g.nz, nyh = ps.nyh;
   const int TI = 2 * P;
   const int TPL = ny / EPT;
@@ -905,25 +942,25 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
       const int mr = u & (half - 1);
       const int pp = u >> (lg - 1);
       const int ia = i0 + 2 * pp, ib = ia + 1;
-      double2 xa = make_double2(0., 0.), xb = make_double2(0., 0.);
-      if (ia <= nx) xa = zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr);
-      if (ib <= nx) xb = zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr);
-      if (mr == 0) { xa.y = 0.; xb.y = 0.; }
-      double2 * line = smem + (size_t)pp * LS;
-      line[pad(mr)] = make_double2(xa.x - xb.y, xa.y + xb.x);
-      if (mr != 0) line[pad(ny - mr)] = make_double2(xa.x + xb.y, -xa.y + xb.x);
+      Z xa = mkc<Z>(0, 0), xb = mkc<Z>(0, 0);
+      if (ia <= nx) xa = sp[((size_t)(ia - 1) * nz + (k - 1)) * nyh + mr];
+      if (ib <= nx) xb = sp[((size_t)(ib - 1) * nz + (k - 1)) * nyh + mr];
+      if (mr == 0) { xa.y = 0; xb.y = 0; }
+      Z * line = zsm + (size_t)pp * LS;
+      line[pad(mr)] = mkc<Z>(xa.x - xb.y, xa.y + xb.x);
+      if (mr != 0) line[pad(ny - mr)] = mkc<Z>(xa.x + xb.y, -xa.y + xb.x);
     }
     for (int pp = threadIdx.x; pp < P; pp += blockDim.x) {
       const int ia = i0 + 2 * pp, ib = ia + 1;
-      const double xa = ia <= nx ? zget(sp + ((size_t)(ia - 1) * nz + (k - 1)) * nyh + half).x : 0.;
-      const double xb = ib <= nx ? zget(sp + ((size_t)(ib - 1) * nz + (k - 1)) * nyh + half).x : 0.;
-      smem[(size_t)pp * LS + pad(half)] = make_double2(xa, xb);
+      const R xa = ia <= nx ? sp[((size_t)(ia - 1) * nz + (k - 1)) * nyh + half].x : R(0);
+      const R xb = ib <= nx ? sp[((size_t)(ib - 1) * nz + (k - 1)) * nyh + half].x : R(0);
+      zsm[(size_t)pp * LS + pad(half)] = mkc<Z>(xa, xb);
     }
   }
   __syncthreads();
   {
     const int p = threadIdx.x / TPL, t = threadIdx.x % TPL;
-    fft_inplace<EPT, +1, true>(smem + (size_t)p * LS, ny, lg, t, TPL, ps.tw_y);
+    fft_inplace<EPT, +1, true>(zsm + (size_t)p * LS, ny, lg, t, TPL, tw_y_of<Z>(ps));
   }
   if (TC_FFT_LINE_BARRIER) __syncthreads();
   // one radial index per thread when TI divides the block size (ny >= 2 EPT),
@@ -938,15 +975,15 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
     const int ii = threadIdx.x & (TI - 1), i = i0 + ii;
     if (i > nx) return;
     const int js = blockDim.x >> lgt;
-    const double2 * zs = smem + (size_t)(ii >> 1) * LS;
+    const Z * zs = zsm + (size_t)(ii >> 1) * LS;
     const bool hi = (ii & 1) != 0, kedge = k == 1 || k == nz;
     int j = (threadIdx.x >> lgt) + 1;
     double * out = psi + cidx(g, i, j, k);
     const size_t step = (size_t)js * (nx + 2);
 #pragma unroll 4
     for (int r = 0; r < 2 * EPT; r++, j += js, out += step) {
-      const double2 z = zs[pad(j - 1)];
-      const double val = hi ? z.y : z.x;
+      const Z z = zs[pad(j - 1)];
+      const double val = (double)(hi ? z.y : z.x);
       *out = val;
       if (i == 1) out[-1] = val;
       if (i == nx) out[1] = val;
@@ -970,8 +1007,8 @@ iffty_kernel(Geo g, Poisson ps, int P, int lg, double * __restrict__ psi) {
     const int j = fixed_i ? (idx >> lgt) + 1 + r * (blockDim.x >> lgt) : (idx >> lgt) + 1;
     const int i = i0 + ii;
     if (i > nx) continue;
-    const double2 z = smem[(size_t)(ii >> 1) * LS + pad(j - 1)];
-    const double val = (ii & 1) ? z.y : z.x;
+    const Z z = zsm[(size_t)(ii >> 1) * LS + pad(j - 1)];
+    const double val = (double)((ii & 1) ? z.y : z.x);
     auto put = [&](int jj, int kk) {
       psi[cidx(g, i, jj, kk)] = val;
       if (i == 1) psi[cidx(g, 0, jj, kk)] = val;
@@ -1111,7 +1148,7 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   const int lgy = ilog2(g.ny), lgz = ilog2(g.nz);
   const int Py = lines_per_cta(g.ny, (g.nx + 1) / 2, EPTY, TC_FFTY_THREADS);
   const int tply = g.ny / EPTY;
-  const size_t smy = sizeof(double2) * (size_t)Py * padded_len(g.ny);
+  const size_t smy = sizeof(Z) * (size_t)Py * padded_len(g.ny);
   dim3 gy((g.nx + 2 * Py - 1) / (2 * Py), g.nz);
   const dim3 gl(g.nx, g.nz);   // one CTA per (i, k) line of the direct transforms in y
   if (fy) div_ffty_kernel<EPTY, T, Z><<<gy, Py * tply, smy, st>>>(g, cf, ps, Py, lgy, f.ux, f.uy, f.uz, dtp, rkstep);
@@ -1119,7 +1156,7 @@ static void launch_poisson_t(const Geo & g, const Coefs & cf, const Poisson & ps
   mark(pm.k_div);
   const int Pz = lines_per_cta(g.nz, ps.nyh, EPTZ, TC_FFTZ_THREADS);
   const int tplz = g.nz / EPTZ;
-  const size_t smz = sizeof(double2) * (size_t)Pz * padded_len(g.nz);
+  const size_t smz = sizeof(Z) * (size_t)Pz * padded_len(g.nz);
 #if TC_FFTZ_MFAST
   dim3 gz((ps.nyh + Pz - 1) / Pz, g.nx);
 #else
