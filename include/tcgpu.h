@@ -245,9 +245,9 @@ int tcgpu_set_device(int device);
  * the RK source terms and the Poisson spectra in 4-byte floats (in a padded
  * device layout; host arrays stay the reference's doubles and are converted on
  * every copy), while p, psi and every coefficient table stay FP64; the
- * predict forms its explicit right-hand sides in FP32 arithmetic, and the
- * implicit solves, the Poisson solve, the correction and the reductions stay
- * FP64. An existing context keeps its storage until tcgpu_release(). Returns 0, or
+ * predict forms its explicit right-hand sides and the power-of-two y/z
+ * transforms run in FP32 arithmetic, and the implicit solves, the radial
+ * Poisson eliminations, the correction and the reductions stay FP64. An existing context keeps its storage until tcgpu_release(). Returns 0, or
  * non-zero for other byte counts. */
 int tcgpu_set_storage(int bytes);
 /* bytes per stored value of this fluid's context (the default for new ones
