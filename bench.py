@@ -595,17 +595,23 @@ def closure_arm(args, lib, d0, case, peaks):
         train_s = time.perf_counter() - t0
         err_train = closure.relative_error(net, data, train)
         err_held = closure.relative_error(net, data, held)
-        # forward pass on the tensor cores: CUDA events on the stream it runs on
+        # forward pass on the tensor cores: CUDA events on the stream it runs on;
+        # the median of 7 repeats of 20 passes, SM clocks sampled meanwhile
+        # (the passes follow the training run, so the clock it left matters)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         x = data.X[0]
         for _ in range(3):
             net.forward(x, keep=False)
-        e0.record()
-        for _ in range(20):
-            net.forward(x, keep=False)
-        e1.record()
-        torch.cuda.synchronize()
-        fwd_ms = e0.elapsed_time(e1) / 20
+        fwd_reps = []
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as fclk:
+            for _ in range(7):
+                e0.record()
+                for _ in range(20):
+                    net.forward(x, keep=False)
+                e1.record()
+                torch.cuda.synchronize()
+                fwd_reps.append(e0.elapsed_time(e1) / 20)
+        fwd_ms = statistics.median(fwd_reps)
         tflops = CLOSURE_FLOP_PER_CELL * net.ncell / (fwd_ms / 1e3) / 1e12
         peak = float(peaks.get("bf16_tflops", 1590.0))
         # torque window: fine, coarse with and without the closure from one state
@@ -658,7 +664,8 @@ def closure_arm(args, lib, d0, case, peaks):
                          "loss_first": hist[0], "loss_last": hist[-1]},
             "apriori_rel_error": {"no_closure": 1.0, "train": err_train, "held_out": err_held,
                                   "held_out_untrained": before},
-            "forward": {"ms": fwd_ms, "tflops": tflops, "peak_tflops": peak, "frac": tflops / peak,
+            "forward": {"ms": fwd_ms, "repeats_ms": fwd_reps, "clocks": fclk.summary(), "tflops": tflops,
+                        "peak_tflops": peak, "frac": tflops / peak,
                         "flop_per_cell": CLOSURE_FLOP_PER_CELL,
                         "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"},
             "wall_model": {"weights": [float(v) for v in wm.w], "fit_samples": wm.samples,
